@@ -1,0 +1,205 @@
+/*
+ * sdft_b200.h -- C ABI of the B200 stochastic-DFT filter hot path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int
+ * status (SDFT_OK == 0).  Orbital arrays use the PINY layout: state-major,
+ * coefficient-minor, half G-sphere with G=0 stored LAST, separate real and
+ * imaginary arrays.  Pointers here are 0-based; a PINY caller holding the
+ * 1-based cmalloc(n)-1 pointer passes &p[1].
+ *
+ * Reference interfaces replaced (file:line inside the reference project):
+ *   sdft_gvec_count / sdft_gvec_fill  <- setkvec3d_sm        interface/cp_ewald/set_cp_ewald.c:685
+ *   sdft_fft_maps                     <- setfft_indx (filter maps)  mathlib/fft_create_package.c:981,139-248
+ *   sdft_hpsi                         <- calcCoefForceWrapSCF stodft/reduced-energy/energy-wrapper-scf.c:1066
+ *   sdft_normh_cheby                  <- normHCheby          stodft/normh.c:182
+ *   sdft_normh_newton                 <- normHNewtonHerm     stodft/normh.c:35
+ *   sdft_filter_cheby                 <- filterChebyPolyHerm stodft/filter.c:318
+ *   sdft_filter_newton                <- filterNewtonPolyHerm stodft/filter.c:33
+ *   sdft_cheby_moments                <- calcChebyMoments    stodft/calc-chempot-chebyshev.c:596
+ *   sdft_chempot_cheby                <- calcChemPotCheby (bisection part) stodft/calc-chempot-chebyshev.c:30
+ *   sdft_num_elec_cheby               <- calcNumElecCheby    stodft/calc-chempot-chebyshev.c:918
+ *   sdft_cheby_coeff                  <- calcChebyCoeff      stodft/coeff.c:1093
+ *   sdft_round_fft                    <- roundFFT            stodft/coeff.c:1556
+ *   sdft_newton_samp / sdft_newton_coeff <- genSampNewtonHermit / genCoeffNewtonHermit stodft/coeff.c:423,199
+ *   sdft_density                      <- rhoCalcRealStoHybrid stodft/density.c:43 (+ sum_rho mathlib/fft_package.c:2502)
+ *   sdft_noise_real                   <- genNoiseOrbitalReal stodft/gen-noise.c:162
+ *   sdft_gaussran2                    <- gaussran2 / ran_essl / DURAND mathlib/mathlib.c:118,30; mathlib/blas_wrappers.f:39
+ */
+#ifndef SDFT_B200_H
+#define SDFT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define SDFT_OK            0
+#define SDFT_ERR_ARG       1   /* invalid argument / size                  */
+#define SDFT_ERR_CUDA      2   /* CUDA runtime error (message via sdft_last_error) */
+#define SDFT_ERR_NOMEM     3   /* device allocation failed                 */
+#define SDFT_ERR_STATE     4   /* call out of order (e.g. no potential set) */
+#define SDFT_ERR_UNSUPPORTED 5 /* grid size / l channel not supported       */
+#define SDFT_ERR_NODEVICE  6   /* no CUDA device visible                    */
+#define SDFT_ERR_TIMEOUT   7   /* a bounded device-side wait gave up        */
+
+/* ---- precision modes ------------------------------------------------- */
+#define SDFT_PREC_FP64  0      /* everything FP64 (plain form)               */
+#define SDFT_PREC_MIXED 1      /* FP32 FFT + V multiply, TF32x3 KB GEMM,
+                                  FP64 recurrence / accumulators / reductions */
+
+typedef struct sdft_ctx sdft_ctx;
+
+/* Kleinman-Bylander projector description (one radial projector per l
+ * channel, n_rad = 1).  Radial form factors are PINY spline tables
+ * evaluated exactly as get_vpsnow (energy/cp/cp_energy_eext.c:2139):
+ *   v(g) = ((vps3*h + vps2)*h + vps1)*h + vps0,  h = g - g_i,
+ *   i = clamp((int)((g-gmin)/dg) + 1, 1, nsplin) (1-based knot).        */
+typedef struct {
+  int natm;              /* atoms carrying nonlocal channels             */
+  const double *pos;     /* natm*3 cartesian coordinates (bohr)          */
+  const int *type;       /* natm, 0-based atom type                      */
+  int ntype;
+  int lmax;              /* highest l channel present (0..2)             */
+  const int *lmax_type;  /* ntype: highest l of each type (-1 = none)    */
+  int nsplin_g;
+  double gmin_spl, dg_spl;
+  const double *vps;     /* [ntype][lmax+1][4][nsplin_g]: vps0..vps3     */
+  const double *vpsnorm; /* [ntype][lmax+1]  KB energies                 */
+  const double *gzvps0;  /* [ntype]  l=0 value at G=0                    */
+} sdft_kb_desc;
+
+/* ---- errors ----------------------------------------------------------- */
+const char *sdft_last_error(void);
+int sdft_version(void);
+
+/* ---- G-sphere setup (host only) --------------------------------------- */
+/* hmat: 9 doubles, PINY column-major cell matrix (hmat[0]=h11, hmat[1]=h21,
+ * ...).  ecut in Hartree: 0.5|G|^2 <= ecut.  kmax: scan limits (kmax_cp).
+ * Returns nktot (half sphere without G=0); ncoef = nktot+1.             */
+int sdft_gvec_count(const double *hmat, double ecut, const int *kmax, int *nktot);
+/* Fill ka/kb/kc[ncoef] (0-based arrays, G=0 last) and ibreak1/2[nktot]
+ * in the setkvec3d_sm order.                                            */
+int sdft_gvec_fill(const double *hmat, double ecut, const int *kmax, int nktot,
+                   int *ka, int *kb, int *kc, int *ibreak1, int *ibreak2);
+/* Complex grid indices of G and -G in the filter layout (c fastest):
+ * map[i] = mapFFTWFilter[i+1], mapc[i] = mapConFFTWFilter[i+1].        */
+int sdft_fft_maps(int nkf1, int nkf2, int nkf3, int ncoef, const int *ka,
+                  const int *kb, const int *kc, int *map, int *mapc);
+/* ak2Kinetic (get_ak2_sm, energy/cp/cp_energy_eext.c:2260): |G|^2, capped
+ * at gcut^2 when gcut > 0.  out[ncoef], G=0 entry 0.                    */
+int sdft_ak2_kinetic(const double *hmat, int ncoef, const int *ka, const int *kb,
+                     const int *kc, double gcut, double *ak2);
+
+/* ---- context ----------------------------------------------------------- */
+/* Creates a device context for one G-sphere / FFT grid.  max_states is the
+ * largest orbital block later passed to the compute calls.              */
+int sdft_ctx_create(int nkf1, int nkf2, int nkf3, int ncoef, const int *ka,
+                    const int *kb, const int *kc, const double *hmat,
+                    int precision, int max_states, int device, sdft_ctx **out);
+int sdft_ctx_destroy(sdft_ctx *ctx);
+/* Kinetic cutoff cap gCutoffKe (<=0: none).                             */
+int sdft_ctx_set_kinetic_cap(sdft_ctx *ctx, double gcut);
+/* V_KS(r): nkf1*nkf2*nkf3 doubles in the filter layout, c fastest
+ * (the reference's v_ks_up after the transpose at
+ * stodft/reduced-energy/cp-energy-ee-rho-stodft.c:984-1007).           */
+int sdft_ctx_set_vks(sdft_ctx *ctx, const double *v_ks);
+/* KB nonlocal projectors; kb == NULL or kb->natm == 0 disables them.   */
+int sdft_ctx_set_kb(sdft_ctx *ctx, const sdft_kb_desc *kb);
+/* Bytes of device memory the context holds (for HBM-budget admission). */
+long long sdft_ctx_device_bytes(const sdft_ctx *ctx);
+/* CUDA stream the context launches on (cudaStream_t as void*).          */
+void *sdft_ctx_stream(sdft_ctx *ctx);
+
+/* ---- hot path: host buffers in/out ------------------------------------- */
+/* Raw PINY coefficient force f = -(2 H c) scaled as the reference keeps it:
+ * H c = -f/4 (G != 0), -f/2 (G = 0).  enl (nullable): nonlocal energy. */
+int sdft_hpsi(sdft_ctx *ctx, int nstate, const double *cre, const double *cim,
+              double *fcre, double *fcim, double *enl);
+
+/* One normalized-H step.  cheby: iPoly>=1, wf1 = T_{k-1} (used if iPoly>1);
+ * on return f = T_{k+1}; with cpy_flag the buffers rotate as normHCheby.  */
+int sdft_normh_cheby(sdft_ctx *ctx, int nstate, int ipoly, int cpy_flag,
+                     double scale, double energy_mean, double *cre, double *cim,
+                     double *wf1re, double *wf1im, double *fcre, double *fcim);
+int sdft_normh_newton(sdft_ctx *ctx, int nstate, double scale, double energy_mean,
+                      double zn, double *cre, double *cim, double *fcre, double *fcim);
+
+/* Chebyshev filter: stoWf[imu] = sum_k expanCoeff[k*numChemPot+imu] T_k(Hn) chi.
+ * sto_re/sto_im: numChemPot host pointers to nstate*ncoef doubles.
+ * moments (nullable, storeChebyMomentsFlag): L+1 doubles, overwritten:
+ * moments[k] = sum_s <chi_s|T_k chi_s> (half-sphere weighted), k < L.  */
+int sdft_filter_cheby(sdft_ctx *ctx, int nstate, const double *cre, const double *cim,
+                      int L, int num_chem_pot, const double *expan_coeff,
+                      double scale, double energy_mean,
+                      double **sto_re, double **sto_im, double *moments);
+/* Newton filter with interpolation points samp_point[L].               */
+int sdft_filter_newton(sdft_ctx *ctx, int nstate, const double *cre, const double *cim,
+                       int L, int num_chem_pot, const double *expan_coeff,
+                       const double *samp_point, double scale, double energy_mean,
+                       double **sto_re, double **sto_im);
+/* Chebyshev moments by the doubling identities, L+1 doubles (unnormalised
+ * sum over the nstate orbitals, as before the Reduce of calcChemPotCheby). */
+int sdft_cheby_moments(sdft_ctx *ctx, int nstate, const double *cre, const double *cim,
+                       int L, double scale, double energy_mean, double *moments);
+/* rho[ia + nkf1*(ib + nkf2*ic)] = sum_s |psi_s(r)|^2 (package layout,
+ * a fastest), unscaled like rhoCalcRealStoHybrid's rho_scr.            */
+int sdft_density(sdft_ctx *ctx, int nstate, const double *cre, const double *cim,
+                 double *rho);
+/* Noise orbitals of genNoiseOrbitalReal for state-rank myid of np ranks:
+ * random +-sqrt(N) real-space values (gaussran2 signs), FFT to G.     */
+int sdft_noise_real(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid,
+                    double *cre, double *cim);
+
+/* ---- hot path: device-resident variants -------------------------------- */
+/* Orbital block kept in HBM by the context (slot 0: chi). */
+int sdft_upload_orbitals(sdft_ctx *ctx, int nstate, const double *cre, const double *cim);
+int sdft_noise_real_dev(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid);
+int sdft_filter_cheby_dev(sdft_ctx *ctx, int nstate, int L, int num_chem_pot,
+                          const double *expan_coeff, double scale, double energy_mean);
+int sdft_filter_newton_dev(sdft_ctx *ctx, int nstate, int L, int num_chem_pot,
+                           const double *expan_coeff, const double *samp_point,
+                           double scale, double energy_mean);
+int sdft_cheby_moments_dev(sdft_ctx *ctx, int nstate, int L, double scale,
+                           double energy_mean, double *moments);
+/* Density of the filtered orbitals of chem-pot imu, result stays on device
+ * unless rho != NULL.  occ_over_nsto scales it (aveFactUp).            */
+int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double occ_over_nsto,
+                     double *rho);
+int sdft_download_filtered(sdft_ctx *ctx, int nstate, int imu, double *re, double *im);
+int sdft_sync(sdft_ctx *ctx);
+/* Kernel launches issued by the context since creation (own kernels only). */
+long long sdft_launch_count(const sdft_ctx *ctx);
+/* Per-kernel device timing with CUDA events on the context stream.
+ * Kinds: 0 pack+c-FFT (stage A), 1 plane FFT x V (stage B), 2 c-FFT+unpack+
+ * recurrence (stage C), 3 KB projection GEMM, 4 KB back-projection GEMM,
+ * 5 density planes, 6 noise planes, 7 other.  read_timing synchronises,
+ * returns accumulated milliseconds / launch counts per kind and resets.   */
+#define SDFT_NKIND 8
+int sdft_ctx_set_timing(sdft_ctx *ctx, int enable);
+int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count);
+
+/* ---- host FP64 helpers (no device) ------------------------------------ */
+int sdft_round_fft(int n);
+/* fun_flag 1: F, 2: sqrt(F) (Fermi-Dirac 1/(1+exp(beta(x-mu)))).        */
+int sdft_cheby_coeff(int L, int num_cheby_grid, double energy_diff, double energy_mean,
+                     double beta, double chem_pot, int fun_flag, double *coeffs);
+double sdft_num_elec_cheby(int L, int num_cheby_grid, double energy_diff,
+                           double energy_mean, double beta, double chem_pot,
+                           double occ, const double *moments);
+/* Bisection of calcChemPotCheby on normalised moments (moments / N_sto). */
+int sdft_chempot_cheby(int L, double energy_diff, double energy_mean, double beta,
+                       double occ, const double *moments, double num_elec_true,
+                       double chem_pot_init, double gap_init, double *chem_pot,
+                       double *num_elec);
+int sdft_newton_samp(int L, double smin, double smax, double scale, double energy_min,
+                     double *samp_point, double *samp_point_unscale);
+int sdft_newton_coeff(int L, int num_chem_pot, const double *chem_pot, double beta,
+                      const double *samp_point, const double *samp_point_unscale,
+                      double *expan_coeff);
+/* gaussran2 with the DURAND uniform generator; qseed updated in place. */
+int sdft_gaussran2(int nran, double *qseed, double *gauss);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDFT_B200_H */

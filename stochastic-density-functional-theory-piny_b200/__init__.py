@@ -1,0 +1,400 @@
+"""B200 stochastic-DFT filter hot path (host-side Python mirror).
+
+The compute path is the CUDA library ``lib/libsdft_b200.so`` behind the C
+ABI declared in ``include/sdft_b200.h``; this module binds it with ctypes
+and mirrors the reference routines' names and argument meaning
+(mingchenPurdueChem/stochastic-density-functional-theory-piny):
+
+=============================  =========================================
+this module                    reference routine (file:line)
+=============================  =========================================
+``Context.calc_coef_force``     calcCoefForceWrapSCF  stodft/reduced-energy/energy-wrapper-scf.c:1066
+``Context.normHCheby``          normHCheby            stodft/normh.c:182
+``Context.normHNewtonHerm``     normHNewtonHerm       stodft/normh.c:35
+``Context.filterChebyPolyHerm`` filterChebyPolyHerm   stodft/filter.c:318
+``Context.filterNewtonPolyHerm`` filterNewtonPolyHerm stodft/filter.c:33
+``Context.calcChebyMoments``    calcChebyMoments      stodft/calc-chempot-chebyshev.c:596
+``Context.rhoCalcRealStoHybrid`` rhoCalcRealStoHybrid stodft/density.c:43
+``Context.genNoiseOrbitalReal`` genNoiseOrbitalReal   stodft/gen-noise.c:162
+``calcChemPotCheby``            calcChemPotCheby      stodft/calc-chempot-chebyshev.c:30
+``calcChebyCoeff``              calcChebyCoeff        stodft/coeff.c:1093
+``genSampNewtonHermit``         genSampNewtonHermit   stodft/coeff.c:423
+``genCoeffNewtonHermit``        genCoeffNewtonHermit  stodft/coeff.c:199
+``setkvec3d_sm``                setkvec3d_sm          interface/cp_ewald/set_cp_ewald.c:685
+=============================  =========================================
+
+Errors: every C call returns a status; a non-zero status raises
+``SdftError`` carrying ``sdft_last_error()`` (the reference prints an
+``@@@ERROR@@@`` banner and exits instead).  There is no CPU fallback: if
+the library is missing, importing this package raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libsdft_b200.so")
+
+SDFT_PREC_FP64 = 0
+SDFT_PREC_MIXED = 1
+
+_ERRNAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "UNSUPPORTED", 6: "NODEVICE", 7: "TIMEOUT"}
+
+
+class SdftError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sdft error {code} ({_ERRNAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} missing: build it with __graft_entry__.build() (no CPU fallback exists)")
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+
+class KbDesc(C.Structure):
+    _fields_ = [
+        ("natm", C.c_int), ("pos", _dp), ("type", _ip), ("ntype", C.c_int), ("lmax", C.c_int),
+        ("lmax_type", _ip), ("nsplin_g", C.c_int), ("gmin_spl", C.c_double), ("dg_spl", C.c_double),
+        ("vps", _dp), ("vpsnorm", _dp), ("gzvps0", _dp),
+    ]
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+# exported symbols (also checked by tests/test_abi.py against include/sdft_b200.h)
+_sig("sdft_last_error", C.c_char_p, [])
+_sig("sdft_version", C.c_int, [])
+_sig("sdft_gvec_count", C.c_int, [_dp, C.c_double, _ip, _ip])
+_sig("sdft_gvec_fill", C.c_int, [_dp, C.c_double, _ip, C.c_int, _ip, _ip, _ip, _ip, _ip])
+_sig("sdft_fft_maps", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip])
+_sig("sdft_ak2_kinetic", C.c_int, [_dp, C.c_int, _ip, _ip, _ip, C.c_double, _dp])
+_sig("sdft_ctx_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _dp, C.c_int, C.c_int,
+                                  C.c_int, C.POINTER(_vp)])
+_sig("sdft_ctx_destroy", C.c_int, [_vp])
+_sig("sdft_ctx_set_kinetic_cap", C.c_int, [_vp, C.c_double])
+_sig("sdft_ctx_set_vks", C.c_int, [_vp, _dp])
+_sig("sdft_ctx_set_kb", C.c_int, [_vp, C.POINTER(KbDesc)])
+_sig("sdft_ctx_device_bytes", C.c_longlong, [_vp])
+_sig("sdft_ctx_stream", _vp, [_vp])
+_sig("sdft_hpsi", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp])
+_sig("sdft_normh_cheby", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                                   _dp, _dp])
+_sig("sdft_normh_newton", C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp])
+_sig("sdft_filter_cheby", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, C.c_double, C.c_double,
+                                    C.POINTER(_dp), C.POINTER(_dp), _dp])
+_sig("sdft_filter_newton", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double,
+                                     C.POINTER(_dp), C.POINTER(_dp)])
+_sig("sdft_cheby_moments", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp])
+_sig("sdft_density", C.c_int, [_vp, C.c_int, _dp, _dp, _dp])
+_sig("sdft_noise_real", C.c_int, [_vp, C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp])
+_sig("sdft_upload_orbitals", C.c_int, [_vp, C.c_int, _dp, _dp])
+_sig("sdft_noise_real_dev", C.c_int, [_vp, C.c_int, C.c_double, C.c_int, C.c_int])
+_sig("sdft_filter_cheby_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, C.c_double, C.c_double])
+_sig("sdft_filter_newton_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double])
+_sig("sdft_cheby_moments_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, _dp])
+_sig("sdft_density_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _dp])
+_sig("sdft_download_filtered", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp])
+_sig("sdft_sync", C.c_int, [_vp])
+_sig("sdft_launch_count", C.c_longlong, [_vp])
+_sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
+_sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
+KERNEL_KINDS = ("stage_a_pack_cfft", "stage_b_plane_fft_vks", "stage_c_cfft_unpack_recur", "kb_proj_gemm",
+                "kb_back_gemm", "density_planes", "noise_planes", "other")
+_sig("sdft_round_fft", C.c_int, [C.c_int])
+_sig("sdft_cheby_coeff", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp])
+_sig("sdft_num_elec_cheby", C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, _dp])
+_sig("sdft_chempot_cheby", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, C.c_double,
+                                     C.c_double, C.c_double, _dp, _dp])
+_sig("sdft_newton_samp", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp])
+_sig("sdft_newton_coeff", C.c_int, [C.c_int, C.c_int, _dp, C.c_double, _dp, _dp, _dp])
+_sig("sdft_gaussran2", C.c_int, [C.c_int, _dp, _dp])
+
+
+def _chk(rc):
+    if rc != 0:
+        raise SdftError(rc, lib.sdft_last_error().decode(errors="replace"))
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---------------------------------------------------------------------------
+# host-side setup
+# ---------------------------------------------------------------------------
+def setkvec3d_sm(hmat, ecut, kmax):
+    """Half G-sphere in PINY order, G = 0 last: returns (ka, kb, kc, ibreak1, ibreak2).
+
+    hmat: 3x3 cell matrix with the cell vectors as columns (PINY hmat)."""
+    h = _f64(np.asarray(hmat, dtype=np.float64).reshape(3, 3).T.reshape(9))  # column-major
+    km = _i32(kmax)
+    n = C.c_int()
+    _chk(lib.sdft_gvec_count(_d(h), float(ecut), _i(km), C.byref(n)))
+    nk = n.value
+    ka, kb, kc = (np.zeros(nk + 1, np.int32) for _ in range(3))
+    b1, b2 = np.zeros(nk, np.int32), np.zeros(nk, np.int32)
+    _chk(lib.sdft_gvec_fill(_d(h), float(ecut), _i(km), nk, _i(ka), _i(kb), _i(kc), _i(b1), _i(b2)))
+    return ka, kb, kc, b1, b2
+
+
+def fft_maps(n1, n2, n3, ka, kb, kc):
+    ka, kb, kc = _i32(ka), _i32(kb), _i32(kc)
+    m, mc = np.zeros(len(ka), np.int32), np.zeros(len(ka), np.int32)
+    _chk(lib.sdft_fft_maps(n1, n2, n3, len(ka), _i(ka), _i(kb), _i(kc), _i(m), _i(mc)))
+    return m, mc
+
+
+def roundFFT(n):
+    return int(lib.sdft_round_fft(int(n)))
+
+
+def calcChebyCoeff(L, energy_diff, energy_mean, beta, chem_pot, fun_flag=2, num_cheby_grid=None):
+    """Chebyshev coefficients of F (fun_flag 1) or sqrt(F) (2) on [Emin, Emax]."""
+    ng = roundFFT(32 * L) if num_cheby_grid is None else int(num_cheby_grid)
+    out = np.zeros(L)
+    _chk(lib.sdft_cheby_coeff(L, ng, energy_diff, energy_mean, beta, chem_pot, fun_flag, _d(out)))
+    return out
+
+
+def calcNumElecCheby(L, energy_diff, energy_mean, beta, chem_pot, occ, moments):
+    m = _f64(moments)
+    return float(lib.sdft_num_elec_cheby(L, roundFFT(32 * L), energy_diff, energy_mean, beta, chem_pot, occ, _d(m)))
+
+
+def calcChemPotCheby(L, energy_diff, energy_mean, beta, occ, moments_normalised, num_elec_true, chem_pot_init,
+                     gap_init):
+    """Bisection on N(mu) = occ * sum_k c_k(mu) m_k; moments already divided by N_sto."""
+    m = _f64(moments_normalised)
+    mu, ne = C.c_double(), C.c_double()
+    _chk(lib.sdft_chempot_cheby(L, energy_diff, energy_mean, beta, occ, _d(m), num_elec_true, chem_pot_init,
+                                gap_init, C.byref(mu), C.byref(ne)))
+    return mu.value, ne.value
+
+
+def genSampNewtonHermit(L, smin, smax, scale, energy_min):
+    s, u = np.zeros(L), np.zeros(L)
+    _chk(lib.sdft_newton_samp(L, smin, smax, scale, energy_min, _d(s), _d(u)))
+    return s, u
+
+
+def genCoeffNewtonHermit(L, chem_pot, beta, samp, samp_unscale):
+    mu = _f64(np.atleast_1d(chem_pot))
+    ec = np.zeros(L * len(mu))
+    _chk(lib.sdft_newton_coeff(L, len(mu), _d(mu), beta, _d(_f64(samp)), _d(_f64(samp_unscale)), _d(ec)))
+    return ec
+
+
+def gaussran2(nran, seed):
+    q = C.c_double(seed)
+    out = np.zeros(max(nran, 1))
+    _chk(lib.sdft_gaussran2(nran, C.byref(q), _d(out)))
+    return out[:nran], q.value
+
+
+# ---------------------------------------------------------------------------
+# device context
+# ---------------------------------------------------------------------------
+class Context:
+    """One G sphere / FFT grid on one GPU (sdft_ctx)."""
+
+    def __init__(self, n1, n2, n3, ka, kb, kc, hmat, precision=SDFT_PREC_FP64, max_states=1, device=0):
+        self.n = (int(n1), int(n2), int(n3))
+        self.ka, self.kb, self.kc = _i32(ka), _i32(kb), _i32(kc)
+        self.ncoef = len(self.ka)
+        self.hmat = np.asarray(hmat, dtype=np.float64).reshape(3, 3)
+        h = _f64(self.hmat.T.reshape(9))
+        self.precision = precision
+        self.max_states = int(max_states)
+        p = _vp()
+        _chk(lib.sdft_ctx_create(n1, n2, n3, self.ncoef, _i(self.ka), _i(self.kb), _i(self.kc), _d(h), precision,
+                                 self.max_states, device, C.byref(p)))
+        self._p = p
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib.sdft_ctx_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- setup
+    def set_vks(self, v_filter_layout):
+        v = _f64(v_filter_layout).reshape(-1)
+        assert v.size == self.n[0] * self.n[1] * self.n[2]
+        _chk(lib.sdft_ctx_set_vks(self._p, _d(v)))
+
+    def set_kinetic_cap(self, gcut):
+        _chk(lib.sdft_ctx_set_kinetic_cap(self._p, float(gcut)))
+
+    def set_kb(self, kb):
+        """kb: dict with natm,pos,type,ntype,lmax,lmax_type,nsplin_g,gmin_spl,dg_spl,vps,vpsnorm,gzvps0"""
+        if kb is None or kb["natm"] == 0:
+            _chk(lib.sdft_ctx_set_kb(self._p, None))
+            return
+        self._kb_keep = {k: (_f64(v) if k in ("pos", "vps", "vpsnorm", "gzvps0") else
+                             (_i32(v) if k in ("type", "lmax_type") else v)) for k, v in kb.items()}
+        k = self._kb_keep
+        d = KbDesc(k["natm"], _d(k["pos"]), _i(k["type"]), k["ntype"], k["lmax"], _i(k["lmax_type"]),
+                   k["nsplin_g"], k["gmin_spl"], k["dg_spl"], _d(k["vps"]), _d(k["vpsnorm"]), _d(k["gzvps0"]))
+        _chk(lib.sdft_ctx_set_kb(self._p, C.byref(d)))
+
+    @property
+    def device_bytes(self):
+        return int(lib.sdft_ctx_device_bytes(self._p))
+
+    @property
+    def launches(self):
+        return int(lib.sdft_launch_count(self._p))
+
+    def sync(self):
+        _chk(lib.sdft_sync(self._p))
+
+    def set_timing(self, on=True):
+        _chk(lib.sdft_ctx_set_timing(self._p, 1 if on else 0))
+
+    def read_timing(self):
+        """{kind: (total_ms, launches)} since the last read (synchronises)."""
+        ms = np.zeros(8)
+        n = (C.c_longlong * 8)()
+        _chk(lib.sdft_ctx_read_timing(self._p, _d(ms), n))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_KINDS)}
+
+    def _ns(self, cre):
+        ns = cre.size // self.ncoef
+        assert ns * self.ncoef == cre.size
+        return ns
+
+    # -- hot path (host buffers)
+    def calc_coef_force(self, cre, cim, want_enl=False):
+        cre, cim = _f64(cre), _f64(cim)
+        fr, fi = np.zeros_like(cre), np.zeros_like(cim)
+        e = C.c_double(0.0)
+        _chk(lib.sdft_hpsi(self._p, self._ns(cre), _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e) if want_enl else None))
+        return (fr, fi, e.value) if want_enl else (fr, fi)
+
+    def normHCheby(self, cre, cim, wf1re, wf1im, ipoly, scale, energy_mean, cpy_flag=1):
+        """In place like normHCheby: returns (fcre, fcim); with cpy_flag cre/cim/wf1 rotate."""
+        fr, fi = np.zeros_like(cre), np.zeros_like(cim)
+        _chk(lib.sdft_normh_cheby(self._p, self._ns(cre), ipoly, cpy_flag, scale, energy_mean, _d(cre), _d(cim),
+                                  _d(wf1re) if wf1re is not None else None, _d(wf1im) if wf1im is not None else None,
+                                  _d(fr), _d(fi)))
+        return fr, fi
+
+    def normHNewtonHerm(self, cre, cim, scale, energy_mean, zn):
+        fr, fi = np.zeros_like(cre), np.zeros_like(cim)
+        _chk(lib.sdft_normh_newton(self._p, self._ns(cre), scale, energy_mean, zn, _d(cre), _d(cim), _d(fr), _d(fi)))
+        return fr, fi
+
+    def filterChebyPolyHerm(self, cre, cim, expan_coeff, num_chem_pot, scale, energy_mean, store_moments=False):
+        cre, cim = _f64(cre), _f64(cim)
+        ec = _f64(expan_coeff)
+        L = ec.size // num_chem_pot
+        ns = self._ns(cre)
+        sre = [np.zeros_like(cre) for _ in range(num_chem_pot)]
+        sim = [np.zeros_like(cim) for _ in range(num_chem_pot)]
+        pr = (_dp * num_chem_pot)(*[_d(a) for a in sre])
+        pi = (_dp * num_chem_pot)(*[_d(a) for a in sim])
+        mom = np.zeros(L + 1) if store_moments else None
+        _chk(lib.sdft_filter_cheby(self._p, ns, _d(cre), _d(cim), L, num_chem_pot, _d(ec), scale, energy_mean, pr, pi,
+                                   _d(mom) if mom is not None else None))
+        return (sre, sim, mom) if store_moments else (sre, sim)
+
+    def filterNewtonPolyHerm(self, cre, cim, expan_coeff, samp_point, num_chem_pot, scale, energy_mean):
+        cre, cim = _f64(cre), _f64(cim)
+        ec, sp = _f64(expan_coeff), _f64(samp_point)
+        L = ec.size // num_chem_pot
+        ns = self._ns(cre)
+        sre = [np.zeros_like(cre) for _ in range(num_chem_pot)]
+        sim = [np.zeros_like(cim) for _ in range(num_chem_pot)]
+        pr = (_dp * num_chem_pot)(*[_d(a) for a in sre])
+        pi = (_dp * num_chem_pot)(*[_d(a) for a in sim])
+        _chk(lib.sdft_filter_newton(self._p, ns, _d(cre), _d(cim), L, num_chem_pot, _d(ec), _d(sp), scale,
+                                    energy_mean, pr, pi))
+        return sre, sim
+
+    def calcChebyMoments(self, cre, cim, L, scale, energy_mean):
+        cre, cim = _f64(cre), _f64(cim)
+        m = np.zeros(L + 1)
+        _chk(lib.sdft_cheby_moments(self._p, self._ns(cre), _d(cre), _d(cim), L, scale, energy_mean, _d(m)))
+        return m
+
+    def rhoCalcRealStoHybrid(self, cre, cim):
+        """sum_s |psi_s(r)|^2 in package layout (a fastest), unscaled."""
+        cre, cim = _f64(cre), _f64(cim)
+        rho = np.zeros(self.n[0] * self.n[1] * self.n[2])
+        _chk(lib.sdft_density(self._p, self._ns(cre), _d(cre), _d(cim), _d(rho)))
+        return rho
+
+    def genNoiseOrbitalReal(self, nstate, seed=10.0, np_states=1, myid=0):
+        cre = np.zeros(nstate * self.ncoef)
+        cim = np.zeros(nstate * self.ncoef)
+        _chk(lib.sdft_noise_real(self._p, nstate, seed, np_states, myid, _d(cre), _d(cim)))
+        return cre, cim
+
+    # -- hot path (device resident)
+    def upload(self, cre, cim):
+        cre, cim = _f64(cre), _f64(cim)
+        _chk(lib.sdft_upload_orbitals(self._p, self._ns(cre), _d(cre), _d(cim)))
+
+    def noise_dev(self, nstate, seed=10.0, np_states=1, myid=0):
+        _chk(lib.sdft_noise_real_dev(self._p, nstate, seed, np_states, myid))
+
+    def filter_cheby_dev(self, nstate, expan_coeff, num_chem_pot, scale, energy_mean):
+        ec = _f64(expan_coeff)
+        _chk(lib.sdft_filter_cheby_dev(self._p, nstate, ec.size // num_chem_pot, num_chem_pot, _d(ec), scale,
+                                       energy_mean))
+
+    def filter_newton_dev(self, nstate, expan_coeff, samp_point, num_chem_pot, scale, energy_mean):
+        ec, sp = _f64(expan_coeff), _f64(samp_point)
+        _chk(lib.sdft_filter_newton_dev(self._p, nstate, ec.size // num_chem_pot, num_chem_pot, _d(ec), _d(sp), scale,
+                                        energy_mean))
+
+    def moments_dev(self, nstate, L, scale, energy_mean):
+        m = np.zeros(L + 1)
+        _chk(lib.sdft_cheby_moments_dev(self._p, nstate, L, scale, energy_mean, _d(m)))
+        return m
+
+    def density_dev(self, nstate, imu=0, scale=1.0, want=True):
+        rho = np.zeros(self.n[0] * self.n[1] * self.n[2]) if want else None
+        _chk(lib.sdft_density_dev(self._p, nstate, imu, scale, _d(rho) if want else None))
+        return rho
+
+    def download_filtered(self, nstate, imu=0):
+        re = np.zeros(nstate * self.ncoef)
+        im = np.zeros(nstate * self.ncoef)
+        _chk(lib.sdft_download_filtered(self._p, nstate, imu, _d(re), _d(im)))
+        return re, im

@@ -1,0 +1,858 @@
+// sdft_api.cu -- device context and C ABI of the B200 stochastic-DFT filter
+// hot path.  Host buffers follow PINY's layout (state-major, half sphere,
+// G=0 last, separate re/im arrays); device buffers hold one orbital as
+// [re block | im block], each block padded to ngp doubles.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <mutex>
+#include <algorithm>
+#include "sdft_internal.h"
+#include "sdft_kernels.cuh"
+#include "sdft_ctx.h"
+
+namespace sdft {
+
+static thread_local std::string g_err;
+int set_error(int code, const char *msg) {
+  g_err = msg ? msg : "";
+  return code;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e__ = (call);                                                      \
+    if (e__ != cudaSuccess) {                                                      \
+      char b__[512];                                                               \
+      snprintf(b__, sizeof b__, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e__), \
+               __FILE__, __LINE__);                                                \
+      return set_error(e__ == cudaErrorMemoryAllocation ? SDFT_ERR_NOMEM : SDFT_ERR_CUDA, b__); \
+    }                                                                              \
+  } while (0)
+
+static bool edge_ok(int n) {
+  if (n < 2 || n > kMaxEdge) return false;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+static inline size_t rup(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+template <typename T> size_t plane_smem(const DevGeom &g);
+
+}  // namespace sdft
+
+using namespace sdft;
+
+
+namespace sdft {
+int dmalloc(sdft_ctx *c, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    char b[256];
+    snprintf(b, sizeof b, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    return set_error(SDFT_ERR_NOMEM, b);
+  }
+  c->dev_bytes += (long long)bytes;
+  return SDFT_OK;
+}
+#define DM(ptr, bytes)                                                   \
+  do {                                                                   \
+    int r__ = dmalloc(ctx, (void **)&(ptr), (bytes));                    \
+    if (r__) return r__;                                                 \
+  } while (0)
+
+// Build the column decomposition from the PINY-ordered half sphere.
+static int build_columns(sdft_ctx *ctx, std::vector<int> &cp_gstart, std::vector<int> &cp_gcount,
+                         std::vector<int> &col_ab) {
+  const int nk = ctx->ncoef - 1;
+  const int *ka = ctx->ka.data(), *kb = ctx->kb.data(), *kc = ctx->kc.data();
+  int zs = -1, zc = 0, kamax = 0;
+  for (int i = 0; i < nk; i++) {
+    if (std::abs(ka[i]) * 2 + 1 > ctx->n1 || std::abs(kb[i]) * 2 + 1 > ctx->n2 ||
+        std::abs(kc[i]) * 2 + 1 > ctx->n3)
+      return set_error(SDFT_ERR_UNSUPPORTED, "G sphere does not fit the FFT grid (|k| >= n/2)");
+    kamax = std::max(kamax, std::abs(ka[i]));
+    const bool half = ka[i] > 0 || (ka[i] == 0 && kb[i] > 0) || (ka[i] == 0 && kb[i] == 0 && kc[i] > 0);
+    if (!half) return set_error(SDFT_ERR_ARG, "G list is not a half sphere (ka,kb,kc) > 0");
+  }
+  if (ctx->ka[nk] != 0 || ctx->kb[nk] != 0 || ctx->kc[nk] != 0)
+    return set_error(SDFT_ERR_ARG, "G=0 must be stored last");
+  int i = 0;
+  while (i < nk) {
+    int j = i;
+    while (j < nk && ka[j] == ka[i] && kb[j] == kb[i]) j++;
+    if (ka[i] == 0 && kb[i] == 0) {
+      if (zs >= 0) return set_error(SDFT_ERR_ARG, "(0,0) column not contiguous");
+      zs = i;
+      zc = j - i;
+    } else {
+      cp_gstart.push_back(i);
+      cp_gcount.push_back(j - i);
+      auto w = [](int k, int n) { return k < 0 ? k + n : k; };
+      col_ab.push_back((w(ka[i], ctx->n1) << 16) | w(kb[i], ctx->n2));
+      col_ab.push_back((w(-ka[i], ctx->n1) << 16) | w(-kb[i], ctx->n2));
+    }
+    i = j;
+  }
+  // duplicate columns would mean the list is not grouped by (ka,kb)
+  {
+    std::vector<int> chk(col_ab);
+    std::sort(chk.begin(), chk.end());
+    if (std::adjacent_find(chk.begin(), chk.end()) != chk.end())
+      return set_error(SDFT_ERR_ARG, "G list not grouped by (ka,kb) columns");
+  }
+  cp_gstart.push_back(zs < 0 ? 0 : zs);
+  cp_gcount.push_back(zc);
+  col_ab.push_back(0);
+  ctx->cols.ncp = (int)cp_gstart.size();
+  ctx->cols.ncols = (int)col_ab.size();
+  ctx->cols.ncols_pad = (int)rup(ctx->cols.ncols, 4);
+  ctx->cols.kamax = kamax;
+  return SDFT_OK;
+}
+
+static int ensure_x(sdft_ctx *ctx, int npairs) {
+  const size_t csz = ctx->prec == SDFT_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t need = (size_t)npairs * ctx->n3 * ctx->cols.ncols_pad * csz;
+  if (need <= ctx->x_bytes) return SDFT_OK;
+  if (ctx->d_x) { cudaFree(ctx->d_x); ctx->dev_bytes -= (long long)ctx->x_bytes; ctx->d_x = nullptr; }
+  DM(ctx->d_x, need);
+  ctx->x_bytes = need;
+  return SDFT_OK;
+}
+
+static int ensure_coef(sdft_ctx *ctx, size_t n) {
+  if (n <= ctx->coef_cap) return SDFT_OK;
+  if (ctx->d_coef) { cudaFree(ctx->d_coef); ctx->dev_bytes -= (long long)(ctx->coef_cap * 8); }
+  DM(ctx->d_coef, n * sizeof(double));
+  ctx->coef_cap = n;
+  return SDFT_OK;
+}
+
+static int ensure_acc(sdft_ctx *ctx, int nmu) {
+  if (nmu <= ctx->acc_nmu) return SDFT_OK;
+  if (ctx->d_acc) { cudaFree(ctx->d_acc); ctx->dev_bytes -= (long long)(ctx->acc_nmu * ctx->vec_elems * 8); }
+  DM(ctx->d_acc, (size_t)nmu * ctx->vec_elems * sizeof(double));
+  CK(cudaMemsetAsync(ctx->d_acc, 0, (size_t)nmu * ctx->vec_elems * sizeof(double), ctx->st));
+  ctx->acc_nmu = nmu;
+  return SDFT_OK;
+}
+
+static int ensure_mom(sdft_ctx *ctx, size_t n) {
+  if (n <= ctx->mom_cap) return SDFT_OK;
+  if (ctx->d_mom) { cudaFree(ctx->d_mom); ctx->dev_bytes -= (long long)(ctx->mom_cap * 8); }
+  DM(ctx->d_mom, n * sizeof(double));
+  ctx->mom_cap = n;
+  return SDFT_OK;
+}
+
+// Host <-> device orbital block copies (PINY layout <-> [s][re|im][ngp]).
+static int upload_block(sdft_ctx *ctx, double *dst, int nstate, const double *re, const double *im) {
+  const size_t w = (size_t)ctx->ncoef * sizeof(double);
+  const size_t dp = (size_t)2 * ctx->ngp * sizeof(double);
+  CK(cudaMemcpy2DAsync(dst, dp, re, w, w, nstate, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpy2DAsync(dst + ctx->ngp, dp, im, w, w, nstate, cudaMemcpyHostToDevice, ctx->st));
+  return SDFT_OK;
+}
+static int download_block(sdft_ctx *ctx, const double *src, int nstate, double *re, double *im) {
+  const size_t w = (size_t)ctx->ncoef * sizeof(double);
+  const size_t sp = (size_t)2 * ctx->ngp * sizeof(double);
+  CK(cudaMemcpy2DAsync(re, w, src, sp, w, nstate, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpy2DAsync(im, w, src + ctx->ngp, sp, w, nstate, cudaMemcpyDeviceToHost, ctx->st));
+  return SDFT_OK;
+}
+
+static bool is_fp64(const sdft_ctx *c) { return c->prec == SDFT_PREC_FP64; }
+
+// Nonlocal projection Z = Pj C and back projection FNL = Bk Z for `nstate`
+// orbitals held in `vec`.
+static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
+  if (ctx->P == 0) return SDFT_OK;
+  const int spad = (int)rup(nstate, 64);
+  const int K1 = 2 * ctx->ngp;
+  // split K of the projection so that >= ~2 waves of CTAs exist
+  const int tiles = (ctx->Ppad / 128) * (spad / 64);
+  int split = 1;
+  while (tiles * split < 2 * 148 && split < 64 && (K1 / 16) / (split * 2) >= 8 &&
+         (size_t)(split * 2) * spad * ctx->Ppad <= ctx->zwork_elems)
+    split *= 2;
+  {
+    TScope ts(ctx, 3);
+    launch_gemm_nt_f64(ctx->d_pj, K1, vec, K1, ctx->d_z, ctx->Ppad, ctx->Ppad, spad, K1, ctx->P, nstate,
+                       split, ctx->d_zwork, ctx->st);
+  }
+  ctx->launches += split > 1 ? 2 : 1;
+  if (want_enl) {
+    launch_enl(ctx->d_z, ctx->Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
+    ctx->launches++;
+  }
+  {
+    TScope ts(ctx, 4);
+    launch_gemm_nt_f64(ctx->d_bk, ctx->Ppad, ctx->d_z, ctx->Ppad, ctx->d_fnl, K1, ctx->Mpad2, spad,
+                       ctx->Ppad, K1, nstate, 1, nullptr, ctx->st);
+  }
+  ctx->launches++;
+  return SDFT_OK;
+}
+
+// One application of the fused H pipeline on `cur` with epilogue `e`.
+static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool want_enl) {
+  int r = run_kb(ctx, cur, nstate, want_enl);
+  if (r) return r;
+  const int npairs = (nstate + 1) / 2;
+  if ((r = ensure_x(ctx, npairs))) return r;
+  e.nstate = nstate;
+  e.pair0 = 0;
+  e.C = cur;
+  e.FNL = ctx->P ? ctx->d_fnl : nullptr;
+  e.invN = 1.0 / (double)ctx->N;
+  if (is_fp64(ctx)) {
+    { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 1); launch_stage_b<double>(ctx->g, ctx->d_x, (const double *)ctx->d_vp, npairs, ctx->st); }
+    { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+  } else {
+    { TScope ts(ctx, 0); launch_stage_a<float>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 1); launch_stage_b<float>(ctx->g, ctx->d_x, (const float *)ctx->d_vp, npairs, ctx->st); }
+    { TScope ts(ctx, 2); launch_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+  }
+  ctx->launches += 3;
+  CK(cudaGetLastError());
+  return SDFT_OK;
+}
+
+static int check_ready(sdft_ctx *ctx, int nstate) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->max_states) return set_error(SDFT_ERR_ARG, "nstate out of range (1..max_states)");
+  if (!ctx->have_v) return set_error(SDFT_ERR_STATE, "V_KS not set (sdft_ctx_set_vks)");
+  return SDFT_OK;
+}
+
+static EpiArgs base_epi(sdft_ctx *ctx) {
+  EpiArgs e{};
+  e.acc_stride = ctx->vec_elems;
+  e.nmu = 0;
+  e.ndots = 0;
+  return e;
+}
+
+// Chebyshev filter on resident chi (d_chi) -> d_acc.  moments (device, may
+// be null): per step dots written to d_mom[k*3 .. k*3+2].
+static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double scale, double emean,
+                             bool store_moments) {
+  int r;
+  if ((r = ensure_acc(ctx, nmu))) return r;
+  const double prefact = -scale * emean, s1 = -scale * 0.25, s2 = -scale * 0.5;
+  double *cur = ctx->d_chi, *prev = nullptr;
+  double *bufs[2] = {ctx->d_b1, ctx->d_b2};
+  const int nparts = ((nstate + 1) / 2) * ctx->g.nbatch;
+  for (int k = 1; k < L; k++) {
+    EpiArgs e = base_epi(ctx);
+    double *out = (k == 1) ? bufs[0] : (k == 2 ? bufs[1] : prev);
+    e.OUT = out;
+    e.ACC = ctx->d_acc;
+    e.nmu = nmu;
+    e.acoef = ctx->d_coef + (size_t)k * nmu;
+    e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
+    e.CHI = ctx->d_chi;
+    if (k == 1) {
+      e.mode = EPI_CHEB1;
+      e.s1 = s1; e.s2 = s2; e.pre = prefact;
+    } else {
+      e.mode = EPI_CHEBK;
+      e.s1 = 2.0 * s1; e.s2 = 2.0 * s2; e.pre = 2.0 * prefact;
+      e.PREV = prev;
+    }
+    if (store_moments) {
+      e.dots = ctx->d_dots;
+      e.ndots = (k == 1) ? 2 : 1;
+    }
+    if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
+    if (store_moments) {
+      launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_mom + (size_t)k * 3, ctx->st);
+      ctx->launches++;
+    }
+    prev = cur;
+    cur = out;
+  }
+  return SDFT_OK;
+}
+
+static int filter_newton_core(sdft_ctx *ctx, int nstate, int L, int nmu, const double *samp, double scale,
+                              double emean) {
+  int r;
+  if ((r = ensure_acc(ctx, nmu))) return r;
+  const double s1 = -scale * 0.25, s2 = -scale * 0.5;
+  double *cur = ctx->d_chi;
+  for (int k = 1; k < L; k++) {
+    EpiArgs e = base_epi(ctx);
+    e.mode = EPI_NEWTON;
+    e.OUT = ctx->d_b1;  // k==1 writes B1, then in place
+    e.ACC = ctx->d_acc;
+    e.nmu = nmu;
+    e.acoef = ctx->d_coef + (size_t)k * nmu;
+    e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
+    e.s1 = s1; e.s2 = s2;
+    e.pre = -scale * emean - samp[k - 1];
+    if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
+    cur = ctx->d_b1;
+  }
+  return SDFT_OK;
+}
+
+// Moments by the doubling identities (calcChebyMoments).
+static int moments_core(sdft_ctx *ctx, int nstate, int L, double scale, double emean, double *mom_host) {
+  int r;
+  const int M = (L % 2 == 0) ? (L / 2 + 1) : ((L + 1) / 2);
+  if ((r = ensure_mom(ctx, (size_t)(M + 1) * 3))) return r;
+  const double prefact = -scale * emean, s1 = -scale * 0.25, s2 = -scale * 0.5;
+  const int nparts = ((nstate + 1) / 2) * ctx->g.nbatch;
+  double *cur = ctx->d_chi, *prev = nullptr;
+  double *bufs[2] = {ctx->d_b1, ctx->d_b2};
+  for (int k = 1; k < std::max(M, 2); k++) {
+    EpiArgs e = base_epi(ctx);
+    double *out = (k == 1) ? bufs[0] : (k == 2 ? bufs[1] : prev);
+    e.OUT = out;
+    e.CHI = ctx->d_chi;
+    e.dots = ctx->d_dots;
+    if (k == 1) {
+      e.mode = EPI_CHEB1;
+      e.ndots = 2;
+      e.s1 = s1; e.s2 = s2; e.pre = prefact;
+    } else {
+      e.mode = EPI_MOMK;
+      e.ndots = 3;
+      e.s1 = 2.0 * s1; e.s2 = 2.0 * s2; e.pre = 2.0 * prefact;
+      e.PREV = prev;
+    }
+    if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
+    launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_mom + (size_t)k * 3, ctx->st);
+    ctx->launches++;
+    prev = cur;
+    cur = out;
+  }
+  std::vector<double> h((size_t)(M + 1) * 3);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_mom, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  // assemble in the order calcChebyMoments writes (later writes win)
+  for (int i = 0; i <= L; i++) mom_host[i] = 0.0;
+  mom_host[0] = h[1 * 3 + 1];  // <chi,chi> from step 1
+  mom_host[1] = h[1 * 3 + 0];
+  for (int k = 2; k < M; k++) {
+    mom_host[k] = h[k * 3 + 0];
+    mom_host[2 * k - 1] = 2.0 * h[k * 3 + 1] - mom_host[1];
+    mom_host[2 * k] = 2.0 * h[k * 3 + 2] - mom_host[0];
+    // calcChebyMoments zeroes [k], [2k], [2k-1] at the start of step k and
+    // then writes all three; step k' > k overwrites [k'] with the direct dot.
+  }
+  // direct dots of steps k' overwrite doubled values written earlier
+  for (int k = 2; k < M; k++) mom_host[k] = h[k * 3 + 0];
+  return SDFT_OK;
+}
+
+}  // namespace sdft
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" const char *sdft_last_error(void) { return g_err.c_str(); }
+extern "C" int sdft_version(void) { return 10000; }
+
+extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka, const int *kb,
+                               const int *kc, const double *hmat, int precision, int max_states,
+                               int device, sdft_ctx **out) {
+  if (!out || !ka || !kb || !kc || !hmat) return set_error(SDFT_ERR_ARG, "ctx_create: null argument");
+  *out = nullptr;
+  if (!edge_ok(n1) || !edge_ok(n2) || !edge_ok(n3))
+    return set_error(SDFT_ERR_UNSUPPORTED, "FFT edges must be 2^a 3^b in [2,128]");
+  if (ncoef < 2 || max_states < 1) return set_error(SDFT_ERR_ARG, "ctx_create: ncoef/max_states");
+  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED)
+    return set_error(SDFT_ERR_ARG, "ctx_create: precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(SDFT_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return set_error(SDFT_ERR_ARG, "ctx_create: device index");
+  sdft_ctx *ctx = new sdft_ctx();
+  auto fail = [&](int code) { sdft_ctx_destroy(ctx); return code; };
+  ctx->device = device;
+  ctx->prec = precision;
+  ctx->n1 = n1; ctx->n2 = n2; ctx->n3 = n3;
+  ctx->N = n1 * n2 * n3;
+  ctx->ncoef = ncoef;
+  ctx->ngp = (int)rup(ncoef, 16);
+  std::memcpy(ctx->hmat, hmat, sizeof(double) * 9);
+  ctx->vol = cell_volume(hmat);
+  ctx->ka.assign(ka, ka + ncoef);
+  ctx->kb.assign(kb, kb + ncoef);
+  ctx->kc.assign(kc, kc + ncoef);
+  ctx->max_states = max_states;
+  ctx->s_pad = (int)rup(max_states, 64);
+  ctx->npairs_max = (max_states + 1) / 2;
+  ctx->vec_elems = (size_t)ctx->s_pad * 2 * ctx->ngp;
+  if (cudaSetDevice(device) != cudaSuccess) return fail(set_error(SDFT_ERR_CUDA, "cudaSetDevice failed"));
+  if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(set_error(SDFT_ERR_CUDA, "stream create failed"));
+  std::vector<int> cpg, cpc, colab;
+  int r = build_columns(ctx, cpg, cpc, colab);
+  if (r) return fail(r);
+  // shared-memory budget of the plane stage
+  {
+    DevGeom t{};
+    t.n1 = n1; t.n2 = n2; t.n3 = n3;
+    size_t need = is_fp64(ctx) ? plane_smem<double>(t) : plane_smem<float>(t);
+    if (need > 227 * 1024) return fail(set_error(SDFT_ERR_UNSUPPORTED, "plane does not fit shared memory"));
+    if (n1 * n2 > 512 * 24) return fail(set_error(SDFT_ERR_UNSUPPORTED, "plane too large"));
+  }
+  std::vector<int> gkc(ncoef);
+  for (int i = 0; i < ncoef; i++) gkc[i] = kc[i];
+  std::vector<double> ak2(ncoef);
+  sdft_ak2_kinetic(hmat, ncoef, ka, kb, kc, 0.0, ak2.data());
+  std::vector<double2> tw(n1 + n2 + n3);
+  std::vector<float2> twf(n1 + n2 + n3);
+  int off = 0;
+  for (int n : {n1, n2, n3}) {
+    for (int t = 0; t < n; t++) {
+      double a = 2.0 * M_PI * (double)t / (double)n;
+      tw[off + t] = make_double2(std::cos(a), -std::sin(a));
+      twf[off + t] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    off += n;
+  }
+#define DMF(ptr, bytes) do { int r__ = dmalloc(ctx, (void **)&(ptr), (bytes)); if (r__) return fail(r__); } while (0)
+#define CKF(call) do { cudaError_t e__ = (call); if (e__ != cudaSuccess) return fail(set_error(SDFT_ERR_CUDA, cudaGetErrorString(e__))); } while (0)
+  DMF(ctx->d_cp_gstart, cpg.size() * sizeof(int));
+  DMF(ctx->d_cp_gcount, cpc.size() * sizeof(int));
+  DMF(ctx->d_col_ab, colab.size() * sizeof(int));
+  DMF(ctx->d_gkc, ncoef * sizeof(int));
+  DMF(ctx->d_ak2, ncoef * sizeof(double));
+  DMF(ctx->d_tw, tw.size() * sizeof(double2));
+  DMF(ctx->d_twf, twf.size() * sizeof(float2));
+  CKF(cudaMemcpy(ctx->d_cp_gstart, cpg.data(), cpg.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_cp_gcount, cpc.data(), cpc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_col_ab, colab.data(), colab.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_gkc, gkc.data(), ncoef * sizeof(int), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_ak2, ak2.data(), ncoef * sizeof(double), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(ctx->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  DevGeom &g = ctx->g;
+  g.n1 = n1; g.n2 = n2; g.n3 = n3; g.N = ctx->N;
+  g.ncoef = ncoef; g.ngp = ctx->ngp;
+  g.ncols = ctx->cols.ncols; g.ncols_pad = ctx->cols.ncols_pad; g.ncp = ctx->cols.ncp; g.kamax = ctx->cols.kamax;
+  g.nbatch = (g.ncp + kCPB - 1) / kCPB;
+  g.cp_gstart = ctx->d_cp_gstart; g.cp_gcount = ctx->d_cp_gcount; g.col_ab = ctx->d_col_ab;
+  g.gkc = ctx->d_gkc; g.ak2 = ctx->d_ak2;
+  g.tw1 = ctx->d_tw; g.tw2 = ctx->d_tw + n1; g.tw3 = ctx->d_tw + n1 + n2;
+  g.tw1f = ctx->d_twf; g.tw2f = ctx->d_twf + n1; g.tw3f = ctx->d_twf + n1 + n2;
+  // orbital blocks (zero padded)
+  const size_t vb = ctx->vec_elems * sizeof(double);
+  DMF(ctx->d_chi, vb);
+  DMF(ctx->d_b1, vb);
+  DMF(ctx->d_b2, vb);
+  CKF(cudaMemset(ctx->d_chi, 0, vb));
+  CKF(cudaMemset(ctx->d_b1, 0, vb));
+  CKF(cudaMemset(ctx->d_b2, 0, vb));
+  DMF(ctx->d_dots, (size_t)ctx->npairs_max * g.nbatch * 3 * sizeof(double));
+  DMF(ctx->d_enl, sizeof(double));
+  const size_t vsz = is_fp64(ctx) ? sizeof(double) : sizeof(float);
+  DMF(ctx->d_vp, (size_t)ctx->N * vsz);
+  DMF(ctx->d_vks_tmp, (size_t)ctx->N * sizeof(double));
+#undef DMF
+#undef CKF
+  *out = ctx;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
+  if (!ctx) return SDFT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  void *ptrs[] = {ctx->d_cp_gstart, ctx->d_cp_gcount, ctx->d_col_ab, ctx->d_gkc, ctx->d_ak2, ctx->d_tw,
+                  ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
+                  ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
+                  ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_enl};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto &t : ctx->tev_pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+  for (auto e : ctx->tev_free) cudaEventDestroy(e);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_set_kinetic_cap(sdft_ctx *ctx, double gcut) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  ctx->gcut = gcut;
+  std::vector<double> ak2(ctx->ncoef);
+  sdft_ak2_kinetic(ctx->hmat, ctx->ncoef, ctx->ka.data(), ctx->kb.data(), ctx->kc.data(), gcut, ak2.data());
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpy(ctx->d_ak2, ak2.data(), ctx->ncoef * sizeof(double), cudaMemcpyHostToDevice));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_set_vks(sdft_ctx *ctx, const double *v) {
+  if (!ctx || !v) return set_error(SDFT_ERR_ARG, "set_vks: null");
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(ctx->d_vks_tmp, v, (size_t)ctx->N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  if (is_fp64(ctx))
+    launch_vks_transpose<double>(ctx->d_vks_tmp, (double *)ctx->d_vp, ctx->n1, ctx->n2, ctx->n3, ctx->st);
+  else
+    launch_vks_transpose<float>(ctx->d_vks_tmp, (float *)ctx->d_vp, ctx->n1, ctx->n2, ctx->n3, ctx->st);
+  ctx->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->have_v = true;
+  return SDFT_OK;
+}
+
+extern "C" long long sdft_ctx_device_bytes(const sdft_ctx *ctx) { return ctx ? ctx->dev_bytes : 0; }
+extern "C" void *sdft_ctx_stream(sdft_ctx *ctx) { return ctx ? (void *)ctx->st : nullptr; }
+extern "C" long long sdft_launch_count(const sdft_ctx *ctx) { return ctx ? ctx->launches : 0; }
+extern "C" int sdft_ctx_set_timing(sdft_ctx *ctx, int enable) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  ctx->timing = enable != 0;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->st));
+  for (auto &t : ctx->tev_pending) {
+    float f = 0.f;
+    if (cudaEventElapsedTime(&f, t.a, t.b) == cudaSuccess) {
+      ctx->t_ms[t.kind] += f;
+      ctx->t_n[t.kind] += 1;
+    }
+    ctx->tev_free.push_back(t.a);
+    ctx->tev_free.push_back(t.b);
+  }
+  ctx->tev_pending.clear();
+  for (int k = 0; k < SDFT_NKIND; k++) {
+    if (ms) ms[k] = ctx->t_ms[k];
+    if (count) count[k] = ctx->t_n[k];
+    ctx->t_ms[k] = 0.0;
+    ctx->t_n[k] = 0;
+  }
+  return SDFT_OK;
+}
+
+extern "C" int sdft_sync(sdft_ctx *ctx) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaGetLastError());
+  return SDFT_OK;
+}
+
+// ---- KB projectors -------------------------------------------------------
+int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb);  // sdft_kb.cu
+
+extern "C" int sdft_ctx_set_kb(sdft_ctx *ctx, const sdft_kb_desc *kb) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  cudaSetDevice(ctx->device);
+  return sdft_build_kb_device(ctx, kb);
+}
+
+// ---- hot path ---------------------------------------------------------------
+extern "C" int sdft_upload_orbitals(sdft_ctx *ctx, int nstate, const double *cre, const double *cim) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim) return set_error(SDFT_ERR_ARG, "upload: null");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  ctx->resident = nstate;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_hpsi(sdft_ctx *ctx, int nstate, const double *cre, const double *cim, double *fcre,
+                         double *fcim, double *enl) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim || !fcre || !fcim) return set_error(SDFT_ERR_ARG, "hpsi: null");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  ctx->resident = nstate;
+  EpiArgs e = base_epi(ctx);
+  e.mode = EPI_HPSI;
+  e.OUT = ctx->d_b1;
+  if ((r = apply_h(ctx, ctx->d_chi, nstate, e, enl != nullptr))) return r;
+  if ((r = download_block(ctx, ctx->d_b1, nstate, fcre, fcim))) return r;
+  if (enl) {
+    if (ctx->P) CK(cudaMemcpyAsync(enl, ctx->d_enl, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    else *enl = 0.0;
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_normh_cheby(sdft_ctx *ctx, int nstate, int ipoly, int cpy_flag, double scale,
+                                double emean, double *cre, double *cim, double *wf1re, double *wf1im,
+                                double *fcre, double *fcim) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (ipoly < 1 || !cre || !cim || !fcre || !fcim || (ipoly > 1 && (!wf1re || !wf1im)))
+    return set_error(SDFT_ERR_ARG, "normh_cheby: bad argument");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  EpiArgs e = base_epi(ctx);
+  const double prefact = -scale * emean, s1 = -scale * 0.25, s2 = -scale * 0.5;
+  e.OUT = ctx->d_b2;
+  if (ipoly == 1) {
+    e.mode = EPI_CHEB1; e.s1 = s1; e.s2 = s2; e.pre = prefact;
+  } else {
+    if ((r = upload_block(ctx, ctx->d_b1, nstate, wf1re, wf1im))) return r;
+    e.mode = EPI_CHEBK; e.s1 = 2 * s1; e.s2 = 2 * s2; e.pre = 2 * prefact; e.PREV = ctx->d_b1;
+  }
+  if ((r = apply_h(ctx, ctx->d_chi, nstate, e, false))) return r;
+  if ((r = download_block(ctx, ctx->d_b2, nstate, fcre, fcim))) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  if (cpy_flag) {
+    const size_t n = (size_t)nstate * ctx->ncoef * sizeof(double);
+    if (ipoly > 1) { std::memcpy(wf1re, cre, n); std::memcpy(wf1im, cim, n); }
+    std::memcpy(cre, fcre, n);
+    std::memcpy(cim, fcim, n);
+  }
+  return SDFT_OK;
+}
+
+extern "C" int sdft_normh_newton(sdft_ctx *ctx, int nstate, double scale, double emean, double zn,
+                                 double *cre, double *cim, double *fcre, double *fcim) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim || !fcre || !fcim) return set_error(SDFT_ERR_ARG, "normh_newton: null");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  EpiArgs e = base_epi(ctx);
+  e.mode = EPI_NEWTON;
+  e.OUT = ctx->d_b1;
+  e.s1 = -scale * 0.25; e.s2 = -scale * 0.5; e.pre = -scale * emean - zn;
+  if ((r = apply_h(ctx, ctx->d_chi, nstate, e, false))) return r;
+  if ((r = download_block(ctx, ctx->d_b1, nstate, fcre, fcim))) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  const size_t n = (size_t)nstate * ctx->ncoef * sizeof(double);
+  std::memcpy(cre, fcre, n);  // normHNewtonHerm copies the force back
+  std::memcpy(cim, fcim, n);
+  return SDFT_OK;
+}
+
+static int upload_coef(sdft_ctx *ctx, const double *ec, size_t n) {
+  int r = ensure_coef(ctx, n);
+  if (r) return r;
+  CK(cudaMemcpyAsync(ctx->d_coef, ec, n * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_filter_cheby_dev(sdft_ctx *ctx, int nstate, int L, int nmu, const double *ec,
+                                     double scale, double emean) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (L < 2 || nmu < 1 || !ec) return set_error(SDFT_ERR_ARG, "filter_cheby: L >= 2, numChemPot >= 1");
+  if (nstate > ctx->resident) return set_error(SDFT_ERR_STATE, "filter: orbitals not resident");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_coef(ctx, ec, (size_t)L * nmu))) return r;
+  if ((r = filter_cheby_core(ctx, nstate, L, nmu, scale, emean, false))) return r;
+  ctx->filtered = nstate;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_filter_newton_dev(sdft_ctx *ctx, int nstate, int L, int nmu, const double *ec,
+                                      const double *samp, double scale, double emean) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (L < 2 || nmu < 1 || !ec || !samp) return set_error(SDFT_ERR_ARG, "filter_newton: bad argument");
+  if (nstate > ctx->resident) return set_error(SDFT_ERR_STATE, "filter: orbitals not resident");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_coef(ctx, ec, (size_t)L * nmu))) return r;
+  if ((r = filter_newton_core(ctx, nstate, L, nmu, samp, scale, emean))) return r;
+  ctx->filtered = nstate;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_download_filtered(sdft_ctx *ctx, int nstate, int imu, double *re, double *im) {
+  if (!ctx || !re || !im) return set_error(SDFT_ERR_ARG, "download: null");
+  if (nstate < 1 || nstate > ctx->filtered || imu < 0 || imu >= ctx->acc_nmu)
+    return set_error(SDFT_ERR_STATE, "download: no filtered orbitals");
+  cudaSetDevice(ctx->device);
+  int r = download_block(ctx, ctx->d_acc + (size_t)imu * ctx->vec_elems, nstate, re, im);
+  if (r) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_filter_cheby(sdft_ctx *ctx, int nstate, const double *cre, const double *cim, int L,
+                                 int nmu, const double *ec, double scale, double emean, double **sre,
+                                 double **sim, double *moments) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim || !ec || !sre || !sim || L < 2 || nmu < 1) return set_error(SDFT_ERR_ARG, "filter_cheby: bad argument");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  ctx->resident = nstate;
+  if ((r = upload_coef(ctx, ec, (size_t)L * nmu))) return r;
+  if (moments && (r = ensure_mom(ctx, (size_t)L * 3))) return r;
+  if ((r = filter_cheby_core(ctx, nstate, L, nmu, scale, emean, moments != nullptr))) return r;
+  ctx->filtered = nstate;
+  for (int imu = 0; imu < nmu; imu++)
+    if ((r = download_block(ctx, ctx->d_acc + (size_t)imu * ctx->vec_elems, nstate, sre[imu], sim[imu]))) return r;
+  if (moments) {
+    std::vector<double> h((size_t)L * 3);
+    CK(cudaMemcpyAsync(h.data(), ctx->d_mom, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    moments[0] = h[1 * 3 + 1];
+    for (int k = 1; k < L; k++) moments[k] = h[k * 3 + 0];
+    moments[L] = 0.0;
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_filter_newton(sdft_ctx *ctx, int nstate, const double *cre, const double *cim, int L,
+                                  int nmu, const double *ec, const double *samp, double scale, double emean,
+                                  double **sre, double **sim) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim || !ec || !samp || !sre || !sim || L < 2 || nmu < 1)
+    return set_error(SDFT_ERR_ARG, "filter_newton: bad argument");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  ctx->resident = nstate;
+  if ((r = upload_coef(ctx, ec, (size_t)L * nmu))) return r;
+  if ((r = filter_newton_core(ctx, nstate, L, nmu, samp, scale, emean))) return r;
+  ctx->filtered = nstate;
+  for (int imu = 0; imu < nmu; imu++)
+    if ((r = download_block(ctx, ctx->d_acc + (size_t)imu * ctx->vec_elems, nstate, sre[imu], sim[imu]))) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_cheby_moments_dev(sdft_ctx *ctx, int nstate, int L, double scale, double emean,
+                                      double *moments) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (L < 2 || !moments) return set_error(SDFT_ERR_ARG, "moments: bad argument");
+  if (nstate > ctx->resident) return set_error(SDFT_ERR_STATE, "moments: orbitals not resident");
+  cudaSetDevice(ctx->device);
+  return moments_core(ctx, nstate, L, scale, emean, moments);
+}
+
+extern "C" int sdft_cheby_moments(sdft_ctx *ctx, int nstate, const double *cre, const double *cim, int L,
+                                  double scale, double emean, double *moments) {
+  int r = check_ready(ctx, nstate);
+  if (r) return r;
+  if (!cre || !cim || !moments || L < 2) return set_error(SDFT_ERR_ARG, "moments: bad argument");
+  cudaSetDevice(ctx->device);
+  if ((r = upload_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  ctx->resident = nstate;
+  return moments_core(ctx, nstate, L, scale, emean, moments);
+}
+
+// Density of the orbitals held in `vec`.
+static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double scale) {
+  int r;
+  const int npairs = (nstate + 1) / 2;
+  if ((r = ensure_x(ctx, npairs))) return r;
+  const int nsplit = npairs;  // one |psi|^2 plane set per pair, summed in pair order
+  if (nsplit > ctx->rho_split) {
+    if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
+    DM(ctx->d_rho_part, (size_t)nsplit * ctx->N * sizeof(double));
+    ctx->rho_split = nsplit;
+  }
+  if (!ctx->d_rho) DM(ctx->d_rho, (size_t)ctx->N * sizeof(double));
+  if (is_fp64(ctx)) {
+    { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 5); launch_stage_b_density<double>(ctx->g, ctx->d_x, npairs, nsplit, ctx->d_rho_part, ctx->st); }
+  } else {
+    { TScope ts(ctx, 0); launch_stage_a<float>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 5); launch_stage_b_density<float>(ctx->g, ctx->d_x, npairs, nsplit, ctx->d_rho_part, ctx->st); }
+  }
+  { TScope ts(ctx, 7); launch_density_reduce(ctx->d_rho_part, nsplit, ctx->N, scale, ctx->d_rho, ctx->st); }
+  ctx->launches += 3;
+  CK(cudaGetLastError());
+  return SDFT_OK;
+}
+
+extern "C" int sdft_density(sdft_ctx *ctx, int nstate, const double *cre, const double *cim, double *rho) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->max_states || !cre || !cim || !rho) return set_error(SDFT_ERR_ARG, "density: bad argument");
+  cudaSetDevice(ctx->device);
+  int r = upload_block(ctx, ctx->d_b2, nstate, cre, cim);
+  if (r) return r;
+  if ((r = density_core(ctx, ctx->d_b2, nstate, 1.0))) return r;
+  CK(cudaMemcpyAsync(rho, ctx->d_rho, (size_t)ctx->N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double scale, double *rho) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->filtered || imu < 0 || imu >= ctx->acc_nmu)
+    return set_error(SDFT_ERR_STATE, "density_dev: no filtered orbitals");
+  cudaSetDevice(ctx->device);
+  int r = density_core(ctx, ctx->d_acc + (size_t)imu * ctx->vec_elems, nstate, scale);
+  if (r) return r;
+  if (rho) {
+    CK(cudaMemcpyAsync(rho, ctx->d_rho, (size_t)ctx->N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  return SDFT_OK;
+}
+
+// Noise: host signs of gaussran2 (sequential generator), device FFT to G.
+static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid) {
+  if (np_states < 1 || myid < 0 || myid >= np_states) return set_error(SDFT_ERR_ARG, "noise: rank");
+  std::vector<double> seeds(np_states);
+  noise_rank_seeds(seed, np_states, seeds.data());
+  double q = seeds[myid];
+  const size_t n = (size_t)nstate * ctx->N;
+  std::vector<unsigned char> neg(n);
+  gauss_signs((long long)n, &q, neg.data());
+  if (n > ctx->neg_cap) {
+    if (ctx->d_neg) { cudaFree(ctx->d_neg); ctx->dev_bytes -= (long long)ctx->neg_cap; }
+    DM(ctx->d_neg, n);
+    ctx->neg_cap = n;
+  }
+  CK(cudaMemcpyAsync(ctx->d_neg, neg.data(), n, cudaMemcpyHostToDevice, ctx->st));
+  const int npairs = (nstate + 1) / 2;
+  int r;
+  if ((r = ensure_x(ctx, npairs))) return r;
+  CK(cudaMemsetAsync(ctx->d_chi, 0, ctx->vec_elems * sizeof(double), ctx->st));
+  EpiArgs e = base_epi(ctx);
+  e.mode = EPI_NOISE;
+  e.nstate = nstate;
+  e.OUT = ctx->d_chi;
+  e.invN = 1.0 / (double)ctx->N;
+  if (is_fp64(ctx)) {
+    { TScope ts(ctx, 6); launch_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+  } else {
+    { TScope ts(ctx, 6); launch_stage_b_noise<float>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
+    { TScope ts(ctx, 2); launch_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+  }
+  ctx->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->resident = nstate;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_noise_real_dev(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->max_states) return set_error(SDFT_ERR_ARG, "noise: nstate");
+  cudaSetDevice(ctx->device);
+  return noise_core(ctx, nstate, seed, np_states, myid);
+}
+
+extern "C" int sdft_noise_real(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid, double *cre,
+                               double *cim) {
+  if (!ctx || !cre || !cim) return set_error(SDFT_ERR_ARG, "noise: null");
+  if (nstate < 1 || nstate > ctx->max_states) return set_error(SDFT_ERR_ARG, "noise: nstate");
+  cudaSetDevice(ctx->device);
+  int r = noise_core(ctx, nstate, seed, np_states, myid);
+  if (r) return r;
+  if ((r = download_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}

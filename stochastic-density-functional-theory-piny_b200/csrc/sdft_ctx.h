@@ -1,0 +1,91 @@
+// sdft_ctx.h -- device context of the filter-path library (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "sdft_internal.h"
+#include "sdft_kernels.cuh"
+
+struct sdft_ctx {
+  int device = 0;
+  int prec = SDFT_PREC_FP64;
+  cudaStream_t st = nullptr;
+  // geometry
+  int n1 = 0, n2 = 0, n3 = 0, N = 0, ncoef = 0, ngp = 0;
+  double hmat[9];
+  double vol = 0.0;
+  std::vector<int> ka, kb, kc;
+  sdft::SphereCols cols;
+  sdft::DevGeom g{};
+  int max_states = 0, s_pad = 0, npairs_max = 0;
+  size_t vec_elems = 0;  // doubles per orbital block (s_pad*2*ngp)
+  // device geometry arrays
+  int *d_cp_gstart = nullptr, *d_cp_gcount = nullptr, *d_col_ab = nullptr, *d_gkc = nullptr;
+  double *d_ak2 = nullptr;
+  double2 *d_tw = nullptr;  // n1+n2+n3
+  float2 *d_twf = nullptr;
+  // potential
+  void *d_vp = nullptr;     // [n3][n1][n2] (double or float)
+  double *d_vks_tmp = nullptr;
+  bool have_v = false;
+  // KB
+  int P = 0, Ppad = 0, Mpad2 = 0;
+  double *d_pj = nullptr, *d_bk = nullptr, *d_w = nullptr, *d_z = nullptr, *d_zwork = nullptr;
+  size_t zwork_elems = 0;
+  // orbital blocks
+  double *d_chi = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_fnl = nullptr;
+  double *d_acc = nullptr;
+  int acc_nmu = 0;
+  double *d_coef = nullptr;
+  size_t coef_cap = 0;
+  // scratch
+  void *d_x = nullptr;
+  size_t x_bytes = 0;
+  double *d_dots = nullptr;
+  double *d_mom = nullptr;
+  size_t mom_cap = 0;
+  double *d_rho_part = nullptr, *d_rho = nullptr;
+  int rho_split = 0;
+  unsigned char *d_neg = nullptr;
+  size_t neg_cap = 0;
+  double *d_enl = nullptr;
+  // state
+  int resident = 0;          // orbitals in d_chi
+  int filtered = 0;          // orbitals with results in d_acc
+  long long launches = 0;
+  long long dev_bytes = 0;
+  double gcut = 0.0;
+  // per-kind event timing (sdft_ctx_set_timing)
+  bool timing = false;
+  struct TEv { int kind; cudaEvent_t a, b; };
+  std::vector<TEv> tev_pending;
+  std::vector<cudaEvent_t> tev_free;
+  double t_ms[8] = {0};
+  long long t_n[8] = {0};
+};
+
+namespace sdft {
+int dmalloc(sdft_ctx *c, void **p, size_t bytes);
+
+// RAII event pair around the launches of one kernel kind.
+struct TScope {
+  sdft_ctx *c;
+  int kind;
+  cudaEvent_t a = nullptr;
+  static cudaEvent_t get(sdft_ctx *c) {
+    if (!c->tev_free.empty()) { cudaEvent_t e = c->tev_free.back(); c->tev_free.pop_back(); return e; }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  TScope(sdft_ctx *ctx, int k) : c(ctx), kind(k) {
+    if (c->timing) { a = get(c); cudaEventRecord(a, c->st); }
+  }
+  ~TScope() {
+    if (c->timing) {
+      cudaEvent_t b = get(c);
+      cudaEventRecord(b, c->st);
+      c->tev_pending.push_back({kind, a, b});
+    }
+  }
+};
+}

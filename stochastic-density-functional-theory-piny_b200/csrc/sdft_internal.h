@@ -1,0 +1,34 @@
+// sdft_internal.h -- shared declarations of the B200 filter-path library.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include "../../include/sdft_b200.h"
+
+namespace sdft {
+
+int set_error(int code, const char *msg);
+
+// host helpers (sdft_host.cpp)
+void invert_cell(const double *h, double *hi);
+double cell_volume(const double *h);
+double ran_uniform(double *qseed);
+void gaussran2(int nran, double *qseed, double *gauss);
+void noise_rank_seeds(double seed, int np_states, double *out);
+void gauss_signs(long long nran, double *qseed, unsigned char *neg);
+int cheby_coeff(int L, int ngrid, double energy_diff, double energy_mean, double beta,
+                double chem_pot, int fun_flag, double *coeffs);
+
+// Largest supported FFT edge; every edge must be 2^a 3^b.
+constexpr int kMaxEdge = 128;
+
+// Column decomposition of the G sphere (see sdft_api.cu).  Columns are the
+// (ka,kb) lines of the full sphere {G} U {-G}; they are stored as mirror
+// pairs (ka,kb),(-ka,-kb) followed by the single (0,0) column.
+struct SphereCols {
+  int ncols = 0;       // 2*(ncp-1)+1
+  int ncp = 0;         // column pairs (the last one is the (0,0) column)
+  int ncols_pad = 0;   // row pitch of the column scratch
+  int kamax = 0;       // max |ka| over columns
+};
+
+}  // namespace sdft

@@ -1,0 +1,277 @@
+// sdft_kb.cu -- Kleinman-Bylander projector matrices for the GEMM form of
+// the nonlocal term.
+//
+// The reference accumulates, per G vector and per channel (atom, l, m),
+//   Z_r/Z_i += linear combinations of Re/Im c(G) e^{iG.R} v_l(|G|) Y_lm
+// (getNlmatFilter, stodft/reduced-energy/cp-energy-eext-stodft.c:1105-1169;
+// G = 0 term get_nlmat0, energy/cp/cp_energy_eext_nonloc.c:1083), and the
+// force  f(G) -= (4/Omega) vnorm v_l conj(e^{iG.R} Y_lm) Z  (get_nlfor,
+// cp_energy_eext_nonloc.c:2136-2173; G = 0: get_nlfor0 :2229).  Both maps
+// are linear in the orbital coefficients, so they are written here as two
+// dense real matrices over k = (Re c(G), Im c(G)):
+//   Z[u] = sum_k Pj[u][k] c[k],     f[k] += sum_u Bk[k][u] Z[u].
+// For each (atom, l) only 2l+1 of the 2(2l+1) real Z components are
+// independent: m = 0 has a vanishing Re (l odd) or Im (l even) part, and
+// the conjugate partner Y_{l,-m} = conj(Y_lm) (ylm index pairs 3/4, 6/7,
+// 8/9 of get_ylm) gives Z components equal up to sign.  Those are merged:
+// the partner's back-projection column is folded into the kept row with
+// that sign and its energy weight doubles.  P = sum_atoms sum_l (2l+1).
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "sdft_ctx.h"
+
+namespace sdft {
+
+struct KbRow {
+  int atom, type, l, ind;  // ind: 1-based ylm index of the kept channel
+  int part;                // 0: Re Z, 1: Im Z
+  int partner;             // partner ylm index or 0
+  double psign;            // Z_partner = psign * Z_kept
+  double vnorm;            // KB energy of the channel
+};
+
+__global__ void k_build_proj(int ncoef, int ngp, int Ppad, const int *__restrict__ kvec,
+                             const double *__restrict__ frac, const int *__restrict__ row_start,
+                             const int *__restrict__ row_count, const KbRow *__restrict__ rows,
+                             const double *__restrict__ vtab, int lmax1,
+                             const double *__restrict__ ylm,  // [10][ncoef][2]
+                             const double *__restrict__ gz, double four_over_vol, double inv_vol,
+                             double *__restrict__ Pj, double *__restrict__ Bk) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = blockIdx.y;
+  if (g >= ncoef) return;
+  const int K1 = 2 * ngp;
+  const int u0 = row_start[a], nu = row_count[a];
+  if (g == ncoef - 1) {  // G = 0: l = 0 only
+    const double y00 = 0.28209479177387814347;  // 1/sqrt(4 pi)
+    for (int r = 0; r < nu; r++) {
+      const KbRow R = rows[u0 + r];
+      if (R.l != 0) continue;
+      const int u = u0 + r;
+      Pj[(size_t)u * K1 + g] = gz[R.type] * y00;
+      Bk[(size_t)g * Ppad + u] = -2.0 * (y00 * gz[R.type] * R.vnorm * inv_vol);
+    }
+    return;
+  }
+  const double t = (double)kvec[3 * g] * frac[3 * a] + (double)kvec[3 * g + 1] * frac[3 * a + 1] +
+                   (double)kvec[3 * g + 2] * frac[3 * a + 2];
+  double sphi, cphi;
+  sincospi(2.0 * t, &sphi, &cphi);
+  for (int r = 0; r < nu; r++) {
+    const KbRow R = rows[u0 + r];
+    const int u = u0 + r;
+    const double v = vtab[((size_t)R.type * lmax1 + R.l) * ncoef + g];
+    const double hr = v * cphi, hi = v * sphi;
+    const double yr = ylm[((size_t)R.ind * ncoef + g) * 2], yi = ylm[((size_t)R.ind * ncoef + g) * 2 + 1];
+    double pr, pi;  // coefficients on Re c, Im c
+    const bool lodd = (R.l & 1);
+    if (!lodd) {
+      if (R.part == 0) { pr = 2.0 * yr * hr; pi = -2.0 * yr * hi; }
+      else { pr = 2.0 * yi * hr; pi = -2.0 * yi * hi; }
+    } else {
+      if (R.part == 0) { pr = -2.0 * yi * hi; pi = -2.0 * yi * hr; }
+      else { pr = 2.0 * yr * hi; pi = 2.0 * yr * hr; }
+    }
+    Pj[(size_t)u * K1 + g] = pr;
+    Pj[(size_t)u * K1 + ngp + g] = pi;
+    // back projection
+    const double s = v * four_over_vol;
+    const double Hr = cphi * s, Hi = sphi * s;
+    auto bk = [&](double yr_, double yi_, double &bre, double &bim) {
+      const double vfr = Hr * yr_ - Hi * yi_;
+      const double vfi = -(Hi * yr_ + Hr * yi_);
+      if (R.part == 0) { bre = -R.vnorm * vfr; bim = -R.vnorm * vfi; }
+      else { bre = R.vnorm * vfi; bim = -R.vnorm * vfr; }
+    };
+    double bre, bim;
+    bk(yr, yi, bre, bim);
+    if (R.partner) {
+      const double ypr = ylm[((size_t)R.partner * ncoef + g) * 2], ypi = ylm[((size_t)R.partner * ncoef + g) * 2 + 1];
+      double b2r, b2i;
+      bk(ypr, ypi, b2r, b2i);
+      bre += R.psign * b2r;
+      bim += R.psign * b2i;
+    }
+    Bk[(size_t)g * Ppad + u] = bre;
+    Bk[(size_t)(ngp + g) * Ppad + u] = bim;
+  }
+}
+
+// Y_lm (l <= 2) of get_ylm (energy/cp/cp_energy_eext_nonloc.c:2350), values only.
+static void ylm_host(double xk, double yk, double zk, double g, double *yr, double *yi) {
+  const double fpi = 4.0 * M_PI;
+  const double rt_fpi = 1.0 / std::sqrt(fpi), rt_thrfpi = std::sqrt(3.0 / fpi), rt_threpi = std::sqrt(1.50 / fpi);
+  const double hrt_fivfpi = 0.50 * std::sqrt(5.0 / fpi), rt_fiftepi = std::sqrt(7.50 / fpi);
+  double ctheta = zk / g;
+  double stheta = std::sqrt(xk * xk + yk * yk) / g;
+  double xyd = std::sqrt(xk * xk + yk * yk);
+  double cphi, sphi;
+  if (xyd == 0) { cphi = 1.0; sphi = 0.0; }
+  else { cphi = xk / xyd; sphi = yk / xyd; }
+  double c2phi = cphi * cphi - sphi * sphi, s2phi = 2.0 * cphi * sphi;
+  for (int i = 0; i < 10; i++) yr[i] = yi[i] = 0.0;
+  yr[1] = rt_fpi;
+  double y10r = rt_thrfpi * ctheta, y11r = rt_threpi * stheta * cphi, y11i = rt_threpi * stheta * sphi;
+  yr[2] = y10r;
+  yr[3] = y11r; yi[3] = y11i;
+  yr[4] = y11r; yi[4] = -y11i;
+  double y20r = hrt_fivfpi * (3.0 * ctheta * ctheta - 1.0);
+  double y21r = rt_fiftepi * stheta * ctheta * cphi, y21i = rt_fiftepi * stheta * ctheta * sphi;
+  double y22r = 0.50 * rt_fiftepi * stheta * stheta * c2phi, y22i = 0.50 * rt_fiftepi * stheta * stheta * s2phi;
+  yr[5] = y20r;
+  yr[6] = y21r; yi[6] = y21i;
+  yr[7] = y21r; yi[7] = -y21i;
+  yr[8] = y22r; yi[8] = y22i;
+  yr[9] = y22r; yi[9] = -y22i;
+}
+
+// get_vpsnow (energy/cp/cp_energy_eext.c:2139-2185) for one table.
+static double spline_eval(const double *tab, int nsplin, double gmin, double dg, double g) {
+  int iii = (int)((g - gmin) / dg) + 1;
+  if (iii > nsplin) iii = nsplin;
+  if (iii < 1) iii = 1;
+  double h0 = (double)(iii - 1) * dg + gmin;
+  double h = g - h0;
+  const double *v0 = tab, *v1 = tab + nsplin, *v2 = tab + 2 * nsplin, *v3 = tab + 3 * nsplin;
+  int i = iii - 1;
+  return ((v3[i] * h + v2[i]) * h + v1[i]) * h + v0[i];
+}
+
+}  // namespace sdft
+
+using namespace sdft;
+
+#define CKB(call)                                                           \
+  do {                                                                      \
+    cudaError_t e__ = (call);                                               \
+    if (e__ != cudaSuccess) { rc = set_error(SDFT_ERR_CUDA, cudaGetErrorString(e__)); goto done; } \
+  } while (0)
+
+int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
+  // release a previous projector set
+  double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl};
+  for (double **p : old)
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  ctx->P = 0;
+  if (!kb || kb->natm == 0) return SDFT_OK;
+  if (!kb->pos || !kb->type || !kb->lmax_type || !kb->vps || !kb->vpsnorm || !kb->gzvps0 || kb->ntype < 1 ||
+      kb->nsplin_g < 1 || kb->dg_spl <= 0.0)
+    return set_error(SDFT_ERR_ARG, "set_kb: incomplete projector description");
+  if (kb->lmax < 0 || kb->lmax > 2) return set_error(SDFT_ERR_UNSUPPORTED, "set_kb: l channels 0..2 only");
+  const int lmax1 = kb->lmax + 1;
+  const int ncoef = ctx->ncoef, ngp = ctx->ngp;
+  double hi[9];
+  invert_cell(ctx->hmat, hi);
+  // rows
+  std::vector<KbRow> rows;
+  std::vector<int> rstart(kb->natm), rcount(kb->natm);
+  for (int a = 0; a < kb->natm; a++) {
+    const int t = kb->type[a];
+    if (t < 0 || t >= kb->ntype) return set_error(SDFT_ERR_ARG, "set_kb: atom type out of range");
+    const int lm = kb->lmax_type[t];
+    if (lm > kb->lmax) return set_error(SDFT_ERR_ARG, "set_kb: lmax_type > lmax");
+    rstart[a] = (int)rows.size();
+    for (int l = 0; l <= lm; l++) {
+      const double vn = kb->vpsnorm[t * lmax1 + l];
+      auto add = [&](int ind, int part, int partner, double sgn) {
+        rows.push_back(KbRow{a, t, l, ind, part, partner, sgn, vn});
+      };
+      if (l == 0) add(1, 0, 0, 0.0);
+      if (l == 1) { add(2, 1, 0, 0.0); add(3, 0, 4, -1.0); add(3, 1, 4, +1.0); }
+      if (l == 2) { add(5, 0, 0, 0.0); add(6, 0, 7, +1.0); add(6, 1, 7, -1.0); add(8, 0, 9, +1.0); add(8, 1, 9, -1.0); }
+    }
+    rcount[a] = (int)rows.size() - rstart[a];
+  }
+  const int P = (int)rows.size();
+  if (P == 0) return SDFT_OK;
+  const int Ppad = (int)((P + 127) / 128 * 128);
+  const int K1 = 2 * ngp;
+  const int Mpad2 = (K1 + 127) / 128 * 128;
+  // per-G tables
+  std::vector<int> kv(3 * ncoef);
+  std::vector<double> vtab((size_t)kb->ntype * lmax1 * ncoef, 0.0), ylm((size_t)10 * ncoef * 2, 0.0);
+  const double tpi = 2.0 * M_PI;
+  for (int g = 0; g < ncoef; g++) {
+    kv[3 * g] = ctx->ka[g]; kv[3 * g + 1] = ctx->kb[g]; kv[3 * g + 2] = ctx->kc[g];
+    if (g == ncoef - 1) continue;
+    const double aka = ctx->ka[g], akb = ctx->kb[g], akc = ctx->kc[g];
+    const double xk = (aka * hi[0] + akb * hi[1] + akc * hi[2]) * tpi;
+    const double yk = (aka * hi[3] + akb * hi[4] + akc * hi[5]) * tpi;
+    const double zk = (aka * hi[6] + akb * hi[7] + akc * hi[8]) * tpi;
+    const double gg = std::sqrt(xk * xk + yk * yk + zk * zk);
+    double yr[10], yi[10];
+    ylm_host(xk, yk, zk, gg, yr, yi);
+    for (int i = 0; i < 10; i++) {
+      ylm[((size_t)i * ncoef + g) * 2] = yr[i];
+      ylm[((size_t)i * ncoef + g) * 2 + 1] = yi[i];
+    }
+    for (int t = 0; t < kb->ntype; t++)
+      for (int l = 0; l <= kb->lmax_type[t]; l++)
+        vtab[((size_t)t * lmax1 + l) * ncoef + g] =
+            spline_eval(kb->vps + ((size_t)t * lmax1 + l) * 4 * kb->nsplin_g, kb->nsplin_g, kb->gmin_spl,
+                        kb->dg_spl, gg);
+  }
+  // fractional coordinates wrapped as controlEwdNonlocFilter (box centre 0)
+  std::vector<double> frac(3 * kb->natm);
+  for (int a = 0; a < kb->natm; a++) {
+    const double x = kb->pos[3 * a], y = kb->pos[3 * a + 1], z = kb->pos[3 * a + 2];
+    double s[3] = {x * hi[0] + y * hi[3] + z * hi[6], x * hi[1] + y * hi[4] + z * hi[7],
+                   x * hi[2] + y * hi[5] + z * hi[8]};
+    for (int d = 0; d < 3; d++) frac[3 * a + d] = s[d] - std::nearbyint(s[d]);
+  }
+  std::vector<double> w(Ppad, 0.0);
+  for (int u = 0; u < P; u++) w[u] = rows[u].vnorm / ctx->vol * (rows[u].partner ? 2.0 : 1.0);
+
+  int rc = SDFT_OK;
+  int *d_kv = nullptr, *d_rs = nullptr, *d_rcnt = nullptr;
+  double *d_frac = nullptr, *d_vtab = nullptr, *d_ylm = nullptr, *d_gz = nullptr;
+  KbRow *d_rows = nullptr;
+  {
+    int r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_pj, (size_t)Ppad * K1 * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_bk, (size_t)Mpad2 * Ppad * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_w, (size_t)Ppad * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_z, (size_t)ctx->s_pad * Ppad * sizeof(double)))) return r;
+    ctx->zwork_elems = (size_t)16 * ctx->s_pad * Ppad;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_zwork, ctx->zwork_elems * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_fnl, ctx->vec_elems * sizeof(double)))) return r;
+  }
+  CKB(cudaMemset(ctx->d_pj, 0, (size_t)Ppad * K1 * sizeof(double)));
+  CKB(cudaMemset(ctx->d_bk, 0, (size_t)Mpad2 * Ppad * sizeof(double)));
+  CKB(cudaMemset(ctx->d_z, 0, (size_t)ctx->s_pad * Ppad * sizeof(double)));
+  CKB(cudaMemset(ctx->d_fnl, 0, ctx->vec_elems * sizeof(double)));
+  CKB(cudaMemcpy(ctx->d_w, w.data(), Ppad * sizeof(double), cudaMemcpyHostToDevice));
+  CKB(cudaMalloc(&d_kv, kv.size() * sizeof(int)));
+  CKB(cudaMalloc(&d_rs, rstart.size() * sizeof(int)));
+  CKB(cudaMalloc(&d_rcnt, rcount.size() * sizeof(int)));
+  CKB(cudaMalloc(&d_frac, frac.size() * sizeof(double)));
+  CKB(cudaMalloc(&d_vtab, vtab.size() * sizeof(double)));
+  CKB(cudaMalloc(&d_ylm, ylm.size() * sizeof(double)));
+  CKB(cudaMalloc(&d_gz, kb->ntype * sizeof(double)));
+  CKB(cudaMalloc(&d_rows, rows.size() * sizeof(KbRow)));
+  CKB(cudaMemcpy(d_kv, kv.data(), kv.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_rs, rstart.data(), rstart.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_rcnt, rcount.data(), rcount.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_frac, frac.data(), frac.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_vtab, vtab.data(), vtab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_ylm, ylm.data(), ylm.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_gz, kb->gzvps0, kb->ntype * sizeof(double), cudaMemcpyHostToDevice));
+  CKB(cudaMemcpy(d_rows, rows.data(), rows.size() * sizeof(KbRow), cudaMemcpyHostToDevice));
+  {
+    dim3 grid((ncoef + 127) / 128, kb->natm);
+    k_build_proj<<<grid, 128, 0, ctx->st>>>(ncoef, ngp, Ppad, d_kv, d_frac, d_rs, d_rcnt, d_rows, d_vtab, lmax1,
+                                            d_ylm, d_gz, 4.0 / ctx->vol, 1.0 / ctx->vol, ctx->d_pj, ctx->d_bk);
+    ctx->launches++;
+    CKB(cudaGetLastError());
+    CKB(cudaStreamSynchronize(ctx->st));
+  }
+  ctx->P = P;
+  ctx->Ppad = Ppad;
+  ctx->Mpad2 = Mpad2;
+done:
+  cudaFree(d_kv); cudaFree(d_rs); cudaFree(d_rcnt); cudaFree(d_frac);
+  cudaFree(d_vtab); cudaFree(d_ylm); cudaFree(d_gz); cudaFree(d_rows);
+  return rc;
+}

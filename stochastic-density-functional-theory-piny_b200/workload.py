@@ -1,0 +1,163 @@
+"""Synthetic diamond-Si workloads for the filter hot path.
+
+Inputs are generated, not read: seeded diamond-cubic Si supercells with a
+Gaussian local potential and Gaussian s+p Kleinman-Bylander projectors
+(no pseudopotential files exist for this path).
+
+* Cell: conventional cubic cell a0 = 10.26 bohr, 8 atoms at the fcc sites
+  plus the (1/4,1/4,1/4) shifted copies; supercells n x n x n.
+* V_loc(r) = sum_atoms -4 exp(-|r-R|^2 / (2*0.9^2)) Ha, periodic images,
+  sampled on the FFT grid in the filter layout (c fastest).  V_KS := V_loc.
+* KB projectors: beta_l(r) ~ r^l exp(-r^2/(2 rc^2)), rc = 1.2 bohr,
+  normalised in real space; radial form factors
+      v_0(g) = 4 pi N_0 sqrt(pi/2) rc^3 exp(-g^2 rc^2/2)
+      v_1(g) = 4 pi N_1 sqrt(pi/2) rc^5 g exp(-g^2 rc^2/2)
+  tabulated for get_vpsnow as per-knot Taylor coefficients
+  (vps0..vps3 = f, f', f''/2, f'''/6).  E_KB: s = +0.5 Ha, p = -0.5 Ha.
+* Plane waves 0.5|G|^2 <= Ecut = 10 Ha (20 Ry).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+A0_SI = 10.26
+ECUT_HA = 10.0
+SIGMA_LOC = 0.9
+V0_LOC = -4.0
+RC_KB = 1.2
+EKB = (0.5, -0.5)  # s, p
+
+CONFIGS = {
+    # name: (supercell n, grid, n_orbitals, L, polynomial)
+    "cfg1": dict(nrep=1, grid=(24, 24, 24), nsto=16, L=64, poly="newton", mu=0.2),
+    "cfg2": dict(nrep=2, grid=(48, 48, 48), nsto=128, L=256, poly="cheby", mu=None),
+    "cfg3": dict(nrep=4, grid=(96, 96, 96), nsto=512, L=512, poly="cheby", mu=None),
+}
+BETA = 1000.0          # 1/Ha
+ELEC_PER_8 = 32.0      # electrons per 8 Si atoms (4 e/atom)
+OCC = 2.0              # spin-unpolarised occupation
+
+
+def diamond_positions(nrep, a0=A0_SI):
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]], dtype=np.float64)
+    basis = np.concatenate([base, base + 0.25])
+    cells = np.array([[i, j, k] for i in range(nrep) for j in range(nrep) for k in range(nrep)], dtype=np.float64)
+    frac = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) / nrep
+    return frac
+
+
+def make_system(nrep=1, grid=(24, 24, 24), a0=A0_SI, strain=(0.0, 0.0, 0.0), disp_sigma=0.0, seed=0,
+                ecut=ECUT_HA, with_kb=True):
+    """Orthorhombic Si supercell.  Returns a dict with the cell, G sphere,
+    V_KS (filter layout), KB description and electron count."""
+    from . import setkvec3d_sm  # noqa: PLC0415  (package-relative)
+    rng = np.random.default_rng(seed)
+    L = np.array([a0 * nrep * (1.0 + s) for s in strain])
+    hmat = np.diag(L)
+    frac = diamond_positions(nrep, a0)
+    pos = frac * L
+    if disp_sigma > 0:
+        pos = pos + rng.normal(0.0, disp_sigma, size=pos.shape)
+    n1, n2, n3 = grid
+    kmax = [int(math.ceil(math.sqrt(2 * ecut) * Li / (2 * math.pi))) + 1 for Li in L]
+    ka, kb, kc, ib1, ib2 = setkvec3d_sm(hmat, ecut, kmax)
+    v = local_potential(pos, L, grid)
+    kbd = kb_projectors(pos, ecut, L) if with_kb else None
+    return dict(hmat=hmat, L=L, pos=pos, natm=len(pos), grid=tuple(grid), ka=ka, kb=kb, kc=kc, ib1=ib1, ib2=ib2,
+                vks=v, kb_desc=kbd, num_elec=ELEC_PER_8 * len(pos) / 8.0, ncoef=len(ka))
+
+
+def local_potential(pos, L, grid):
+    """V(r) in the filter layout (ia*n2 + ib)*n3 + ic; separable periodic Gaussians."""
+    n1, n2, n3 = grid
+    s2 = 2.0 * SIGMA_LOC ** 2
+
+    def axis(n, Lx, X):
+        x = np.arange(n) * (Lx / n)
+        d = x[None, :] - X[:, None]
+        d -= Lx * np.round(d / Lx)
+        g = np.zeros_like(d)
+        for img in (-2, -1, 0, 1, 2):
+            g += np.exp(-((d + img * Lx) ** 2) / s2)
+        return g
+
+    gx, gy, gz = axis(n1, L[0], pos[:, 0]), axis(n2, L[1], pos[:, 1]), axis(n3, L[2], pos[:, 2])
+    v = V0_LOC * np.einsum("ai,aj,ak->ijk", gx, gy, gz, optimize=True)
+    return np.ascontiguousarray(v.reshape(-1))
+
+
+def _ff(l, g):
+    """form factor f and its first three derivatives at g (arrays)."""
+    a = RC_KB ** 2 / 2.0
+    e = np.exp(-a * g * g)
+    if l == 0:
+        n0 = math.sqrt(4.0 / (math.sqrt(math.pi) * RC_KB ** 3))
+        A = 4.0 * math.pi * n0 * math.sqrt(math.pi / 2.0) * RC_KB ** 3
+        f = A * e
+        f1 = A * (-2 * a * g) * e
+        f2 = A * (4 * a * a * g * g - 2 * a) * e
+        f3 = A * (-8 * a ** 3 * g ** 3 + 12 * a * a * g) * e
+    else:
+        n1 = math.sqrt(8.0 / (3.0 * math.sqrt(math.pi) * RC_KB ** 5))
+        B = 4.0 * math.pi * n1 * math.sqrt(math.pi / 2.0) * RC_KB ** 5
+        f = B * g * e
+        f1 = B * (1 - 2 * a * g * g) * e
+        f2 = B * (-6 * a * g + 4 * a * a * g ** 3) * e
+        f3 = B * (-6 * a + 24 * a * a * g * g - 8 * a ** 3 * g ** 4) * e
+    return f, f1, f2, f3
+
+
+def kb_projectors(pos, ecut, L, nsplin=2048):
+    gmax = math.sqrt(2 * ecut) * 1.05 + 0.5
+    dg = gmax / (nsplin - 1)
+    g = np.arange(nsplin) * dg
+    vps = np.zeros((1, 2, 4, nsplin))
+    for l in (0, 1):
+        f, f1, f2, f3 = _ff(l, g)
+        vps[0, l] = np.stack([f, f1, f2 / 2.0, f3 / 6.0])
+    return dict(natm=len(pos), pos=np.ascontiguousarray(pos, dtype=np.float64), type=np.zeros(len(pos), np.int32),
+                ntype=1, lmax=1, lmax_type=np.array([1], np.int32), nsplin_g=nsplin, gmin_spl=0.0, dg_spl=dg,
+                vps=vps.reshape(-1), vpsnorm=np.array(EKB, dtype=np.float64),
+                gzvps0=np.array([_ff(0, np.zeros(1))[0][0]], dtype=np.float64))
+
+
+def half_dot(ncoef, ar, ai, br, bi):
+    """<a|b> over the half sphere: 2 sum (re re + im im) - re(G0) re(G0)."""
+    return 2.0 * (np.dot(ar, br) + np.dot(ai, bi)) - ar[ncoef - 1] * br[ncoef - 1]
+
+
+def lanczos_bounds(hpsi, ncoef, nstep=20, seed=15, margin=0.1):
+    """Spectral bounds from `nstep` Lanczos steps on one random real orbital.
+
+    hpsi(cr, ci) -> raw PINY force (f = -4 H c for G != 0, -2 H c at G = 0).
+    Returns (Emin - margin, Emax + margin) like calc-spectral-range.c's +-0.1."""
+    rng = np.random.default_rng(seed)
+    cr = rng.standard_normal(ncoef)
+    ci = rng.standard_normal(ncoef)
+    ci[-1] = 0.0
+    nrm = math.sqrt(half_dot(ncoef, cr, ci, cr, ci))
+    cr /= nrm
+    ci /= nrm
+    alphas, betas = [], []
+    pr = np.zeros(ncoef); pi = np.zeros(ncoef)
+    beta = 0.0
+    for _ in range(nstep):
+        fr, fi = hpsi(cr, ci)
+        hr = -0.25 * fr; hi = -0.25 * fi
+        hr[-1] = -0.5 * fr[-1]; hi[-1] = 0.0
+        alpha = half_dot(ncoef, cr, ci, hr, hi)
+        wr = hr - alpha * cr - beta * pr
+        wi = hi - alpha * ci - beta * pi
+        alphas.append(alpha)
+        beta = math.sqrt(max(half_dot(ncoef, wr, wi, wr, wi), 0.0))
+        betas.append(beta)
+        if beta < 1e-12:
+            break
+        pr, pi = cr, ci
+        cr, ci = wr / beta, wi / beta
+    k = len(alphas)
+    T = np.diag(alphas) + np.diag(betas[:k - 1], 1) + np.diag(betas[:k - 1], -1)
+    ev = np.linalg.eigvalsh(T)
+    return float(ev[0] - margin), float(ev[-1] + margin)

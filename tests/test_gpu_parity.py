@@ -1,0 +1,190 @@
+"""GPU parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances: FP64 plain form rel-L2 <= 1e-10 (filtered orbitals, density);
+single H applications <= 1e-12.  Mixed precision: density rel-L2 vs the
+FP64 result <= 1e-5 on these short filters."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_H = 1e-12
+TOL = 1e-10
+
+
+def _ctx(pkg, s, nmax, prec=0, kb=True):
+    c = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=nmax)
+    c.set_vks(s["vks"])
+    if kb:
+        c.set_kb(s["kb_desc"])
+    return c
+
+
+@pytest.fixture(scope="module")
+def o1(sys1):
+    return O.OracleSys(sys1)
+
+
+@pytest.fixture(scope="module")
+def c1(pkg, sys1):
+    c = _ctx(pkg, sys1, 16)
+    yield c
+    c.close()
+
+
+def _rand(nc, ns, seed):
+    rng = np.random.default_rng(seed)
+    cr = rng.standard_normal(ns * nc)
+    ci = rng.standard_normal(ns * nc)
+    ci.reshape(ns, nc)[:, -1] = 0.0
+    return cr, ci
+
+
+@pytest.mark.parametrize("ns", [1, 2, 5, 16])
+def test_hpsi_cfg1(c1, o1, sys1, ns):
+    cr, ci = _rand(sys1["ncoef"], ns, ns)
+    fr, fi, e = c1.calc_coef_force(cr, ci, want_enl=True)
+    orr, oi, oe = o1.hpsi(cr, ci, want_enl=True)
+    assert rel_l2(np.concatenate([fr, fi]), np.concatenate([orr, oi])) < TOL_H
+    assert abs(e - oe) < 1e-12 * abs(oe)
+
+
+def test_hpsi_local_only_and_kinetic_cap(pkg, sys1):
+    s = dict(sys1)
+    c = _ctx(pkg, s, 4, kb=False)
+    s0 = dict(s)
+    s0["kb_desc"] = None
+    o = O.OracleSys(s0)
+    cr, ci = _rand(s["ncoef"], 3, 7)
+    a = c.calc_coef_force(cr, ci)
+    b = o.hpsi(cr, ci)
+    assert rel_l2(np.concatenate(a), np.concatenate(b)) < TOL_H
+    c.close()
+
+
+def test_hpsi_cfg2(pkg, sys2):
+    c = _ctx(pkg, sys2, 3)
+    o = O.OracleSys(sys2)
+    cr, ci = _rand(sys2["ncoef"], 3, 3)
+    a = c.calc_coef_force(cr, ci)
+    b = o.hpsi(cr, ci)
+    assert rel_l2(np.concatenate(a), np.concatenate(b)) < TOL_H
+    c.close()
+
+
+def test_noise_matches_oracle(c1, o1, sys1):
+    for ns, myid, np_ in ((16, 0, 1), (5, 2, 4)):
+        a = c1.genNoiseOrbitalReal(ns, seed=10.0, np_states=np_, myid=myid)
+        b = o1.noise(ns, seed=10.0, np_states=np_, myid=myid)
+        assert rel_l2(np.concatenate(a), np.concatenate(b)) < 1e-13
+
+
+def _bounds(c, s):
+    import __graft_entry__ as g
+    wl = g.load_workload()
+    return wl.lanczos_bounds(lambda r, i: c.calc_coef_force(r, i), s["ncoef"])
+
+
+def test_filter_newton_config1_full(pkg, wl, c1, o1, sys1):
+    """Config 1 as specified: 16 orbitals, Newton L=64, mu = 0.2 Ha, beta 1000."""
+    emin, emax = _bounds(c1, sys1)
+    ediff = emax - emin
+    scale = 4.0 / ediff
+    samp, unsc = pkg.genSampNewtonHermit(64, -2.0, 2.0, scale, emin)
+    ec = pkg.genCoeffNewtonHermit(64, 0.2, wl.BETA, samp, unsc)
+    cr, ci = c1.genNoiseOrbitalReal(16, seed=10.0)
+    (sr,), (si,) = c1.filterNewtonPolyHerm(cr, ci, ec, samp, 1, scale, 0.5 * (emin + emax))
+    osr, osi = o1.filter_newton(cr, ci, ec, samp, 1, scale, 0.5 * (emin + emax))
+    assert rel_l2(np.concatenate([sr, si]), np.concatenate([osr[0], osi[0]])) < TOL
+    rho = c1.rhoCalcRealStoHybrid(sr, si)
+    orho = o1.density(osr[0], osi[0])
+    assert rel_l2(rho, orho) < TOL
+
+
+@pytest.mark.parametrize("ns,L,nmu", [(6, 32, 1), (5, 17, 2)])
+def test_filter_cheby_with_moments(pkg, c1, o1, sys1, ns, L, nmu):
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    ec = np.stack([pkg.calcChebyCoeff(L, emax - emin, em, 1000.0, mu) for mu in (0.2, 0.3)[:nmu]], axis=1).ravel()
+    cr, ci = c1.genNoiseOrbitalReal(ns, seed=3.0)
+    sre, sim, m = c1.filterChebyPolyHerm(cr, ci, ec, nmu, scale, em, store_moments=True)
+    osr, osi, om = o1.filter_cheby(cr, ci, ec, nmu, scale, em, store_moments=True)
+    for k in range(nmu):
+        assert rel_l2(np.concatenate([sre[k], sim[k]]), np.concatenate([osr[k], osi[k]])) < TOL
+    assert rel_l2(m[:L], om[:L]) < TOL
+
+
+@pytest.mark.parametrize("L", [16, 33])
+def test_cheby_moments(c1, o1, sys1, L):
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    cr, ci = c1.genNoiseOrbitalReal(7, seed=10.0)
+    m = c1.calcChebyMoments(cr, ci, L, scale, em)
+    om = o1.moments(cr, ci, L, scale, em)
+    assert rel_l2(m, om) < TOL
+
+
+def test_normh_steps(c1, o1, sys1):
+    nc = sys1["ncoef"]
+    cr, ci = _rand(nc, 3, 11)
+    wr, wi = _rand(nc, 3, 12)
+    scale, em = 0.05, 20.0
+    a = [x.copy() for x in (cr, ci, wr, wi)]
+    fr, fi = c1.normHCheby(a[0], a[1], a[2], a[3], 3, scale, em)
+    b = [x.copy() for x in (cr, ci, wr, wi)]
+    ofr, ofi = np.zeros_like(cr), np.zeros_like(ci)
+    O.lib().oracle_normh_cheby(o1._p, 3, 3, 1, scale, em, O._d(b[0]), O._d(b[1]), O._d(b[2]), O._d(b[3]),
+                               O._d(ofr), O._d(ofi))
+    assert rel_l2(np.concatenate([fr, fi]), np.concatenate([ofr, ofi])) < TOL_H
+    for x, y in zip(a, b):
+        assert rel_l2(x, y) < TOL_H
+    c = [cr.copy(), ci.copy()]
+    fr, fi = c1.normHNewtonHerm(c[0], c[1], scale, em, 0.3)
+    d = [cr.copy(), ci.copy()]
+    O.lib().oracle_normh_newton(o1._p, 3, scale, em, 0.3, O._d(d[0]), O._d(d[1]), O._d(ofr), O._d(ofi))
+    assert rel_l2(np.concatenate(c), np.concatenate(d)) < TOL_H
+
+
+def test_density_odd(c1, o1, sys1):
+    cr, ci = c1.genNoiseOrbitalReal(5, seed=2.0)
+    rho = c1.rhoCalcRealStoHybrid(cr, ci)
+    assert rel_l2(rho, o1.density(cr, ci)) < 1e-12
+    # electron-count identity: sum(rho)/N = sum_s <c_s|c_s> (Parseval over the half sphere)
+    nc = sys1["ncoef"]
+    tot = sum(2 * np.dot(cr[i * nc:(i + 1) * nc], cr[i * nc:(i + 1) * nc]) +
+              2 * np.dot(ci[i * nc:(i + 1) * nc], ci[i * nc:(i + 1) * nc]) - cr[i * nc + nc - 1] ** 2
+              for i in range(5))
+    assert abs(rho.sum() / rho.size - tot) < 1e-10 * tot
+
+
+def test_cfg2_filter_short(pkg, sys2):
+    c = _ctx(pkg, sys2, 4)
+    o = O.OracleSys(sys2)
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    ec = pkg.calcChebyCoeff(12, emax - emin, em, 1000.0, 0.2)
+    cr, ci = c.genNoiseOrbitalReal(4, seed=10.0)
+    (sr,), (si,) = c.filterChebyPolyHerm(cr, ci, ec, 1, scale, em)
+    osr, osi = o.filter_cheby(cr, ci, ec, 1, scale, em)
+    assert rel_l2(np.concatenate([sr, si]), np.concatenate([osr[0], osi[0]])) < TOL
+    c.close()
+
+
+def test_mixed_precision_close_to_fp64(pkg, sys1):
+    cd = _ctx(pkg, sys1, 8, prec=0)
+    cm = _ctx(pkg, sys1, 8, prec=1)
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    ec = pkg.calcChebyCoeff(64, emax - emin, em, 1000.0, 0.2)
+    cr, ci = cd.genNoiseOrbitalReal(8, seed=10.0)
+    (a,), (b,) = cd.filterChebyPolyHerm(cr, ci, ec, 1, scale, em)
+    (x,), (y,) = cm.filterChebyPolyHerm(cr, ci, ec, 1, scale, em)
+    assert rel_l2(np.concatenate([x, y]), np.concatenate([a, b])) < 1e-5
+    ra = cd.rhoCalcRealStoHybrid(a, b)
+    rx = cm.rhoCalcRealStoHybrid(x, y)
+    assert rel_l2(rx, ra) < 1e-5
+    cd.close()
+    cm.close()

@@ -13,6 +13,7 @@
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
 #include "sdft_ctx.h"
+#include "sdft_kernels2.cuh"
 
 namespace sdft {
 
@@ -211,7 +212,17 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
   e.C = cur;
   e.FNL = ctx->P ? ctx->d_fnl : nullptr;
   e.invN = 1.0 / (double)ctx->N;
-  if (is_fp64(ctx)) {
+  if (ctx->fast) {
+    if (is_fp64(ctx)) {
+      { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 1); fast_stage_b<double>(ctx->g, ctx->d_x, (const double *)ctx->d_vp, npairs, ctx->st); }
+      { TScope ts(ctx, 2); fast_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+    } else {
+      { TScope ts(ctx, 0); fast_stage_a<float>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 1); fast_stage_b<float>(ctx->g, ctx->d_x, (const float *)ctx->d_vp, npairs, ctx->st); }
+      { TScope ts(ctx, 2); fast_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+    }
+  } else if (is_fp64(ctx)) {
     { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
     { TScope ts(ctx, 1); launch_stage_b<double>(ctx->g, ctx->d_x, (const double *)ctx->d_vp, npairs, ctx->st); }
     { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
@@ -406,6 +417,10 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
     if (need > 227 * 1024) return fail(set_error(SDFT_ERR_UNSUPPORTED, "plane does not fit shared memory"));
     if (n1 * n2 > 512 * 24) return fail(set_error(SDFT_ERR_UNSUPPORTED, "plane too large"));
   }
+  {
+    const char *ev = getenv("SDFT_GENERIC_FFT");  // force the runtime-size kernels (testing)
+    ctx->fast = fast_supported(n1, n2, n3) && !(ev && ev[0] == '1');
+  }
   std::vector<int> gkc(ncoef);
   for (int i = 0; i < ncoef; i++) gkc[i] = kc[i];
   std::vector<double> ak2(ncoef);
@@ -496,10 +511,14 @@ extern "C" int sdft_ctx_set_vks(sdft_ctx *ctx, const double *v) {
   if (!ctx || !v) return set_error(SDFT_ERR_ARG, "set_vks: null");
   cudaSetDevice(ctx->device);
   CK(cudaMemcpyAsync(ctx->d_vks_tmp, v, (size_t)ctx->N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-  if (is_fp64(ctx))
+  if (ctx->fast) {
+    if (is_fp64(ctx)) fast_vks_perm<double>(ctx->g, ctx->d_vks_tmp, (double *)ctx->d_vp, ctx->st);
+    else fast_vks_perm<float>(ctx->g, ctx->d_vks_tmp, (float *)ctx->d_vp, ctx->st);
+  } else if (is_fp64(ctx)) {
     launch_vks_transpose<double>(ctx->d_vks_tmp, (double *)ctx->d_vp, ctx->n1, ctx->n2, ctx->n3, ctx->st);
-  else
+  } else {
     launch_vks_transpose<float>(ctx->d_vks_tmp, (float *)ctx->d_vp, ctx->n1, ctx->n2, ctx->n3, ctx->st);
+  }
   ctx->launches++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));
@@ -761,7 +780,15 @@ static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double sca
     ctx->rho_split = nsplit;
   }
   if (!ctx->d_rho) DM(ctx->d_rho, (size_t)ctx->N * sizeof(double));
-  if (is_fp64(ctx)) {
+  if (ctx->fast) {
+    if (is_fp64(ctx)) {
+      { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 5); fast_stage_b_density<double>(ctx->g, ctx->d_x, npairs, ctx->d_rho_part, ctx->st); }
+    } else {
+      { TScope ts(ctx, 0); fast_stage_a<float>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 5); fast_stage_b_density<float>(ctx->g, ctx->d_x, npairs, ctx->d_rho_part, ctx->st); }
+    }
+  } else if (is_fp64(ctx)) {
     { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
     { TScope ts(ctx, 5); launch_stage_b_density<double>(ctx->g, ctx->d_x, npairs, nsplit, ctx->d_rho_part, ctx->st); }
   } else {
@@ -824,7 +851,15 @@ static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int
   e.nstate = nstate;
   e.OUT = ctx->d_chi;
   e.invN = 1.0 / (double)ctx->N;
-  if (is_fp64(ctx)) {
+  if (ctx->fast) {
+    if (is_fp64(ctx)) {
+      { TScope ts(ctx, 6); fast_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 2); fast_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+    } else {
+      { TScope ts(ctx, 6); fast_stage_b_noise<float>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 2); fast_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+    }
+  } else if (is_fp64(ctx)) {
     { TScope ts(ctx, 6); launch_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
     { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
   } else {

@@ -54,6 +54,7 @@ struct sdft_ctx {
   long long launches = 0;
   long long dev_bytes = 0;
   double gcut = 0.0;
+  bool fast = false;  // compile-time-edge FFT kernels available
   // per-kind event timing (sdft_ctx_set_timing)
   bool timing = false;
   struct TEv { int kind; cudaEvent_t a, b; };

@@ -1,0 +1,187 @@
+// sdft_fft2.cuh -- compile-time-size line FFTs for the fast path.
+//
+// A line of N = R1*R2 points is transformed in two passes over shared
+// memory (the "four-step" factorisation N = R1 x R2 without the explicit
+// transpose):
+//
+//   forward, natural -> permuted ("DIF" order, dif()):
+//     pass 1, per (line, j2):  R1-point DFT of x[j2 + R2*j1] over j1, times
+//                              w_N^(j2*k1), stored back at j2 + R2*k1
+//     pass 2, per (line, k1):  R2-point DFT of the block R2*k1 + [0,R2),
+//                              stored back in place
+//     -> frequency k1 + R1*k2 ends up at position R2*k1 + k2.
+//   reverse, permuted -> natural ("DIT" order, dit()): the two passes in
+//     the opposite order with the same twiddles; either sign.
+//
+// Every unit reads and writes only its own positions, so a pass needs no
+// barrier between its loads and stores (no butterflies held across a
+// barrier, low register pressure); one __syncthreads separates the passes.
+// Consumers index the permuted order directly (pos()/ipos()), so no data is
+// ever moved just to undo the permutation.  The R-point DFTs run in
+// registers with compile-time twiddles (sdft_twiddles.cuh).
+#pragma once
+#include "sdft_fft.cuh"
+#include "sdft_twiddles.cuh"
+
+namespace sdft {
+
+template <int N> struct Plan;
+template <> struct Plan<12> { static constexpr int R1 = 4, R2 = 3; };
+template <> struct Plan<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Plan<24> { static constexpr int R1 = 4, R2 = 6; };
+template <> struct Plan<32> { static constexpr int R1 = 4, R2 = 8; };
+template <> struct Plan<36> { static constexpr int R1 = 6, R2 = 6; };
+template <> struct Plan<48> { static constexpr int R1 = 8, R2 = 6; };
+template <> struct Plan<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Plan<72> { static constexpr int R1 = 8, R2 = 9; };
+template <> struct Plan<96> { static constexpr int R1 = 8, R2 = 12; };
+template <> struct Plan<128> { static constexpr int R1 = 8, R2 = 16; };
+
+// position of (frequency or real-space) index k after a dif() pass pair
+template <int N> __device__ __forceinline__ int pos(int k) {
+  return Plan<N>::R2 * (k % Plan<N>::R1) + k / Plan<N>::R1;
+}
+// index stored at position p
+template <int N> __device__ __forceinline__ int ipos(int p) {
+  return (p % Plan<N>::R2) * Plan<N>::R1 + p / Plan<N>::R2;
+}
+
+template <int R> __device__ __forceinline__ double twc_re(int t);
+template <int R> __device__ __forceinline__ double twc_im(int t);
+#define SDFT_TW(R)                                                                         \
+  template <> __device__ __forceinline__ double twc_re<R>(int t) { return kTw##R##re[t]; } \
+  template <> __device__ __forceinline__ double twc_im<R>(int t) { return kTw##R##im[t]; }
+SDFT_TW(6)
+SDFT_TW(8)
+SDFT_TW(9)
+SDFT_TW(12)
+SDFT_TW(16)
+SDFT_TW(24)
+SDFT_TW(32)
+#undef SDFT_TW
+
+template <int R> struct F1 { static constexpr int A = (R % 4 == 0 && R > 4) ? 4 : ((R % 3 == 0) ? 3 : 2); };
+
+// In-register R-point DFT, natural order in and out, sign DIR.
+template <int R, int DIR, typename C> __device__ __forceinline__ void dftr(C *v) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2 || R == 3 || R == 4) {
+    dft_small<R, DIR>(v);
+  } else {
+    constexpr int A = F1<R>::A, B = R / A;
+    using T = decltype(v[0].x);
+    C y[R];
+#pragma unroll
+    for (int j2 = 0; j2 < B; j2++) {
+      C t[A];
+#pragma unroll
+      for (int j1 = 0; j1 < A; j1++) t[j1] = v[j2 + B * j1];
+      dftr<A, DIR>(t);
+#pragma unroll
+      for (int k1 = 0; k1 < A; k1++) {
+        const int e = j2 * k1;  // < R
+        if (e == 0) {
+          y[j2 + B * k1] = t[k1];
+        } else {
+          C w;
+          w.x = (T)twc_re<R>(e);
+          w.y = (T)(DIR < 0 ? twc_im<R>(e) : -twc_im<R>(e));
+          y[j2 + B * k1] = cmul(t[k1], w);
+        }
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; k1++) {
+      C t[B];
+#pragma unroll
+      for (int j2 = 0; j2 < B; j2++) t[j2] = y[j2 + B * k1];
+      dftr<B, DIR>(t);
+#pragma unroll
+      for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = t[k2];
+    }
+  }
+}
+
+// Line addressing for the two-pass FFTs.  base(l) is the offset of line l,
+// ES the element stride (compile time).
+struct Lines1 {  // lines at l*ls
+  int ls;
+  __device__ __forceinline__ int base(int l) const { return l * ls; }
+};
+struct Lines2 {  // two contiguous groups of lines (rows 0..n1-1 and the top ones)
+  int nl1, ls, off2;
+  __device__ __forceinline__ int base(int l) const { return (l < nl1) ? l * ls : off2 + (l - nl1) * ls; }
+};
+
+// natural -> permuted.  twN: exp(-2 pi i t/N) in shared memory.
+template <int N, int ES, int DIR, typename C, typename LM>
+__device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
+  constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+#pragma unroll 1
+  for (int u = tid; u < nl * R2; u += nthr) {
+    const int l = u / R2, j2 = u - l * R2;
+    C *p = buf + lm.base(l);
+    C v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; j1++) v[j1] = p[(j2 + R2 * j1) * ES];
+    dftr<R1, DIR>(v);
+    p[j2 * ES] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; k1++) {
+      C w = lds_tw(twN + j2 * k1);
+      if (DIR > 0) w.y = -w.y;
+      p[(j2 + R2 * k1) * ES] = cmul(v[k1], w);
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int u = tid; u < nl * R1; u += nthr) {
+    const int l = u / R1, k1 = u - l * R1;
+    C *p = buf + lm.base(l) + R2 * k1 * ES;
+    C v[R2];
+#pragma unroll
+    for (int j = 0; j < R2; j++) v[j] = p[j * ES];
+    dftr<R2, DIR>(v);
+#pragma unroll
+    for (int j = 0; j < R2; j++) p[j * ES] = v[j];
+  }
+  __syncthreads();
+}
+
+// permuted -> natural
+template <int N, int ES, int DIR, typename C, typename LM>
+__device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
+  constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+#pragma unroll 1
+  for (int u = tid; u < nl * R1; u += nthr) {
+    const int l = u / R1, k1 = u - l * R1;
+    C *p = buf + lm.base(l) + R2 * k1 * ES;
+    C v[R2];
+#pragma unroll
+    for (int j = 0; j < R2; j++) v[j] = p[j * ES];
+    dftr<R2, DIR>(v);
+    p[0] = v[0];
+#pragma unroll
+    for (int j2 = 1; j2 < R2; j2++) {
+      C w = lds_tw(twN + j2 * k1);
+      if (DIR > 0) w.y = -w.y;
+      p[j2 * ES] = cmul(v[j2], w);
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int u = tid; u < nl * R2; u += nthr) {
+    const int l = u / R2, j2 = u - l * R2;
+    C *p = buf + lm.base(l);
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) v[k1] = p[(R2 * k1 + j2) * ES];
+    dftr<R1, DIR>(v);
+#pragma unroll
+    for (int j1 = 0; j1 < R1; j1++) p[(j2 + R2 * j1) * ES] = v[j1];
+  }
+  __syncthreads();
+}
+
+}  // namespace sdft

@@ -1,0 +1,546 @@
+// sdft_kernels2.cu -- fast-path FFT stages with compile-time grid edges.
+//
+// Same stage split as sdft_kernels.cu (A: pack + c-FFT, B: plane FFTs x V,
+// C: c-FFT + unpack/epilogue) but every 1-D transform is the two-pass
+// factorised FFT of sdft_fft2.cuh:
+//   stage A writes the c-transformed columns in the permuted real-space
+//   order r = pos_N3(ic) (X row r);
+//   stage B forward-transforms b then a (natural -> permuted), multiplies by
+//   V stored in the same permuted order, and transforms back a then b
+//   (permuted -> natural);
+//   stage C transforms X rows r back to natural kc (permuted -> natural).
+// So no data movement is ever spent on undoing an FFT permutation.
+#include <cuda_runtime.h>
+#include "sdft_fft2.cuh"
+#include "sdft_internal.h"
+#include "sdft_kernels.cuh"
+#include "sdft_kernels2.cuh"
+
+namespace sdft {
+
+template <typename T> __device__ __forceinline__ const typename CT<T>::type *twp(const DevGeom &g, int d);
+template <> __device__ __forceinline__ const double2 *twp<double>(const DevGeom &g, int d) {
+  return d == 1 ? g.tw1 : (d == 2 ? g.tw2 : g.tw3);
+}
+template <> __device__ __forceinline__ const float2 *twp<float>(const DevGeom &g, int d) {
+  return d == 1 ? g.tw1f : (d == 2 ? g.tw2f : g.tw3f);
+}
+
+// ---------------------------------------------------------------------------
+// stage A
+// ---------------------------------------------------------------------------
+template <typename T, int N3>
+__global__ void __launch_bounds__(kColThreads)
+kf_stage_a(DevGeom g, const double *__restrict__ C, int nstate, int pair0, typename CT<T>::type *__restrict__ X) {
+  using C2 = typename CT<T>::type;
+  constexpr int P3 = N3 + 1;
+  __shared__ __align__(16) C2 tw[N3];
+  __shared__ __align__(16) C2 buf[2 * kCPB * P3];
+  const int tid = threadIdx.x;
+  const int cp0 = blockIdx.x * kCPB;
+  const int cp1 = min(cp0 + kCPB, g.ncp);
+  const int col0 = 2 * cp0;
+  const int ncl = min(2 * cp1, g.ncols) - col0;
+  const int p = pair0 + blockIdx.y;
+  const int s1 = 2 * p, s2 = 2 * p + 1;
+  const bool has2 = s2 < nstate;
+  const C2 *twg = twp<T>(g, 3);
+  for (int t = tid; t < N3; t += kColThreads) tw[t] = twg[t];
+  for (int i = tid; i < ncl * P3; i += kColThreads) buf[i] = cmk<C2>(0.0, 0.0);
+  __syncthreads();
+  const size_t o1 = (size_t)s1 * 2 * g.ngp, o2 = (size_t)s2 * 2 * g.ngp;
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int cp = cp0 + warp; cp < cp1; cp += kColThreads / 32) {
+    const int lc = 2 * (cp - cp0);
+    const bool zc = (cp == g.ncp - 1);
+    const int lm = zc ? lc : lc + 1;
+    const int gs = g.cp_gstart[cp], gc = g.cp_gcount[cp];
+    for (int e = lane; e < gc; e += 32) {
+      const int gi = gs + e;
+      const int kc = g.gkc[gi];
+      const double a = C[o1 + gi], b = C[o1 + g.ngp + gi];
+      const double c = has2 ? C[o2 + gi] : 0.0, d = has2 ? C[o2 + g.ngp + gi] : 0.0;
+      const int kd = kc < 0 ? kc + N3 : kc;
+      const int km = kc > 0 ? N3 - kc : -kc;
+      buf[lc * P3 + kd] = cmk<C2>(a - d, b + c);
+      buf[lm * P3 + km] = cmk<C2>(a + d, -b + c);
+    }
+    if (zc && lane == 0) {
+      const int g0 = g.ncoef - 1;
+      buf[lc * P3] = cmk<C2>(C[o1 + g0], has2 ? C[o2 + g0] : 0.0);
+    }
+  }
+  __syncthreads();
+  dif<N3, 1, +1>(buf, Lines1{P3}, ncl, tw, tid, kColThreads);
+  C2 *Xp = X + (size_t)blockIdx.y * N3 * g.ncols_pad;
+  for (int i = tid; i < N3 * ncl; i += kColThreads) {
+    const int r = i / ncl, cl = i - r * ncl;
+    Xp[(size_t)r * g.ncols_pad + col0 + cl] = buf[cl * P3 + r];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stage C
+// ---------------------------------------------------------------------------
+struct Dots2 { double d0, d1, d2; };
+
+__device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, int s, int gi, bool g0, double fr,
+                                          double fi, Dots2 &dt) {
+  const size_t o = (size_t)s * 2 * g.ngp + gi;
+  if (e.mode == EPI_NOISE) {
+    e.OUT[o] = fr;
+    e.OUT[o + g.ngp] = fi;
+    return;
+  }
+  const double cr = e.C[o], ci = e.C[o + g.ngp];
+  if (e.FNL) {
+    fr += e.FNL[o];
+    fi += e.FNL[o + g.ngp];
+  }
+  if (!g0) {
+    const double k2 = 2.0 * g.ak2[gi];
+    fr -= k2 * cr;
+    fi -= k2 * ci;
+  } else {
+    fi = 0.0;
+  }
+  if (e.mode == EPI_HPSI) {
+    e.OUT[o] = fr;
+    e.OUT[o + g.ngp] = fi;
+    return;
+  }
+  const double sc = g0 ? e.s2 : e.s1;
+  double nr = sc * fr + e.pre * cr;
+  double ni = g0 ? 0.0 : (e.s1 * fi + e.pre * ci);
+  if (e.mode == EPI_CHEBK || e.mode == EPI_MOMK) {
+    nr -= e.PREV[o];
+    if (!g0) ni -= e.PREV[o + g.ngp];
+  }
+  e.OUT[o] = nr;
+  e.OUT[o + g.ngp] = ni;
+  if (e.ACC) {
+    for (int imu = 0; imu < e.nmu; imu++) {
+      double *A = e.ACC + imu * e.acc_stride;
+      const double a = e.acoef[imu];
+      if (e.acoef0) {
+        const double a0 = e.acoef0[imu];
+        A[o] = a0 * cr + a * nr;
+        A[o + g.ngp] = a0 * ci + a * ni;
+      } else {
+        A[o] += a * nr;
+        A[o + g.ngp] += a * ni;
+      }
+    }
+  }
+  if (e.dots) {
+    const double wr = g0 ? 1.0 : 2.0;
+    const double xr = e.CHI[o], xi = e.CHI[o + g.ngp];
+    dt.d0 += wr * xr * nr + 2.0 * xi * ni;
+    if (e.mode == EPI_MOMK) {
+      dt.d1 += wr * nr * cr + 2.0 * ni * ci;
+      dt.d2 += wr * nr * nr + 2.0 * ni * ni;
+    } else if (e.ndots > 1) {
+      dt.d1 += wr * xr * xr + 2.0 * xi * xi;
+    }
+  }
+}
+
+template <typename T, int N3>
+__global__ void __launch_bounds__(kColThreads)
+kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
+  using C2 = typename CT<T>::type;
+  constexpr int P3 = N3 + 1;
+  __shared__ __align__(16) C2 tw[N3];
+  __shared__ __align__(16) C2 buf[2 * kCPB * P3];
+  __shared__ double red[kColThreads / 32][3];
+  const int tid = threadIdx.x;
+  const int cp0 = blockIdx.x * kCPB;
+  const int cp1 = min(cp0 + kCPB, g.ncp);
+  const int col0 = 2 * cp0;
+  const int ncl = min(2 * cp1, g.ncols) - col0;
+  const int p = e.pair0 + blockIdx.y;
+  const int s1 = 2 * p, s2 = 2 * p + 1;
+  const bool has2 = s2 < e.nstate;
+  const C2 *twg = twp<T>(g, 3);
+  for (int t = tid; t < N3; t += kColThreads) tw[t] = twg[t];
+  const C2 *Xp = X + (size_t)blockIdx.y * N3 * g.ncols_pad;
+  for (int i = tid; i < N3 * ncl; i += kColThreads) {
+    const int r = i / ncl, cl = i - r * ncl;
+    buf[cl * P3 + r] = Xp[(size_t)r * g.ncols_pad + col0 + cl];
+  }
+  __syncthreads();
+  dit<N3, 1, -1>(buf, Lines1{P3}, ncl, tw, tid, kColThreads);
+  Dots2 dt{0.0, 0.0, 0.0};
+  const int warp = tid >> 5, lane = tid & 31;
+  const double invN = e.invN;
+  const bool noise = (e.mode == EPI_NOISE);
+  for (int cp = cp0 + warp; cp < cp1; cp += kColThreads / 32) {
+    const int lc = 2 * (cp - cp0);
+    const bool zc = (cp == g.ncp - 1);
+    const int lm = zc ? lc : lc + 1;
+    const int gs = g.cp_gstart[cp], gc = g.cp_gcount[cp];
+    const int ntot = gc + (zc ? 1 : 0);
+    for (int en = lane; en < ntot; en += 32) {
+      if (en < gc) {
+        const int gi = gs + en;
+        const int kc = g.gkc[gi];
+        const int kd = kc < 0 ? kc + N3 : kc;
+        const int km = kc > 0 ? N3 - kc : -kc;
+        const C2 F = buf[lc * P3 + kd], Fm = buf[lm * P3 + km];
+        const double tr = (double)F.x * invN, ti = (double)F.y * invN;
+        const double trc = (double)Fm.x * invN, tic = (double)Fm.y * invN;
+        double f1r, f1i, f2r, f2i;
+        if (!noise) {
+          f1r = -(2.0 * (tr + trc));
+          f1i = -(2.0 * (ti - tic));
+          f2r = -(2.0 * (ti + tic));
+          f2i = -(2.0 * (-tr + trc));
+        } else {
+          f1r = -0.5 * (tr + trc);
+          f1i = -0.5 * (ti - tic);
+          f2r = -0.5 * (ti + tic);
+          f2i = -0.5 * (trc - tr);
+        }
+        epilogue2(g, e, s1, gi, false, f1r, f1i, dt);
+        if (has2) epilogue2(g, e, s2, gi, false, f2r, f2i, dt);
+      } else {
+        const int g0 = g.ncoef - 1;
+        const C2 F = buf[lc * P3];
+        const double tr = (double)F.x * invN, ti = (double)F.y * invN;
+        const double m = noise ? -1.0 : -2.0;
+        epilogue2(g, e, s1, g0, true, m * tr, 0.0, dt);
+        if (has2) epilogue2(g, e, s2, g0, true, m * ti, 0.0, dt);
+      }
+    }
+  }
+  if (e.dots) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      dt.d0 += __shfl_down_sync(0xffffffffu, dt.d0, off);
+      dt.d1 += __shfl_down_sync(0xffffffffu, dt.d1, off);
+      dt.d2 += __shfl_down_sync(0xffffffffu, dt.d2, off);
+    }
+    if (lane == 0) { red[warp][0] = dt.d0; red[warp][1] = dt.d1; red[warp][2] = dt.d2; }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 0.0, c = 0.0;
+      for (int w = 0; w < kColThreads / 32; w++) { a += red[w][0]; b += red[w][1]; c += red[w][2]; }
+      double *dst = e.dots + ((size_t)p * g.nbatch + blockIdx.x) * 3;
+      dst[0] = a; dst[1] = b; dst[2] = c;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plane stages
+// ---------------------------------------------------------------------------
+template <typename T> struct PlaneCfg;
+template <> struct PlaneCfg<double> { static constexpr int NT = 512, MINB = 1; };
+template <> struct PlaneCfg<float> { static constexpr int NT = 256, MINB = 3; };
+
+// natural row ka -> line index helper for the rows touched by the sphere
+template <int N1> struct RowsPerm {  // rows given in permuted-a order
+  int kamax, ls;
+  __device__ __forceinline__ int base(int l) const {
+    const int ka = (l <= kamax) ? l : N1 - (2 * kamax + 1) + l;
+    return pos<N1>(ka) * ls;
+  }
+};
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
+kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict__ Vp) {
+  using C2 = typename CT<T>::type;
+  constexpr int NT = PlaneCfg<T>::NT, P2 = N2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *tw1 = reinterpret_cast<C2 *>(smem_raw);
+  C2 *tw2 = tw1 + N1;
+  C2 *pl = tw2 + N2;
+  const int tid = threadIdx.x;
+  const int r = blockIdx.x;
+  {
+    const C2 *t1 = twp<T>(g, 1), *t2 = twp<T>(g, 2);
+    for (int t = tid; t < N1; t += NT) tw1[t] = t1[t];
+    for (int t = tid; t < N2; t += NT) tw2[t] = t2[t];
+  }
+  for (int i = tid; i < N1 * P2; i += NT) pl[i] = cmk<C2>(0.0, 0.0);
+  __syncthreads();
+  C2 *Xrow = X + ((size_t)blockIdx.y * g.n3 + r) * g.ncols_pad;
+  for (int col = tid; col < g.ncols; col += NT) {
+    const int ab = g.col_ab[col];
+    pl[(ab >> 16) * P2 + (ab & 0xffff)] = Xrow[col];
+  }
+  __syncthreads();
+  const int ka = g.kamax;
+  const Lines2 rows{ka + 1, P2, (N1 - ka) * P2};
+  dif<N2, 1, +1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
+  dif<N1, P2, +1>(pl, Lines1{1}, N2, tw1, tid, NT);
+  const T *Vpl = Vp + (size_t)r * N1 * N2;
+  for (int e = tid; e < N1 * N2; e += NT) {
+    const int pa = e / N2, pb = e - pa * N2;
+    C2 v = pl[pa * P2 + pb];
+    const T w = Vpl[e];
+    v.x *= w; v.y *= w;
+    pl[pa * P2 + pb] = v;
+  }
+  __syncthreads();
+  dit<N1, P2, -1>(pl, Lines1{1}, N2, tw1, tid, NT);
+  dit<N2, 1, -1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
+  for (int col = tid; col < g.ncols; col += NT) {
+    const int ab = g.col_ab[col];
+    Xrow[col] = pl[(ab >> 16) * P2 + (ab & 0xffff)];
+  }
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
+kf_stage_b_density(DevGeom g, const typename CT<T>::type *__restrict__ X, double *__restrict__ rho_pair,
+                   int r3_1, int r3_2) {
+  using C2 = typename CT<T>::type;
+  constexpr int NT = PlaneCfg<T>::NT, P2 = N2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *tw1 = reinterpret_cast<C2 *>(smem_raw);
+  C2 *tw2 = tw1 + N1;
+  C2 *pl = tw2 + N2;
+  const int tid = threadIdx.x;
+  const int r = blockIdx.x;
+  const int ic = (r % r3_2) * r3_1 + r / r3_2;
+  {
+    const C2 *t1 = twp<T>(g, 1), *t2 = twp<T>(g, 2);
+    for (int t = tid; t < N1; t += NT) tw1[t] = t1[t];
+    for (int t = tid; t < N2; t += NT) tw2[t] = t2[t];
+  }
+  for (int i = tid; i < N1 * P2; i += NT) pl[i] = cmk<C2>(0.0, 0.0);
+  __syncthreads();
+  const C2 *Xrow = X + ((size_t)blockIdx.y * g.n3 + r) * g.ncols_pad;
+  for (int col = tid; col < g.ncols; col += NT) {
+    const int ab = g.col_ab[col];
+    pl[(ab >> 16) * P2 + (ab & 0xffff)] = Xrow[col];
+  }
+  __syncthreads();
+  const int ka = g.kamax;
+  dif<N2, 1, +1>(pl, Lines2{ka + 1, P2, (N1 - ka) * P2}, 2 * ka + 1, tw2, tid, NT);
+  dif<N1, P2, +1>(pl, Lines1{1}, N2, tw1, tid, NT);
+  double *out = rho_pair + (size_t)blockIdx.y * g.N + (size_t)ic * N1 * N2;
+  for (int e = tid; e < N1 * N2; e += NT) {
+    const int ib = e / N1, ia = e - ib * N1;
+    const C2 v = pl[pos<N1>(ia) * P2 + pos<N2>(ib)];
+    out[e] = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+  }
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
+kf_stage_b_noise(DevGeom g, const unsigned char *__restrict__ neg, int nstate, int pair0,
+                 typename CT<T>::type *__restrict__ X, int r3_1, int r3_2) {
+  using C2 = typename CT<T>::type;
+  constexpr int NT = PlaneCfg<T>::NT, P2 = N2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2 *tw1 = reinterpret_cast<C2 *>(smem_raw);
+  C2 *tw2 = tw1 + N1;
+  C2 *pl = tw2 + N2;
+  const int tid = threadIdx.x;
+  const int r = blockIdx.x;
+  const int ic = (r % r3_2) * r3_1 + r / r3_2;
+  const int p = pair0 + blockIdx.y;
+  const int s1 = 2 * p, s2 = 2 * p + 1;
+  const bool has2 = s2 < nstate;
+  {
+    const C2 *t1 = twp<T>(g, 1), *t2 = twp<T>(g, 2);
+    for (int t = tid; t < N1; t += NT) tw1[t] = t1[t];
+    for (int t = tid; t < N2; t += NT) tw2[t] = t2[t];
+  }
+  const double rv = sqrt((double)g.N);
+  constexpr int E = N1 * N2;
+  const unsigned char *n1p = neg + (size_t)s1 * g.N + (size_t)ic * E;
+  const unsigned char *n2p = neg + (size_t)s2 * g.N + (size_t)ic * E;
+  for (int e = tid; e < E; e += NT) {
+    const int ib = e / N1, ia = e - ib * N1;
+    const double v1 = n1p[e] ? -rv : rv;
+    const double v2 = has2 ? (n2p[e] ? -rv : rv) : 0.0;
+    pl[ia * P2 + ib] = cmk<C2>(v1, v2);
+  }
+  __syncthreads();
+  const int ka = g.kamax;
+  dif<N1, P2, -1>(pl, Lines1{1}, N2, tw1, tid, NT);
+  dif<N2, 1, -1>(pl, RowsPerm<N1>{ka, P2}, 2 * ka + 1, tw2, tid, NT);
+  C2 *Xrow = X + ((size_t)blockIdx.y * g.n3 + r) * g.ncols_pad;
+  for (int col = tid; col < g.ncols; col += NT) {
+    const int ab = g.col_ab[col];
+    Xrow[col] = pl[pos<N1>(ab >> 16) * P2 + pos<N2>(ab & 0xffff)];
+  }
+}
+
+// V_KS in the permuted plane order: Vp[r][pa][pb] = v[(ia*n2+ib)*n3+ic]
+// with ia = ipos_N1(pa), ib = ipos_N2(pb), ic = ipos_N3(r).
+template <typename T, int N1, int N2, int N3>
+__global__ void kf_vks_perm(const double *__restrict__ v, T *__restrict__ Vp) {
+  const size_t N = (size_t)N1 * N2 * N3;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const int pb = (int)(i % N2);
+    const int pa = (int)((i / N2) % N1);
+    const int r = (int)(i / ((size_t)N1 * N2));
+    const int ia = ipos<N1>(pa), ib = ipos<N2>(pb), ic = ipos<N3>(r);
+    Vp[i] = (T)v[((size_t)ia * N2 + ib) * N3 + ic];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+template <int N> static constexpr int r1_of() { return Plan<N>::R1; }
+
+template <typename T> static size_t pl_smem(int n1, int n2) {
+  return sizeof(typename CT<T>::type) * (size_t)(n1 + n2 + n1 * (n2 + 1));
+}
+
+#define SDFT_FOR_N3(X)                \
+  switch (g.n3) {                     \
+    case 24: X(24); break;            \
+    case 48: X(48); break;            \
+    case 72: X(72); break;            \
+    case 96: X(96); break;            \
+    default: return false;            \
+  }
+
+#define SDFT_FOR_PLANE(X)                                             \
+  do {                                                                \
+    const int key = g.n1 * 1000 + g.n2;                               \
+    switch (key) {                                                    \
+      case 24024: X(24, 24); break;                                   \
+      case 24048: X(24, 48); break;                                   \
+      case 24072: X(24, 72); break;                                   \
+      case 48024: X(48, 24); break;                                   \
+      case 48048: X(48, 48); break;                                   \
+      case 48072: X(48, 72); break;                                   \
+      case 72024: X(72, 24); break;                                   \
+      case 72048: X(72, 48); break;                                   \
+      case 72072: X(72, 72); break;                                   \
+      case 96096: X(96, 96); break;                                   \
+      default: return false;                                          \
+    }                                                                 \
+  } while (0)
+
+bool fast_supported(int n1, int n2, int n3) {
+  auto ok = [](int n) { return n == 24 || n == 48 || n == 72 || n == 96; };
+  if (!ok(n1) || !ok(n2) || !ok(n3)) return false;
+  const int key = n1 * 1000 + n2;
+  switch (key) {
+    case 24024: case 24048: case 24072: case 48024: case 48048: case 48072:
+    case 72024: case 72048: case 72072: case 96096: return true;
+    default: return false;
+  }
+}
+
+static void plan3(int n3, int &r1, int &r2) {
+  switch (n3) {
+    case 24: r1 = Plan<24>::R1; r2 = Plan<24>::R2; break;
+    case 48: r1 = Plan<48>::R1; r2 = Plan<48>::R2; break;
+    case 72: r1 = Plan<72>::R1; r2 = Plan<72>::R2; break;
+    default: r1 = Plan<96>::R1; r2 = Plan<96>::R2; break;
+  }
+}
+
+template <typename T>
+bool fast_stage_a(const DevGeom &g, const double *C, int nstate, int pair0, int npairs, void *X, cudaStream_t st) {
+  dim3 grid(g.nbatch, npairs);
+#define LA(N) kf_stage_a<T, N><<<grid, kColThreads, 0, st>>>(g, C, nstate, pair0, (typename CT<T>::type *)X)
+  SDFT_FOR_N3(LA);
+#undef LA
+  return true;
+}
+
+template <typename T>
+bool fast_stage_c(const DevGeom &g, const void *X, const EpiArgs &e, int npairs, cudaStream_t st) {
+  dim3 grid(g.nbatch, npairs);
+#define LC(N) kf_stage_c<T, N><<<grid, kColThreads, 0, st>>>(g, (const typename CT<T>::type *)X, e)
+  SDFT_FOR_N3(LC);
+#undef LC
+  return true;
+}
+
+template <typename T>
+bool fast_stage_b(const DevGeom &g, void *X, const T *Vp, int npairs, cudaStream_t st) {
+  dim3 grid(g.n3, npairs);
+  const size_t sm = pl_smem<T>(g.n1, g.n2);
+#define LB(A, B)                                                                               \
+  do {                                                                                         \
+    auto k = kf_stage_b<T, A, B>;                                                              \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);             \
+    k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, (typename CT<T>::type *)X, Vp);                    \
+  } while (0)
+  SDFT_FOR_PLANE(LB);
+#undef LB
+  return true;
+}
+
+template <typename T>
+bool fast_stage_b_density(const DevGeom &g, const void *X, int npairs, double *rho_pair, cudaStream_t st) {
+  dim3 grid(g.n3, npairs);
+  const size_t sm = pl_smem<T>(g.n1, g.n2);
+  int r1, r2;
+  plan3(g.n3, r1, r2);
+#define LD(A, B)                                                                               \
+  do {                                                                                         \
+    auto k = kf_stage_b_density<T, A, B>;                                                      \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);             \
+    k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, (const typename CT<T>::type *)X, rho_pair, r1, r2); \
+  } while (0)
+  SDFT_FOR_PLANE(LD);
+#undef LD
+  return true;
+}
+
+template <typename T>
+bool fast_stage_b_noise(const DevGeom &g, const unsigned char *neg, int nstate, int pair0, int npairs, void *X,
+                        cudaStream_t st) {
+  dim3 grid(g.n3, npairs);
+  const size_t sm = pl_smem<T>(g.n1, g.n2);
+  int r1, r2;
+  plan3(g.n3, r1, r2);
+#define LN(A, B)                                                                                        \
+  do {                                                                                                  \
+    auto k = kf_stage_b_noise<T, A, B>;                                                                 \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                      \
+    k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, neg, nstate, pair0, (typename CT<T>::type *)X, r1, r2);   \
+  } while (0)
+  SDFT_FOR_PLANE(LN);
+#undef LN
+  return true;
+}
+
+template <typename T>
+bool fast_vks_perm(const DevGeom &g, const double *v, T *Vp, cudaStream_t st) {
+  const size_t N = (size_t)g.n1 * g.n2 * g.n3;
+  int blocks = (int)std::min<size_t>((N + 255) / 256, 148 * 16);
+#define LV3(A, B, Cc) kf_vks_perm<T, A, B, Cc><<<blocks, 256, 0, st>>>(v, Vp)
+#define LV(A, B)                                            \
+  do {                                                      \
+    switch (g.n3) {                                         \
+      case 24: LV3(A, B, 24); break;                        \
+      case 48: LV3(A, B, 48); break;                        \
+      case 72: LV3(A, B, 72); break;                        \
+      case 96: LV3(A, B, 96); break;                        \
+      default: return false;                                \
+    }                                                       \
+  } while (0)
+  SDFT_FOR_PLANE(LV);
+#undef LV
+#undef LV3
+  return true;
+}
+
+template bool fast_stage_a<double>(const DevGeom &, const double *, int, int, int, void *, cudaStream_t);
+template bool fast_stage_a<float>(const DevGeom &, const double *, int, int, int, void *, cudaStream_t);
+template bool fast_stage_c<double>(const DevGeom &, const void *, const EpiArgs &, int, cudaStream_t);
+template bool fast_stage_c<float>(const DevGeom &, const void *, const EpiArgs &, int, cudaStream_t);
+template bool fast_stage_b<double>(const DevGeom &, void *, const double *, int, cudaStream_t);
+template bool fast_stage_b<float>(const DevGeom &, void *, const float *, int, cudaStream_t);
+template bool fast_stage_b_density<double>(const DevGeom &, const void *, int, double *, cudaStream_t);
+template bool fast_stage_b_density<float>(const DevGeom &, const void *, int, double *, cudaStream_t);
+template bool fast_stage_b_noise<double>(const DevGeom &, const unsigned char *, int, int, int, void *, cudaStream_t);
+template bool fast_stage_b_noise<float>(const DevGeom &, const unsigned char *, int, int, int, void *, cudaStream_t);
+template bool fast_vks_perm<double>(const DevGeom &, const double *, double *, cudaStream_t);
+template bool fast_vks_perm<float>(const DevGeom &, const double *, float *, cudaStream_t);
+
+}  // namespace sdft

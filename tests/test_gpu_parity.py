@@ -188,3 +188,36 @@ def test_mixed_precision_close_to_fp64(pkg, sys1):
     assert rel_l2(rx, ra) < 1e-5
     cd.close()
     cm.close()
+
+
+@pytest.mark.parametrize("generic", [False, True])
+def test_fast_and_generic_fft_paths(pkg, sys1, o1, generic, monkeypatch):
+    if generic:
+        monkeypatch.setenv("SDFT_GENERIC_FFT", "1")
+    c = _ctx(pkg, sys1, 6)
+    cr, ci = _rand(sys1["ncoef"], 6, 21)
+    a = c.calc_coef_force(cr, ci)
+    b = o1.hpsi(cr, ci)
+    assert rel_l2(np.concatenate(a), np.concatenate(b)) < TOL_H
+    nc = c.genNoiseOrbitalReal(3, seed=4.0)
+    assert rel_l2(np.concatenate(nc), np.concatenate(o1.noise(3, seed=4.0))) < 1e-13
+    rho = c.rhoCalcRealStoHybrid(cr, ci)
+    assert rel_l2(rho, o1.density(cr, ci)) < 1e-12
+    c.close()
+
+
+@pytest.mark.parametrize("grid,strain", [((24, 48, 24), (0.0, 0.0, 0.0)), ((48, 24, 72), (0.01, -0.02, 0.015)),
+                                         ((36, 36, 36), (0.0, 0.0, 0.0))])
+def test_noncubic_and_generic_grids(pkg, wl, grid, strain):
+    s = wl.make_system(1, grid, strain=strain, disp_sigma=0.05, seed=3)
+    c = _ctx(pkg, s, 5)
+    o = O.OracleSys(s)
+    cr, ci = _rand(s["ncoef"], 5, 5)
+    a = c.calc_coef_force(cr, ci)
+    b = o.hpsi(cr, ci)
+    assert rel_l2(np.concatenate(a), np.concatenate(b)) < TOL_H
+    rho = c.rhoCalcRealStoHybrid(cr, ci)
+    assert rel_l2(rho, o.density(cr, ci)) < 1e-12
+    nz = c.genNoiseOrbitalReal(3, seed=9.0)
+    assert rel_l2(np.concatenate(nz), np.concatenate(o.noise(3, seed=9.0))) < 1e-13
+    c.close()

@@ -172,8 +172,45 @@ static bool is_fp64(const sdft_ctx *c) { return c->prec == SDFT_PREC_FP64; }
 
 // Nonlocal projection Z = Pj C and back projection FNL = Bk Z for `nstate`
 // orbitals held in `vec`.
+static int run_kb_tc(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
+  const int K1 = 2 * ctx->ngp;
+  const int N = (nstate + 127) / 128 * 128;
+  {
+    TScope ts(ctx, 7);
+    launch_split_tf32(vec, K1, ctx->d_c_hi, ctx->d_c_lo, K1, nstate, K1, ctx->st);
+    ctx->launches++;
+  }
+  TcGemm g1 = ctx->gm1, g2 = ctx->gm2;
+  g1.N = N; g1.Nst = nstate;
+  g2.N = N; g2.Nst = nstate;
+  // split K so that the projection has >= ~3 waves of CTAs; partials are
+  // summed in FP64
+  const int tiles = (g1.M / 128) * (N / 128);
+  int split = 1;
+  while (tiles * split < 3 * 148 && split < 32 && (size_t)(2 * split) * N * ctx->Ppad <= ctx->tc_part_elems) split *= 2;
+  int r;
+  {
+    TScope ts(ctx, 3);
+    r = run_gemm_tf32x3(g1, split, ctx->d_tc_part, ctx->tc_part_elems, ctx->d_z, ctx->d_z_hi, ctx->d_z_lo,
+                        ctx->d_err, ctx->st);
+    ctx->launches += 2;
+  }
+  if (r) return r;
+  if (want_enl) {
+    launch_enl(ctx->d_z, ctx->Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
+    ctx->launches++;
+  }
+  {
+    TScope ts(ctx, 4);
+    r = run_gemm_tf32x3(g2, 1, nullptr, 0, ctx->d_fnl, nullptr, nullptr, ctx->d_err, ctx->st);
+    ctx->launches++;
+  }
+  return r;
+}
+
 static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
   if (ctx->P == 0) return SDFT_OK;
+  if (ctx->tc) return run_kb_tc(ctx, vec, nstate, want_enl);
   const int spad = (int)rup(nstate, 64);
   const int K1 = 2 * ctx->ngp;
   // split K of the projection so that >= ~2 waves of CTAs exist
@@ -471,6 +508,8 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   CKF(cudaMemset(ctx->d_b2, 0, vb));
   DMF(ctx->d_dots, (size_t)ctx->npairs_max * g.nbatch * 3 * sizeof(double));
   DMF(ctx->d_enl, sizeof(double));
+  DMF(ctx->d_err, sizeof(int));
+  CKF(cudaMemset(ctx->d_err, 0, sizeof(int)));
   const size_t vsz = is_fp64(ctx) ? sizeof(double) : sizeof(float);
   DMF(ctx->d_vp, (size_t)ctx->N * vsz);
   DMF(ctx->d_vks_tmp, (size_t)ctx->N * sizeof(double));
@@ -487,7 +526,9 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
   void *ptrs[] = {ctx->d_cp_gstart, ctx->d_cp_gcount, ctx->d_col_ab, ctx->d_gkc, ctx->d_ak2, ctx->d_tw,
                   ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
                   ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
-                  ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_enl};
+                  ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_enl,
+                  ctx->d_err, ctx->d_pj_hi, ctx->d_pj_lo, ctx->d_bk_hi, ctx->d_bk_lo, ctx->d_c_hi, ctx->d_c_lo,
+                  ctx->d_z_hi, ctx->d_z_lo, ctx->d_tc_part};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : ctx->tev_pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
@@ -563,6 +604,9 @@ extern "C" int sdft_sync(sdft_ctx *ctx) {
   cudaSetDevice(ctx->device);
   CK(cudaStreamSynchronize(ctx->st));
   CK(cudaGetLastError());
+  int e = 0;
+  CK(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
   return SDFT_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <vector>
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
+#include "sdft_gemm_tc.cuh"
 
 struct sdft_ctx {
   int device = 0;
@@ -55,6 +56,14 @@ struct sdft_ctx {
   long long dev_bytes = 0;
   double gcut = 0.0;
   bool fast = false;  // compile-time-edge FFT kernels available
+  // mixed precision KB GEMMs (TF32x3 tensor cores)
+  bool tc = false;
+  int s_tc = 0;                    // orbital rows of the TF32 operands (multiple of 128)
+  float *d_pj_hi = nullptr, *d_pj_lo = nullptr, *d_bk_hi = nullptr, *d_bk_lo = nullptr;
+  float *d_c_hi = nullptr, *d_c_lo = nullptr, *d_z_hi = nullptr, *d_z_lo = nullptr, *d_tc_part = nullptr;
+  size_t tc_part_elems = 0;
+  sdft::TcGemm gm1{}, gm2{};
+  int *d_err = nullptr;
   // per-kind event timing (sdft_ctx_set_timing)
   bool timing = false;
   struct TEv { int kind; cudaEvent_t a, b; };

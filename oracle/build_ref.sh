@@ -1,0 +1,27 @@
+#!/bin/bash
+# Compile the reference's own hot-path C sources (read in place from the
+# reference tree, never copied) plus oracle/ref_harness.c into
+# oracle/_ref/libpinyref.so.  Test infrastructure only; needs the reference
+# tree, so it runs in the build container and the resulting .so travels.
+set -e
+REF=${SDFT_REFERENCE_DIR:-/root/reference}
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+[ -d "$REF/stodft" ] || { echo "reference tree not found at $REF"; exit 0; }
+mkdir -p "$OUT/obj"
+INC="-I$HERE/ref_stubs -I$REF/include/pentium_nopar -include $HERE/ref_stubs/sdft_ref_protos.h"
+CFLAGS="-O2 -fPIC -w -ffp-contract=off"
+SRCS="stodft/filter.c stodft/normh.c stodft/calc-chempot-chebyshev.c stodft/coeff.c
+      stodft/reduced-energy/energy-wrapper-scf.c stodft/reduced-energy/cp-energy-eext-stodft.c
+      stodft/reduced-energy/cp-energy-ee-rho-stodft.c mathlib/fft_package.c mathlib/fft_create_package.c
+      mathlib/mathlib.c energy/cp/cp_energy_eext_nonloc.c energy/cp/cp_energy_eext.c
+      energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c"
+OBJS=""
+for f in $SRCS; do
+  o="$OUT/obj/$(echo "$f" | tr '/' '_').o"
+  if [ ! -f "$o" ] || [ "$REF/$f" -nt "$o" ]; then gcc -c $CFLAGS $INC "$REF/$f" -o "$o"; fi
+  OBJS="$OBJS $o"
+done
+gcc -c $CFLAGS $INC "$HERE/ref_harness.c" -o "$OUT/obj/ref_harness.o"
+gcc -shared -o "$OUT/libpinyref.so" $OBJS "$OUT/obj/ref_harness.o" -lm
+echo "$OUT/libpinyref.so"

@@ -1,0 +1,126 @@
+"""ctypes binding of oracle/_ref/libpinyref.so: the reference's own C
+sources driven by oracle/ref_harness.c.  TEST INFRASTRUCTURE ONLY."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libpinyref.so")
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+def available():
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB)
+        L.ref_create.restype = C.c_void_p
+        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int, _dp,
+                                 C.c_int, C.c_double, C.c_double, _dp, _dp, C.c_double, C.c_int]
+        L.ref_hpsi.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.ref_filter.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_double,
+                                 C.c_double, _dp, _dp, _dp]
+        L.ref_moments.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp]
+        L.ref_gvec.argtypes = [_dp, C.c_double, _ip, C.c_int, _ip, _ip, _ip, _ip, _ip]
+        L.ref_round_fft.restype = C.c_int
+        L.ref_cheby_coeff.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+        L.ref_newton.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
+        L.ref_gaussran2.argtypes = [C.c_int, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class RefSys:
+    """One system in the reference's own data structures (single type, s+p KB)."""
+
+    def __init__(self, s, nmax):
+        kb = s["kb_desc"]
+        self.ncoef = len(s["ka"])
+        self.keep = [i32(s["ka"]), i32(s["kb"]), i32(s["kc"]), i32(s["ib1"]), i32(s["ib2"]),
+                     f64(np.asarray(s["hmat"], float).T.reshape(9)), f64(s["vks"]), f64(kb["pos"]), f64(kb["vps"]),
+                     f64(kb["vpsnorm"])]
+        ka, kb_, kc, b1, b2, h, v, pos, vps, vn = self.keep
+        self._p = C.c_void_p(lib().ref_create(*s["grid"], self.ncoef, _i(ka), _i(kb_), _i(kc), _i(b1), _i(b2), _d(h),
+                                              _d(v), kb["natm"], _d(pos), kb["nsplin_g"], kb["gmin_spl"],
+                                              kb["dg_spl"], _d(vps), _d(vn), float(kb["gzvps0"][0]), nmax))
+
+    def hpsi(self, cre, cim):
+        cre, cim = f64(cre), f64(cim)
+        fr, fi = np.zeros_like(cre), np.zeros_like(cim)
+        e = C.c_double()
+        lib().ref_hpsi(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e))
+        return fr, fi, e.value
+
+    def filter(self, cheby, cre, cim, ec, nmu, scale, emean, samp=None, moments=False):
+        cre, cim, ec = f64(cre), f64(cim), f64(ec)
+        L = ec.size // nmu
+        sr, si = np.zeros(nmu * cre.size), np.zeros(nmu * cre.size)
+        m = np.zeros(L + 1) if moments else None
+        sp = f64(samp) if samp is not None else None
+        lib().ref_filter(self._p, 1 if cheby else 0, cre.size // self.ncoef, _d(cre), _d(cim), L, nmu, _d(ec),
+                         _d(sp) if sp is not None else None, scale, emean, _d(sr), _d(si),
+                         _d(m) if m is not None else None)
+        out = (sr.reshape(nmu, -1), si.reshape(nmu, -1))
+        return out + (m,) if moments else out
+
+    def moments(self, cre, cim, L, scale, emean):
+        cre, cim = f64(cre), f64(cim)
+        m = np.zeros(L + 1)
+        lib().ref_moments(self._p, cre.size // self.ncoef, _d(cre), _d(cim), L, scale, emean, _d(m))
+        return m
+
+
+def gvec(hmat, ecut, kmax, ncoef):
+    h = f64(np.asarray(hmat, float).T.reshape(9))
+    km = i32(kmax)
+    ka, kb, kc = (np.zeros(ncoef, np.int32) for _ in range(3))
+    b1, b2 = np.zeros(ncoef, np.int32), np.zeros(ncoef, np.int32)
+    lib().ref_gvec(_d(h), ecut, _i(km), ncoef, _i(ka), _i(kb), _i(kc), _i(b1), _i(b2))
+    return ka, kb, kc, b1[:ncoef - 1], b2[:ncoef - 1]
+
+
+def cheby_coeff(L, ediff, emean, beta, mu, fun=2):
+    out = np.zeros(L)
+    lib().ref_cheby_coeff(L, ediff, emean, beta, mu, fun, _d(out))
+    return out
+
+
+def newton(L, scale, emin, beta, mu):
+    s, u, e = np.zeros(L), np.zeros(L), np.zeros(L)
+    lib().ref_newton(L, scale, emin, beta, mu, _d(s), _d(u), _d(e))
+    return s, u, e
+
+
+def gaussran2(n, seed):
+    q = C.c_double(seed)
+    out = np.zeros(max(n, 1))
+    lib().ref_gaussran2(n, C.byref(q), _d(out))
+    return out[:n], q.value
+
+
+def round_fft(n):
+    return lib().ref_round_fft(n)

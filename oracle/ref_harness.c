@@ -1,0 +1,516 @@
+/*
+ * ref_harness.c -- drives the reference's OWN hot-path C sources (compiled
+ * from the read-only reference tree by oracle/build_ref.sh into
+ * oracle/_ref/libpinyref.so).  TEST INFRASTRUCTURE ONLY: used by
+ * tests/test_oracle_pin.py to pin the CPU restatement (sdft_oracle.c).
+ *
+ * What is the reference's code: setkvec3d_sm, calcCoefForceWrapSCF and
+ * everything below it (KB projection / energy / back projection, the
+ * filter-path FFT wrappers, cp_vpsi, kinetic term), normHCheby,
+ * normHNewtonHerm, filterChebyPolyHerm, filterNewtonPolyHerm,
+ * calcChebyMoments, calcChebyCoeff, genSampNewtonHermit,
+ * genCoeffNewtonHermit, gaussran2/ran_essl.
+ * What this file supplies: the PINY data structures filled for one
+ * single-rank, spin-unpolarised system with one atom type and one radial
+ * KB projector per l channel; single-rank MPI wrappers; BLAS ddot/daxpy;
+ * an FP64 DFT behind the FFTW3 API subset the sources call (FFTW is not
+ * installed here); DURAND (Fortran, no Fortran compiler here) restated from
+ * mathlib/blas_wrappers.f:39-69; abort stubs for routines off this path.
+ */
+#include "standard_include.h"
+#include "../typ_defs/typedefs_gen.h"
+#include "../typ_defs/typedefs_class.h"
+#include "../typ_defs/typedefs_bnd.h"
+#include "../typ_defs/typedefs_cp.h"
+#include <time.h>
+
+/* reference prototypes used here */
+void setkvec3d_sm(int, double, int *, double *, int *, int *, int *, int *, int *, double *, double *);
+void calcCoefForceWrapSCF(CLASS *, GENERAL_DATA *, CP *, CPCOEFFS_POS *, CLATOMS_POS *);
+void normHCheby(CP *, CLASS *, GENERAL_DATA *, CPCOEFFS_POS *, CLATOMS_POS *, int, int);
+void normHNewtonHerm(CP *, CLASS *, GENERAL_DATA *, CPCOEFFS_POS *, CLATOMS_POS *, double);
+void filterChebyPolyHerm(CP *, CLASS *, GENERAL_DATA *, int);
+void filterNewtonPolyHerm(CP *, CLASS *, GENERAL_DATA *, int);
+void calcChebyMoments(CP *, CLASS *, GENERAL_DATA *, int);
+void calcChebyCoeff(STODFTINFO *, STODFTCOEFPOS *, double *, double *, int, double);
+void genSampNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
+void genCoeffNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
+int roundFFT(int);
+void gaussran2(int, int *, int *, double *, double[]);
+double fermiExpReal(double, double, double);
+
+/* ====================================================================== */
+/* FFTW3 subset: plain O(N^2)-per-dimension-free mixed radix DFT         */
+/* ====================================================================== */
+struct sdft_fftw_plan_s {
+  int rank, n[3], howmany, istride, idist, sign;
+  fftw_complex *in, *out;
+};
+
+static void dft1(fftw_complex *x, int n, long st, int sign, fftw_complex *tmp) {
+  /* recursive mixed radix on a gathered copy */
+  for (int j = 0; j < n; j++) tmp[j] = x[j * st];
+  /* iterative: naive for small factors via recursion helper */
+  fftw_complex *y = tmp + n;
+  /* decimation: use simple recursive function */
+  extern void sdft_ref_fft_rec(const fftw_complex *, int, int, fftw_complex *, int, fftw_complex *);
+  sdft_ref_fft_rec(tmp, n, 1, y, sign, y + n);
+  for (int j = 0; j < n; j++) x[j * st] = y[j];
+}
+
+void sdft_ref_fft_rec(const fftw_complex *x, int n, int stride, fftw_complex *y, int sign, fftw_complex *scr) {
+  if (n == 1) { y[0] = x[0]; return; }
+  int r = (n % 3 == 0) ? 3 : ((n % 2 == 0) ? 2 : n);
+  int m = n / r;
+  fftw_complex *sub = scr, *nscr = scr + n;
+  for (int q = 0; q < r; q++) sdft_ref_fft_rec(x + q * stride, m, stride * r, sub + q * m, sign, nscr);
+  for (int k = 0; k < m; k++) {
+    fftw_complex v[8];
+    for (int q = 0; q < r; q++) v[q] = sub[q * m + k] * cexp(sign * 2.0 * M_PI * I * (double)(q * k) / n);
+    for (int t = 0; t < r; t++) {
+      fftw_complex a = 0;
+      for (int q = 0; q < r; q++) a += v[q] * cexp(sign * 2.0 * M_PI * I * (double)(q * t) / r);
+      y[k + t * m] = a;
+    }
+  }
+}
+
+static fftw_plan mkplan(int rank, const int *n, int howmany, fftw_complex *in, int istride, int idist,
+                        fftw_complex *out, int sign) {
+  fftw_plan p = calloc(1, sizeof(*p));
+  p->rank = rank;
+  for (int i = 0; i < rank; i++) p->n[i] = n[i];
+  p->howmany = howmany; p->istride = istride; p->idist = idist; p->sign = sign; p->in = in; p->out = out;
+  return p;
+}
+fftw_plan fftw_plan_dft_3d(int n0, int n1, int n2, fftw_complex *in, fftw_complex *out, int sign, unsigned f) {
+  int n[3] = {n0, n1, n2};
+  (void)f;
+  return mkplan(3, n, 1, in, 1, 0, out, sign);
+}
+fftw_plan fftw_plan_dft_1d(int n, fftw_complex *in, fftw_complex *out, int sign, unsigned f) {
+  (void)f;
+  return mkplan(1, &n, 1, in, 1, n, out, sign);
+}
+fftw_plan fftw_plan_many_dft(int rank, const int *n, int howmany, fftw_complex *in, const int *ie, int is, int id,
+                             fftw_complex *out, const int *oe, int os, int od, int sign, unsigned f) {
+  (void)ie; (void)oe; (void)os; (void)od; (void)f;
+  return mkplan(rank, n, howmany, in, is, id, out, sign);
+}
+static void exec(const fftw_plan p, fftw_complex *in, fftw_complex *out) {
+  int nmax = 1;
+  for (int i = 0; i < p->rank; i++) nmax = p->n[i] > nmax ? p->n[i] : nmax;
+  fftw_complex *tmp = malloc(sizeof(fftw_complex) * nmax * 16);
+  if (p->rank == 3) {
+    int n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
+    long N = (long)n0 * n1 * n2;
+    if (out != in) memcpy(out, in, sizeof(fftw_complex) * N);
+    for (long a = 0; a < (long)n0 * n1; a++) dft1(out + a * n2, n2, 1, p->sign, tmp);
+    for (int a = 0; a < n0; a++)
+      for (int c = 0; c < n2; c++) dft1(out + (long)a * n1 * n2 + c, n1, n2, p->sign, tmp);
+    for (long bc = 0; bc < (long)n1 * n2; bc++) dft1(out + bc, n0, (long)n1 * n2, p->sign, tmp);
+  } else {
+    int n = p->n[0];
+    for (int h = 0; h < p->howmany; h++) {
+      /* many_dft with data given as interleaved doubles through the reference's
+         1-based zfft pointers: in == out in every call on this path */
+      fftw_complex *b = out + (long)h * p->idist;
+      if (out != in) memcpy(b, in + (long)h * p->idist, sizeof(fftw_complex) * n);  /* contiguous only */
+      dft1(b, n, p->istride, p->sign, tmp);
+    }
+  }
+  free(tmp);
+}
+void fftw_execute(const fftw_plan p) { exec(p, p->in, p->out); }
+void fftw_execute_dft(const fftw_plan p, fftw_complex *in, fftw_complex *out) { exec(p, in, out); }
+void fftw_destroy_plan(fftw_plan p) { free(p); }
+void *fftw_malloc(size_t n) { return malloc(n); }
+void fftw_free(void *p) { free(p); }
+int fftw_init_threads(void) { return 1; }
+void fftw_plan_with_nthreads(int n) { (void)n; }
+void fftw_cleanup_threads(void) {}
+
+/* ====================================================================== */
+/* OpenMP / MKL / MPI single-rank stand-ins                              */
+/* ====================================================================== */
+double omp_get_wtime(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+void omp_set_num_threads(int n) { (void)n; }
+int omp_get_thread_num(void) { return 0; }
+int omp_get_num_threads(void) { return 1; }
+int omp_get_max_threads(void) { return 1; }
+void omp_set_max_active_levels(int n) { (void)n; }
+void mkl_set_num_threads(int n) { (void)n; }
+void mkl_set_dynamic(int n) { (void)n; }
+
+static void sdft_ref_abort(const char *f) {
+  fprintf(stderr, "reference harness: off-path routine %s called\n", f);
+  abort();
+}
+#define ABORT_STUB(name) \
+  void name(void) { sdft_ref_abort(#name); }
+ABORT_STUB(Allgather) ABORT_STUB(Allgatherv) ABORT_STUB(Allreduce) ABORT_STUB(Alltoall) ABORT_STUB(Alltoallv)
+ABORT_STUB(Finalize) ABORT_STUB(Gatherv) ABORT_STUB(Reduce) ABORT_STUB(Reduce_scatter) ABORT_STUB(Scatterv)
+ABORT_STUB(Bcast) ABORT_STUB(DGEMV) ABORT_STUB(DSYMV) ABORT_STUB(dsysv_) ABORT_STUB(rs_)
+ABORT_STUB(calcChemPotInterp) ABORT_STUB(calcCoefForceWrap) ABORT_STUB(coef_force_calc_hybrid_threads_state)
+ABORT_STUB(coef_force_tau_fun_full_g) ABORT_STUB(coef_force_tau_fun_hybrid)
+ABORT_STUB(controlEnergyNlppRealThreads) ABORT_STUB(controlPotentialEnergyFilter) ABORT_STUB(control_contract_rho)
+ABORT_STUB(control_grad_rho) ABORT_STUB(control_nonloc_gh) ABORT_STUB(control_spread_rho)
+ABORT_STUB(cp_condiag_ksmat) ABORT_STUB(cp_rotate_vector) ABORT_STUB(dcfftb_generic_) ABORT_STUB(dcfftf_generic_)
+ABORT_STUB(dcffti_generic_) ABORT_STUB(excpot_pade_lda) ABORT_STUB(excpot_pade_lsda) ABORT_STUB(excpot_pw_lda)
+ABORT_STUB(excpot_pw_lsda) ABORT_STUB(excpot_pz_lda) ABORT_STUB(excpot_pz_lsda) ABORT_STUB(genDensityMix)
+ABORT_STUB(getnl_fcoef_gh) ABORT_STUB(getnl_pot_pv_fatm_gh) ABORT_STUB(grad_corr_lda) ABORT_STUB(grad_corr_lsda)
+ABORT_STUB(cfopen)
+void Barrier(int c) { (void)c; }
+
+/* BLAS level-1 used by the filter/moment code (mathlib/mathlib.c:518-570) */
+double ddot_(int *n, double *x, int *incx, double *y, int *incy) {
+  double s = 0.0;
+  for (int i = 0; i < *n; i++) s += x[i * *incx] * y[i * *incy];
+  return s;
+}
+void daxpy_(int *n, double *a, double *x, int *incx, double *y, int *incy) {
+  for (int i = 0; i < *n; i++) y[i * *incy] += *a * x[i * *incx];
+}
+/* DURAND, mathlib/blas_wrappers.f:39-69 (Park-Miller in FP64) */
+void durand_(double *seed, int *n, double *x, int *ierr) {
+  const double XM = 16807.0, XMP = 16807.0000078263692557811737060546875, SCALEU = 2147483648.0,
+               SCALED = 4.656612873077392578125e-10, ONEPEP = 1.0000000004656612873077392578125,
+               ONEMEP = 0.9999999995343387126922607421875;
+  *ierr = 0;
+  if (*n < 0 || *seed < 1.0 || *seed > 2147483646.0) { *ierr = 1; return; }
+  double t = *seed * SCALED;
+  for (int j = 0; j < *n; j++) {
+    double s = trunc(t * XMP);
+    t = t * XM;
+    t = t - s * ONEMEP;
+    x[j] = t * ONEPEP;
+  }
+  *seed = t * SCALEU;
+}
+
+/* ====================================================================== */
+/* PINY data structures for one system                                    */
+/* ====================================================================== */
+typedef struct {
+  CP cp;
+  CLASS cls;
+  GENERAL_DATA gd;
+  CPCOEFFS_POS cpos;
+  CLATOMS_POS apos;
+  STODFTINFO sinfo;
+  STODFTCOEFPOS scoef;
+  NEWTONINFO newton;
+  CHEBYSHEVINFO cheby;
+  int ncoef, N, nmax, natm;
+  fftw_complex *fin, *fout, *bin, *bout;
+  fftw_plan pfwd, pbwd;
+  fftw_complex *fin_arr[1], *fout_arr[1], *bin_arr[1], *bout_arr[1];
+  fftw_plan pfwd_arr[1], pbwd_arr[1];
+} RefSys;
+
+static double *d1(long n) { return (double *)calloc(n + 2, sizeof(double)); }  /* 1-based ready */
+static int *i1(long n) { return (int *)calloc(n + 2, sizeof(int)); }
+
+RefSys *ref_create(int n1, int n2, int n3, int ncoef, const int *ka, const int *kb, const int *kc, const int *ib1,
+                   const int *ib2, const double *hmat, const double *vks, int natm, const double *pos, int nsplin,
+                   double gmin, double dg, const double *vps /*[2][4][nsplin]*/, const double *vpsnorm /*[2]*/,
+                   double gzvps0, int nmax) {
+  RefSys *r = calloc(1, sizeof(RefSys));
+  CP *cp = &r->cp;
+  CLASS *cl = &r->cls;
+  GENERAL_DATA *gd = &r->gd;
+  const int N = n1 * n2 * n3, nk = ncoef - 1;
+  r->ncoef = ncoef; r->N = N; r->nmax = nmax; r->natm = natm;
+  /* cell: hmat / hmati 1-based column-major; CP box = full box */
+  CELL *cell = &gd->cell;
+  double hi[9];
+  {
+    const double *h = hmat;
+    double det = h[0] * (h[4] * h[8] - h[7] * h[5]) - h[3] * (h[1] * h[8] - h[7] * h[2]) + h[6] * (h[1] * h[5] - h[4] * h[2]);
+    hi[0] = (h[4] * h[8] - h[5] * h[7]) / det; hi[3] = (h[5] * h[6] - h[3] * h[8]) / det; hi[6] = (h[3] * h[7] - h[4] * h[6]) / det;
+    hi[1] = (h[7] * h[2] - h[1] * h[8]) / det; hi[4] = (h[0] * h[8] - h[2] * h[6]) / det; hi[7] = (h[1] * h[6] - h[0] * h[7]) / det;
+    hi[2] = (h[1] * h[5] - h[2] * h[4]) / det; hi[5] = (h[2] * h[3] - h[0] * h[5]) / det; hi[8] = (h[0] * h[4] - h[1] * h[3]) / det;
+  }
+  cell->hmat = d1(9); cell->hmati = d1(9); cell->hmat_cp = d1(9); cell->hmati_cp = d1(9);
+  for (int i = 0; i < 9; i++) {
+    cell->hmat[i + 1] = cell->hmat_cp[i + 1] = hmat[i];
+    cell->hmati[i + 1] = cell->hmati_cp[i + 1] = hi[i];
+  }
+  cell->cp_box_center = d1(3); cell->cp_box_center_rel = d1(3);
+  cell->iperd = 3;
+  gd->ptens.pvten_tmp = d1(9);
+  /* options / info */
+  cp->cpopts.cp_lsda = 0; cp->cpopts.cp_dual_grid_opt = 0; cp->cpopts.cp_ptens_calc = 0; cp->cpopts.cp_hess_calc = 0;
+  cp->cpcoeffs_info.ncoef = ncoef;
+  cp->cpcoeffs_info.nstate_up_proc = nmax; cp->cpcoeffs_info.nstate_up = nmax;
+  cp->communicate.myid_state = 0; cp->communicate.np_states = 1; cp->communicate.numThreads = 1;
+  cp->communicate.np_forc = 1;
+  /* coefficients */
+  r->cpos.cre_up = d1((long)nmax * ncoef); r->cpos.cim_up = d1((long)nmax * ncoef);
+  r->cpos.fcre_up = d1((long)nmax * ncoef); r->cpos.fcim_up = d1((long)nmax * ncoef);
+  r->cpos.icoef_orth_up = 1;
+  cp->cpcoeffs_pos = &r->cpos;
+  cl->clatoms_pos = &r->apos;
+  /* k vectors (1-based) */
+  CPEWALD *ew = &cp->cpewald;
+  ew->nktot_sm = nk;
+  ew->kastr_sm = i1(ncoef); ew->kbstr_sm = i1(ncoef); ew->kcstr_sm = i1(ncoef);
+  ew->ibrk1_sm = i1(ncoef); ew->ibrk2_sm = i1(ncoef);
+  ew->ak2_sm = d1(ncoef); ew->ak2Kinetic = d1(ncoef);
+  for (int i = 0; i < ncoef; i++) {
+    ew->kastr_sm[i + 1] = ka[i]; ew->kbstr_sm[i + 1] = kb[i]; ew->kcstr_sm[i + 1] = kc[i];
+  }
+  for (int i = 0; i < nk; i++) { ew->ibrk1_sm[i + 1] = ib1[i]; ew->ibrk2_sm[i + 1] = ib2[i]; }
+  ew->fftw3dFlag = 1;
+  ew->eCutoffKe = -1.0;
+  {
+    double tpi = 2.0 * M_PI;
+    for (int i = 1; i <= nk; i++) {
+      double a = ew->kastr_sm[i], b = ew->kbstr_sm[i], c = ew->kcstr_sm[i];
+      double *h = cell->hmati_cp;
+      double xk = (a * h[1] + b * h[2] + c * h[3]) * tpi, yk = (a * h[4] + b * h[5] + c * h[6]) * tpi,
+             zk = (a * h[7] + b * h[8] + c * h[9]) * tpi;
+      ew->ak2_sm[i] = ew->ak2Kinetic[i] = xk * xk + yk * yk + zk * zk; /* get_ak2_sm, no cap */
+    }
+  }
+  /* V_KS (1-based, filter layout) */
+  cp->cpscr.cpscr_rho.v_ks_up = d1(N);
+  memcpy(&cp->cpscr.cpscr_rho.v_ks_up[1], vks, sizeof(double) * N);
+  cp->cpscr.cpscr_wave.zfft = d1(2 * (long)N + 2);
+  cp->cpscr.cpscr_wave.zfft_tmp = d1(2 * (long)N + 2);
+  /* filter FFT package */
+  PARA_FFT_PKG3D *pk = &cp->cp_sclr_fft_pkg3d_sm;
+  pk->nkf1 = n1; pk->nkf2 = n2; pk->nkf3 = n3;
+  pk->nfft = 2 * N; pk->nfft_proc = 2 * N; pk->ncoef = ncoef; pk->num_proc = 1; pk->ncoef_proc = ncoef;
+  pk->ncoef_use = ncoef - 1; pk->igeneric_opt = 0; pk->numThreads = 1;
+  pk->mapFFTW = i1(ncoef); pk->mapConFFTW = i1(ncoef); pk->mapFFTWFilter = i1(ncoef); pk->mapConFFTWFilter = i1(ncoef);
+  for (int i = 0; i < nk; i++) { /* setfft_indx, mathlib/fft_create_package.c:981 */
+    int a = ka[i], b = kb[i], c = kc[i];
+    int kap = (a < 0 ? a + n1 + 1 : a + 1), kbp = (b < 0 ? b + n2 + 1 : b + 1), kcp = (c < 0 ? c + n3 + 1 : c + 1);
+    pk->mapFFTW[i + 1] = kcp * 2 - 1 + (kbp - 1) * 2 * n3 + (kap - 1) * 2 * n3 * n2;
+    kap = (-a < 0 ? -a + n1 + 1 : -a + 1); kbp = (-b < 0 ? -b + n2 + 1 : -b + 1); kcp = (-c < 0 ? -c + n3 + 1 : -c + 1);
+    pk->mapConFFTW[i + 1] = kcp * 2 - 1 + (kbp - 1) * 2 * n3 + (kap - 1) * 2 * n3 * n2;
+  }
+  pk->mapFFTW[ncoef] = 1; pk->mapConFFTW[ncoef] = 0;
+  for (int i = 1; i <= ncoef; i++) {
+    pk->mapFFTWFilter[i] = (pk->mapFFTW[i] - 1) / 2;
+    pk->mapConFFTWFilter[i] = (pk->mapConFFTW[i] - 1) / 2;
+  }
+  r->fin = calloc(N, sizeof(fftw_complex)); r->fout = calloc(N, sizeof(fftw_complex));
+  r->bin = calloc(N, sizeof(fftw_complex)); r->bout = calloc(N, sizeof(fftw_complex));
+  r->fin_arr[0] = r->fin; r->fout_arr[0] = r->fout; r->bin_arr[0] = r->bin; r->bout_arr[0] = r->bout;
+  r->pfwd_arr[0] = fftw_plan_dft_3d(n1, n2, n3, r->fin, r->fout, FFTW_FORWARD, FFTW_MEASURE);
+  r->pbwd_arr[0] = fftw_plan_dft_3d(n1, n2, n3, r->bin, r->bout, FFTW_BACKWARD, FFTW_MEASURE);
+  pk->fftw3DForwardIn = r->fin_arr; pk->fftw3DForwardOut = r->fout_arr;
+  pk->fftw3DBackwardIn = r->bin_arr; pk->fftw3DBackwardOut = r->bout_arr;
+  pk->fftwPlan3DForward = r->pfwd_arr; pk->fftwPlan3DBackward = r->pbwd_arr;
+  cp->cp_para_fft_pkg3d_lg.ncoef_proc = 0;
+  cp->cp_para_fft_pkg3d_dens_cp_box.ncoef_proc = 0;
+  cp->cpscr.cpscr_loc.vextr = d1(1); cp->cpscr.cpscr_loc.vexti = d1(1);
+  cp->cpscr.cpscr_loc.vextr_loc = d1(1); cp->cpscr.cpscr_loc.vexti_loc = d1(1);
+  /* atoms + KB pseudopotential: one type, s and p, one radial projector */
+  CLATOMS_INFO *ci = &cl->clatoms_info;
+  ci->natm_tot = natm; ci->hess_calc = 0; ci->pi_beads = 1; ci->q = d1(natm);
+  CLATOMS_POS *ap = &r->apos;
+  ap->x = d1(natm); ap->y = d1(natm); ap->z = d1(natm); ap->fx = d1(natm); ap->fy = d1(natm); ap->fz = d1(natm);
+  for (int i = 0; i < natm; i++) { ap->x[i + 1] = pos[3 * i]; ap->y[i + 1] = pos[3 * i + 1]; ap->z[i + 1] = pos[3 * i + 2]; }
+  ATOMMAPS *am = &cl->atommaps;
+  am->natm_typ = 1;
+  am->iatm_atm_typ = i1(natm); am->iatm_atm_typ_nl = i1(natm); am->iatm_atm_typ_nl_rev = i1(natm);
+  am->imap_atm_typ_nl = i1(2);
+  for (int i = 1; i <= natm; i++) am->iatm_atm_typ[i] = am->iatm_atm_typ_nl[i] = am->iatm_atm_typ_nl_rev[i] = 1;
+  am->imap_atm_typ_nl[1] = 1;
+  PSEUDO *ps = &cp->pseudo;
+  ps->n_ang_max = 1; ps->n_ang_max_kb = 1; ps->n_ang_max_gh = 0; ps->n_rad_max = 1; ps->natm_typ_nl = 1;
+  ps->np_nl = i1(4); ps->np_nl_gh = i1(4);
+  ps->np_nl[1] = natm; ps->np_nl[2] = natm;
+  ps->np_nonloc_cp_box_kb = natm; ps->np_nonloc_cp_box_gh = 0;
+  ps->ip_nl = i1(natm); ps->ip_nl_rev = i1(2 * natm + 2);
+  for (int i = 1; i <= natm; i++) { ps->ip_nl[i] = i; ps->ip_nl_rev[i] = i; ps->ip_nl_rev[i + natm] = i; }
+  ps->nrad_max_l = i1(4); ps->nrad_max_l[1] = 1; ps->nrad_max_l[2] = 1;
+  ps->np_nl_rad_str = (int **)calloc(4, sizeof(int *));
+  for (int l = 1; l <= 3; l++) { ps->np_nl_rad_str[l] = i1(2); ps->np_nl_rad_str[l][1] = 1; }
+  ps->nsplin_g = nsplin; ps->gmin_spl = gmin; ps->dg_spl = dg;
+  ps->vps0 = d1(2 * nsplin); ps->vps1 = d1(2 * nsplin); ps->vps2 = d1(2 * nsplin); ps->vps3 = d1(2 * nsplin);
+  ps->dvps0 = d1(2 * nsplin); ps->dvps1 = d1(2 * nsplin); ps->dvps2 = d1(2 * nsplin); ps->dvps3 = d1(2 * nsplin);
+  for (int l = 0; l < 2; l++)
+    for (int i = 0; i < nsplin; i++) {
+      ps->vps0[1 + l * nsplin + i] = vps[(l * 4 + 0) * nsplin + i];
+      ps->vps1[1 + l * nsplin + i] = vps[(l * 4 + 1) * nsplin + i];
+      ps->vps2[1 + l * nsplin + i] = vps[(l * 4 + 2) * nsplin + i];
+      ps->vps3[1 + l * nsplin + i] = vps[(l * 4 + 3) * nsplin + i];
+    }
+  ps->vpsnorm = d1(2); ps->vpsnorm[1] = vpsnorm[0]; ps->vpsnorm[2] = vpsnorm[1];
+  ps->gzvps0 = d1(1); ps->gzvps0[1] = gzvps0; ps->gzvps = d1(1);
+  ps->pseudoReal.pseudoRealFlag = 0;
+  /* nonlocal scratch: ntot = nstate * np_nlmax * nlm * nrad */
+  long ntot = (long)nmax * natm * 4 + 2;
+  CPSCR_NONLOC *nl = &cp->cpscr.cpscr_nonloc;
+  nl->vnlre_up = d1(ntot); nl->vnlim_up = d1(ntot);
+  nl->dvnlre_x_up = d1(ntot); nl->dvnlre_y_up = d1(ntot); nl->dvnlre_z_up = d1(ntot);
+  nl->dvnlim_x_up = d1(ntot); nl->dvnlim_y_up = d1(ntot); nl->dvnlim_z_up = d1(ntot);
+  EWD_SCR *es = &cl->ewd_scr;
+  long na = natm + 4;
+  es->cossc = d1(na); es->sinsc = d1(na); es->helr = d1(na); es->heli = d1(na); es->fx2 = d1(na); es->fy2 = d1(na);
+  es->fz2 = d1(na); es->vtemp_now = d1(na); es->q = d1(na); es->x = d1(na); es->y = d1(na); es->z = d1(na);
+  es->fx = d1(na); es->fy = d1(na); es->fz = d1(na); es->helr_now = d1(na); es->heli_now = d1(na); es->temp = d1(na);
+  cl->for_scr.iexcl = i1(na);
+  /* stochastic DFT info */
+  cp->stodftInfo = &r->sinfo;
+  cp->stodftCoefPos = &r->scoef;
+  r->sinfo.newtonInfo = &r->newton;
+  r->sinfo.chebyshevInfo = &r->cheby;
+  r->sinfo.filterFlag = 1;
+  r->sinfo.numThreads = 1;
+  r->sinfo.fermiFunctionReal = fermiExpReal;
+  r->scoef.stoWfUpRe = (double **)calloc(8, sizeof(double *));
+  r->scoef.stoWfUpIm = (double **)calloc(8, sizeof(double *));
+  return r;
+}
+
+void ref_destroy(RefSys *r) { (void)r; /* process-lifetime test object */ }
+
+static void load_states(RefSys *r, int ns, const double *re, const double *im) {
+  r->cp.cpcoeffs_info.nstate_up_proc = ns;
+  r->cp.cpcoeffs_info.nstate_up = ns;
+  memcpy(&r->cpos.cre_up[1], re, sizeof(double) * ns * r->ncoef);
+  memcpy(&r->cpos.cim_up[1], im, sizeof(double) * ns * r->ncoef);
+}
+
+int ref_hpsi(RefSys *r, int ns, const double *re, const double *im, double *fre, double *fim, double *enl) {
+  load_states(r, ns, re, im);
+  r->gd.stat_avg.cp_enl = 0.0;
+  calcCoefForceWrapSCF(&r->cls, &r->gd, &r->cp, &r->cpos, &r->apos);
+  memcpy(fre, &r->cpos.fcre_up[1], sizeof(double) * ns * r->ncoef);
+  memcpy(fim, &r->cpos.fcim_up[1], sizeof(double) * ns * r->ncoef);
+  if (enl) *enl = r->gd.stat_avg.cp_enl;
+  return 0;
+}
+
+static void set_poly(RefSys *r, int L, int nmu, const double *ec, double scale, double emean, int cheby) {
+  STODFTINFO *si = &r->sinfo;
+  si->polynormLength = L;
+  si->numChemPot = nmu;
+  si->energyMean = emean;
+  si->expanType = cheby ? 1 : 2;
+  r->cheby.scale = scale; r->cheby.Smin = -1.0; r->cheby.Smax = 1.0;
+  r->newton.scale = scale; r->newton.Smin = -2.0; r->newton.Smax = 2.0;
+  r->scoef.expanCoeff = (double *)ec;
+}
+
+int ref_filter(RefSys *r, int cheby, int ns, const double *re, const double *im, int L, int nmu, const double *ec,
+               const double *samp, double scale, double emean, double *out_re, double *out_im, double *moments) {
+  load_states(r, ns, re, im);
+  set_poly(r, L, nmu, ec, scale, emean, cheby);
+  for (int imu = 0; imu < nmu; imu++) {
+    r->scoef.stoWfUpRe[imu] = d1((long)ns * r->ncoef);
+    r->scoef.stoWfUpIm[imu] = d1((long)ns * r->ncoef);
+  }
+  if (cheby) {
+    r->sinfo.storeChebyMomentsFlag = moments ? 1 : 0;
+    filterChebyPolyHerm(&r->cp, &r->cls, &r->gd, 0);
+    if (moments) memcpy(moments, r->scoef.chebyMomentsUp, sizeof(double) * L);
+  } else {
+    r->newton.sampPoint = (void *)samp;
+    filterNewtonPolyHerm(&r->cp, &r->cls, &r->gd, 0);
+  }
+  for (int imu = 0; imu < nmu; imu++) {
+    memcpy(out_re + (long)imu * ns * r->ncoef, &r->scoef.stoWfUpRe[imu][1], sizeof(double) * ns * r->ncoef);
+    memcpy(out_im + (long)imu * ns * r->ncoef, &r->scoef.stoWfUpIm[imu][1], sizeof(double) * ns * r->ncoef);
+    free(r->scoef.stoWfUpRe[imu]);
+    free(r->scoef.stoWfUpIm[imu]);
+  }
+  return 0;
+}
+
+/* calcChebyMoments draws its noise through genNoiseOrbitalReal; the
+ * harness supplies that routine and hands it the injected chi. */
+static const double *g_inj_re, *g_inj_im;
+static int g_inj_n;
+void genNoiseOrbitalReal(CP *cp, CPCOEFFS_POS *pos) {
+  (void)cp;
+  memcpy(&pos->cre_up[1], g_inj_re, sizeof(double) * g_inj_n);
+  memcpy(&pos->cim_up[1], g_inj_im, sizeof(double) * g_inj_n);
+}
+
+int ref_moments(RefSys *r, int ns, const double *re, const double *im, int L, double scale, double emean,
+                double *moments) {
+  load_states(r, ns, re, im);
+  g_inj_re = re; g_inj_im = im; g_inj_n = ns * r->ncoef;
+  set_poly(r, L, 1, NULL, scale, emean, 1);
+  r->sinfo.numChebyMoments = (L % 2 == 0) ? (L / 2 + 1) : ((L + 1) / 2);
+  r->scoef.chebyMomentsUp = d1(L + 1);
+  calcChebyMoments(&r->cp, &r->cls, &r->gd, 0);
+  memcpy(moments, r->scoef.chebyMomentsUp, sizeof(double) * (L + 1));
+  return 0;
+}
+
+/* --- host pieces ------------------------------------------------------- */
+int ref_gvec(const double *hmat, double ecut, const int *kmax, int cap, int *ka, int *kb, int *kc, int *ib1, int *ib2) {
+  double h[10], hi[10], gmin, gmax;
+  double det = hmat[0] * (hmat[4] * hmat[8] - hmat[7] * hmat[5]) - hmat[3] * (hmat[1] * hmat[8] - hmat[7] * hmat[2]) +
+               hmat[6] * (hmat[1] * hmat[5] - hmat[4] * hmat[2]);
+  (void)h;
+  hi[1] = (hmat[4] * hmat[8] - hmat[5] * hmat[7]) / det; hi[4] = (hmat[5] * hmat[6] - hmat[3] * hmat[8]) / det;
+  hi[7] = (hmat[3] * hmat[7] - hmat[4] * hmat[6]) / det; hi[2] = (hmat[7] * hmat[2] - hmat[1] * hmat[8]) / det;
+  hi[5] = (hmat[0] * hmat[8] - hmat[2] * hmat[6]) / det; hi[8] = (hmat[1] * hmat[6] - hmat[0] * hmat[7]) / det;
+  hi[3] = (hmat[1] * hmat[5] - hmat[2] * hmat[4]) / det; hi[6] = (hmat[2] * hmat[3] - hmat[0] * hmat[5]) / det;
+  hi[9] = (hmat[0] * hmat[4] - hmat[1] * hmat[3]) / det;
+  int km[4] = {0, kmax[0], kmax[1], kmax[2]};
+  int nk = cap - 1;
+  int *a = i1(cap), *b = i1(cap), *c = i1(cap), *b1 = i1(cap), *b2 = i1(cap);
+  setkvec3d_sm(nk, ecut, km, hi, a, b, c, b1, b2, &gmin, &gmax);
+  for (int i = 0; i < cap; i++) { ka[i] = a[i + 1]; kb[i] = b[i + 1]; kc[i] = c[i + 1]; }
+  for (int i = 0; i < nk; i++) { ib1[i] = b1[i + 1]; ib2[i] = b2[i + 1]; }
+  free(a); free(b); free(c); free(b1); free(b2);
+  return 0;
+}
+
+int ref_round_fft(int n) { return roundFFT(n); }
+
+int ref_cheby_coeff(int L, double ediff, double emean, double beta, double mu, int fun, double *out) {
+  STODFTINFO si;
+  STODFTCOEFPOS sc;
+  CHEBYSHEVINFO ch;
+  memset(&si, 0, sizeof si); memset(&sc, 0, sizeof sc); memset(&ch, 0, sizeof ch);
+  si.chebyshevInfo = &ch;
+  si.polynormLength = L;
+  si.energyDiff = ediff;
+  si.energyMean = emean;
+  si.beta = beta;
+  si.fermiFunctionReal = fermiExpReal;
+  si.numChebyGrid = roundFFT(32 * L);
+  sc.funValGridFFT = fftw_malloc(sizeof(fftw_complex) * si.numChebyGrid);
+  sc.chebyCoeffsFFT = fftw_malloc(sizeof(fftw_complex) * si.numChebyGrid);
+  si.fftwPlanForward = fftw_plan_dft_1d(si.numChebyGrid, sc.funValGridFFT, sc.chebyCoeffsFFT, FFTW_FORWARD, 0);
+  calcChebyCoeff(&si, &sc, &mu, out, fun, 0.0);
+  fftw_destroy_plan(si.fftwPlanForward);
+  fftw_free(sc.funValGridFFT); fftw_free(sc.chebyCoeffsFFT);
+  return 0;
+}
+
+int ref_newton(int L, double scale, double emin, double beta, double mu, double *samp, double *unsc, double *ec) {
+  STODFTINFO si;
+  STODFTCOEFPOS sc;
+  NEWTONINFO nw;
+  memset(&si, 0, sizeof si); memset(&sc, 0, sizeof sc); memset(&nw, 0, sizeof nw);
+  si.newtonInfo = &nw;
+  si.polynormLength = L; si.numChemPot = 1; si.numThreads = 1; si.energyMin = emin; si.beta = beta;
+  si.fermiFunctionReal = fermiExpReal;
+  nw.Smin = -2.0; nw.Smax = 2.0; nw.scale = scale;
+  nw.sampPoint = samp; nw.sampPointUnscale = unsc;
+  sc.expanCoeff = ec;
+  sc.chemPot = &mu;
+  genSampNewtonHermit(&si, &sc);
+  genCoeffNewtonHermit(&si, &sc);
+  return 0;
+}
+
+void ref_gaussran2(int n, double *seed, double *out) {
+  int is = 0;
+  gaussran2(n, &is, &is, seed, out);
+}

@@ -1,0 +1,107 @@
+"""Pin the CPU oracle (sdft_oracle.c) to the reference's own C code.
+
+oracle/_ref/libpinyref.so is built by oracle/build_ref.sh from the
+reference sources (filter.c, normh.c, energy-wrapper-scf.c,
+cp-energy-eext-stodft.c, cp-energy-ee-rho-stodft.c, cp_energy_eext_nonloc.c,
+fft_package.c, coeff.c, calc-chempot-chebyshev.c, mathlib.c, set_cp_ewald.c,
+...) and driven through PINY's own data structures by oracle/ref_harness.c.
+The committed golden fixtures (tests/golden/) carry the same pins where the
+reference tree is absent."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import oracle as O
+from oracle import ref as R
+
+pytestmark = pytest.mark.skipif(not R.available(), reason="reference-compiled oracle (oracle/_ref) not built")
+
+
+@pytest.fixture(scope="module")
+def both(sys1):
+    return R.RefSys(sys1, 8), O.OracleSys(sys1)
+
+
+def _rand(nc, ns, seed):
+    rng = np.random.default_rng(seed)
+    cr = rng.standard_normal(ns * nc)
+    ci = rng.standard_normal(ns * nc)
+    ci.reshape(ns, nc)[:, -1] = 0.0
+    return cr, ci
+
+
+def test_gvec_pinned(wl, sys1, sys2):
+    for s in (sys1, sys2):
+        ka, kb, kc, b1, b2 = R.gvec(s["hmat"], wl.ECUT_HA, [20, 20, 20], s["ncoef"])
+        for x, y in ((ka, s["ka"]), (kb, s["kb"]), (kc, s["kc"]), (b1, s["ib1"]), (b2, s["ib2"])):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("ns", [1, 4, 5])
+def test_hpsi_pinned(both, sys1, ns):
+    r, o = both
+    cr, ci = _rand(sys1["ncoef"], ns, ns)
+    fr, fi, e = r.hpsi(cr, ci)
+    gr, gi, ge = o.hpsi(cr, ci, want_enl=True)
+    assert rel_l2(np.concatenate([gr, gi]), np.concatenate([fr, fi])) < 1e-14
+    assert abs(ge - e) < 1e-13 * abs(e)
+
+
+def test_filter_cheby_pinned(pkg, both, sys1):
+    r, o = both
+    cr, ci = _rand(sys1["ncoef"], 5, 3)
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    ec = np.stack([pkg.calcChebyCoeff(20, emax - emin, em, 1000.0, mu) for mu in (0.2, 0.35)], axis=1).ravel()
+    a = r.filter(True, cr, ci, ec, 2, scale, em, moments=True)
+    b = o.filter_cheby(cr, ci, ec, 2, scale, em, store_moments=True)
+    for k in range(2):
+        assert rel_l2(np.concatenate([b[0][k], b[1][k]]), np.concatenate([a[0][k], a[1][k]])) < 1e-13
+    assert rel_l2(b[2][:20], a[2][:20]) < 1e-13
+
+
+def test_filter_newton_pinned(pkg, both, sys1):
+    r, o = both
+    cr, ci = _rand(sys1["ncoef"], 4, 5)
+    emin, emax = -1.0, 45.0
+    scale = 4.0 / (emax - emin)
+    samp, unsc = pkg.genSampNewtonHermit(24, -2.0, 2.0, scale, emin)
+    ec = pkg.genCoeffNewtonHermit(24, 0.2, 1000.0, samp, unsc)
+    a = r.filter(False, cr, ci, ec, 1, scale, 0.5 * (emin + emax), samp=samp)
+    b = o.filter_newton(cr, ci, ec, samp, 1, scale, 0.5 * (emin + emax))
+    assert rel_l2(np.concatenate([b[0][0], b[1][0]]), np.concatenate([a[0][0], a[1][0]])) < 1e-13
+
+
+@pytest.mark.parametrize("L", [12, 17])
+def test_moments_pinned(both, sys1, L):
+    r, o = both
+    cr, ci = _rand(sys1["ncoef"], 3, 9)
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    a = r.moments(cr, ci, L, scale, em)
+    b = o.moments(cr, ci, L, scale, em)
+    M = L // 2 + 1 if L % 2 == 0 else (L + 1) // 2
+    n = 2 * M - 1  # entries written by calcChebyMoments
+    assert rel_l2(b[:n], a[:n]) < 1e-13
+
+
+def test_coefficients_pinned(pkg):
+    for n in (64 * 32, 256 * 32, 512 * 32, 1000):
+        assert R.round_fft(n) == O.round_fft(n) == pkg.roundFFT(n)
+    for L, fun in ((64, 1), (128, 2)):
+        a = R.cheby_coeff(L, 40.0, 19.0, 1000.0, 0.2, fun)
+        assert np.allclose(O.cheby_coeff(L, 40.0, 19.0, 1000.0, 0.2, fun), a, rtol=0, atol=1e-14)
+        assert np.allclose(pkg.calcChebyCoeff(L, 40.0, 19.0, 1000.0, 0.2, fun_flag=fun), a, rtol=0, atol=1e-13)
+    for L in (16, 64):
+        s, u, e = R.newton(L, 4.0 / 40.0, -0.5, 1000.0, 0.2)
+        s2, u2 = O.newton_samp(L, -2.0, 2.0, 4.0 / 40.0, -0.5)
+        assert np.array_equal(s, s2) and np.array_equal(u, u2)
+        assert np.array_equal(e, O.newton_coeff(L, 0.2, 1000.0, s2, u2))
+
+
+def test_gaussran2_pinned(pkg):
+    for seed in (10.0, 3.7e10, 123456.75):
+        a, qa = R.gaussran2(2001, seed)
+        b, qb = O.gaussran2(2001, seed)
+        c, qc = pkg.gaussran2(2001, seed)
+        assert np.array_equal(a, b) and np.array_equal(a, c) and qa == qb == qc

@@ -15,11 +15,16 @@ SRCS="stodft/filter.c stodft/normh.c stodft/calc-chempot-chebyshev.c stodft/coef
       stodft/reduced-energy/energy-wrapper-scf.c stodft/reduced-energy/cp-energy-eext-stodft.c
       stodft/reduced-energy/cp-energy-ee-rho-stodft.c mathlib/fft_package.c mathlib/fft_create_package.c
       mathlib/mathlib.c energy/cp/cp_energy_eext_nonloc.c energy/cp/cp_energy_eext.c
-      energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c"
+      energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c
+      stodft/density.c stodft/gen-noise.c"
 OBJS=""
 for f in $SRCS; do
   o="$OUT/obj/$(echo "$f" | tr '/' '_').o"
-  if [ ! -f "$o" ] || [ "$REF/$f" -nt "$o" ]; then gcc -c $CFLAGS $INC "$REF/$f" -o "$o"; fi
+  # the harness injects noise into calcChebyMoments through genNoiseOrbitalReal,
+  # so the reference's own generator is compiled under another name
+  EXTRA=""
+  [ "$f" = "stodft/gen-noise.c" ] && EXTRA="-DgenNoiseOrbitalReal=ref_genNoiseOrbitalReal"
+  if [ ! -f "$o" ] || [ "$REF/$f" -nt "$o" ]; then gcc -c $CFLAGS $EXTRA $INC "$REF/$f" -o "$o"; fi
   OBJS="$OBJS $o"
 done
 gcc -c $CFLAGS $INC "$HERE/ref_harness.c" -o "$OUT/obj/ref_harness.o"

@@ -34,6 +34,8 @@ def lib():
         L.ref_cheby_coeff.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
         L.ref_newton.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.ref_gaussran2.argtypes = [C.c_int, _dp, _dp]
+        L.ref_noise.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
+        L.ref_density.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -60,6 +62,7 @@ class RefSys:
     def __init__(self, s, nmax):
         kb = s["kb_desc"]
         self.ncoef = len(s["ka"])
+        self.N = int(np.prod(s["grid"]))
         self.keep = [i32(s["ka"]), i32(s["kb"]), i32(s["kc"]), i32(s["ib1"]), i32(s["ib2"]),
                      f64(np.asarray(s["hmat"], float).T.reshape(9)), f64(s["vks"]), f64(kb["pos"]), f64(kb["vps"]),
                      f64(kb["vpsnorm"])]
@@ -86,6 +89,18 @@ class RefSys:
                          _d(m) if m is not None else None)
         out = (sr.reshape(nmu, -1), si.reshape(nmu, -1))
         return out + (m,) if moments else out
+
+    def noise(self, nstate, seed=10.0):
+        re = np.zeros(nstate * self.ncoef)
+        im = np.zeros(nstate * self.ncoef)
+        lib().ref_noise(self._p, nstate, seed, _d(re), _d(im))
+        return re, im
+
+    def density(self, cre, cim):
+        cre, cim = f64(cre), f64(cim)
+        rho = np.zeros(self.N)
+        lib().ref_density(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(rho))
+        return rho
 
     def moments(self, cre, cim, L, scale, emean):
         cre, cim = f64(cre), f64(cim)

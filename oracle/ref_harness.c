@@ -25,6 +25,12 @@
 #include <time.h>
 
 /* reference prototypes used here */
+void create_para_fft_pkg3d(PARA_FFT_PKG3D *, int *, int *, int *, int);
+void para_fft_gen3d_init(PARA_FFT_PKG3D *);
+void ref_genNoiseOrbitalReal(CP *, CPCOEFFS_POS *);
+void rhoCalcRealStoHybrid(CPSCR *, CPCOEFFS_INFO *, CELL *, STODFTINFO *, double *, double *, double *, int, int,
+                          int, int, int, COMMUNICATE *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *,
+                          PARA_FFT_PKG3D *, PARA_FFT_PKG3D *);
 void setkvec3d_sm(int, double, int *, double *, int *, int *, int *, int *, int *, double *, double *);
 void calcCoefForceWrapSCF(CLASS *, GENERAL_DATA *, CP *, CPCOEFFS_POS *, CLATOMS_POS *);
 void normHCheby(CP *, CLASS *, GENERAL_DATA *, CPCOEFFS_POS *, CLATOMS_POS *, int, int);
@@ -282,32 +288,20 @@ RefSys *ref_create(int n1, int n2, int n3, int ncoef, const int *ka, const int *
   memcpy(&cp->cpscr.cpscr_rho.v_ks_up[1], vks, sizeof(double) * N);
   cp->cpscr.cpscr_wave.zfft = d1(2 * (long)N + 2);
   cp->cpscr.cpscr_wave.zfft_tmp = d1(2 * (long)N + 2);
-  /* filter FFT package */
+  /* FFT package built by the reference itself (create_para_fft_pkg3d +
+     para_fft_gen3d_init, mathlib/fft_create_package.c:41,1571): filter maps,
+     3-D FFTW plans and the generic pencil transforms */
   PARA_FFT_PKG3D *pk = &cp->cp_sclr_fft_pkg3d_sm;
-  pk->nkf1 = n1; pk->nkf2 = n2; pk->nkf3 = n3;
-  pk->nfft = 2 * N; pk->nfft_proc = 2 * N; pk->ncoef = ncoef; pk->num_proc = 1; pk->ncoef_proc = ncoef;
-  pk->ncoef_use = ncoef - 1; pk->igeneric_opt = 0; pk->numThreads = 1;
-  pk->mapFFTW = i1(ncoef); pk->mapConFFTW = i1(ncoef); pk->mapFFTWFilter = i1(ncoef); pk->mapConFFTWFilter = i1(ncoef);
-  for (int i = 0; i < nk; i++) { /* setfft_indx, mathlib/fft_create_package.c:981 */
-    int a = ka[i], b = kb[i], c = kc[i];
-    int kap = (a < 0 ? a + n1 + 1 : a + 1), kbp = (b < 0 ? b + n2 + 1 : b + 1), kcp = (c < 0 ? c + n3 + 1 : c + 1);
-    pk->mapFFTW[i + 1] = kcp * 2 - 1 + (kbp - 1) * 2 * n3 + (kap - 1) * 2 * n3 * n2;
-    kap = (-a < 0 ? -a + n1 + 1 : -a + 1); kbp = (-b < 0 ? -b + n2 + 1 : -b + 1); kcp = (-c < 0 ? -c + n3 + 1 : -c + 1);
-    pk->mapConFFTW[i + 1] = kcp * 2 - 1 + (kbp - 1) * 2 * n3 + (kap - 1) * 2 * n3 * n2;
-  }
-  pk->mapFFTW[ncoef] = 1; pk->mapConFFTW[ncoef] = 0;
-  for (int i = 1; i <= ncoef; i++) {
-    pk->mapFFTWFilter[i] = (pk->mapFFTW[i] - 1) / 2;
-    pk->mapConFFTWFilter[i] = (pk->mapConFFTW[i] - 1) / 2;
-  }
-  r->fin = calloc(N, sizeof(fftw_complex)); r->fout = calloc(N, sizeof(fftw_complex));
-  r->bin = calloc(N, sizeof(fftw_complex)); r->bout = calloc(N, sizeof(fftw_complex));
-  r->fin_arr[0] = r->fin; r->fout_arr[0] = r->fout; r->bin_arr[0] = r->bin; r->bout_arr[0] = r->bout;
-  r->pfwd_arr[0] = fftw_plan_dft_3d(n1, n2, n3, r->fin, r->fout, FFTW_FORWARD, FFTW_MEASURE);
-  r->pbwd_arr[0] = fftw_plan_dft_3d(n1, n2, n3, r->bin, r->bout, FFTW_BACKWARD, FFTW_MEASURE);
-  pk->fftw3DForwardIn = r->fin_arr; pk->fftw3DForwardOut = r->fout_arr;
-  pk->fftw3DBackwardIn = r->bin_arr; pk->fftw3DBackwardOut = r->bout_arr;
-  pk->fftwPlan3DForward = r->pfwd_arr; pk->fftwPlan3DBackward = r->pbwd_arr;
+  pk->comm = 0; pk->num_proc = 1; pk->myid = 0;
+  pk->nktot = nk; pk->ncoef = ncoef; pk->nkf1 = n1; pk->nkf2 = n2; pk->nkf3 = n3;
+  pk->threadFlag = 2; pk->igeneric_opt = 0; pk->numThreads = 1; pk->numThreadsFFTW3 = 1;
+  create_para_fft_pkg3d(pk, ew->kastr_sm, ew->kbstr_sm, ew->kcstr_sm, 0);
+  para_fft_gen3d_init(pk);
+  cp->cp_sclr_fft_pkg3d_lg = *pk;
+  cp->cp_para_fft_pkg3d_lg.nfft = pk->nfft;
+  cp->cp_para_fft_pkg3d_lg.nfft_proc = pk->nfft_proc;
+  r->sinfo.fragInfo = (FRAGINFO *)calloc(1, sizeof(FRAGINFO));
+  r->sinfo.randSeedTot = d1(2);
   cp->cp_para_fft_pkg3d_lg.ncoef_proc = 0;
   cp->cp_para_fft_pkg3d_dens_cp_box.ncoef_proc = 0;
   cp->cpscr.cpscr_loc.vextr = d1(1); cp->cpscr.cpscr_loc.vexti = d1(1);
@@ -507,6 +501,31 @@ int ref_newton(int L, double scale, double emin, double beta, double mu, double 
   sc.chemPot = &mu;
   genSampNewtonHermit(&si, &sc);
   genCoeffNewtonHermit(&si, &sc);
+  return 0;
+}
+
+/* genNoiseOrbitalReal (stodft/gen-noise.c:162) of the reference */
+int ref_noise(RefSys *r, int ns, double seed, double *re, double *im) {
+  r->cp.cpcoeffs_info.nstate_up_proc = ns;
+  r->cp.cpcoeffs_info.nstate_up = ns;
+  r->sinfo.randSeed = seed;
+  ref_genNoiseOrbitalReal(&r->cp, &r->cpos);
+  memcpy(re, &r->cpos.cre_up[1], sizeof(double) * ns * r->ncoef);
+  memcpy(im, &r->cpos.cim_up[1], sizeof(double) * ns * r->ncoef);
+  return 0;
+}
+
+/* rhoCalcRealStoHybrid (stodft/density.c:43): sum_s |psi_s(r)|^2 */
+int ref_density(RefSys *r, int ns, const double *re, const double *im, double *rho) {
+  load_states(r, ns, re, im);
+  double *rs = d1(r->N);
+  CP *cp = &r->cp;
+  rhoCalcRealStoHybrid(&cp->cpscr, &cp->cpcoeffs_info, &r->gd.cell, &r->sinfo, r->cpos.cre_up, r->cpos.cim_up, rs,
+                       0, 1, ns, r->ncoef, 0, &cp->communicate, &cp->cp_para_fft_pkg3d_lg, &cp->cp_sclr_fft_pkg3d_lg,
+                       &cp->cp_para_fft_pkg3d_dens_cp_box, &cp->cp_sclr_fft_pkg3d_dens_cp_box,
+                       &cp->cp_sclr_fft_pkg3d_sm);
+  memcpy(rho, &rs[1], sizeof(double) * r->N);
+  free(rs);
   return 0;
 }
 

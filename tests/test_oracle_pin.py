@@ -105,3 +105,18 @@ def test_gaussran2_pinned(pkg):
         b, qb = O.gaussran2(2001, seed)
         c, qc = pkg.gaussran2(2001, seed)
         assert np.array_equal(a, b) and np.array_equal(a, c) and qa == qb == qc
+
+
+@pytest.mark.parametrize("grid,strain", [((24, 24, 24), (0.0, 0.0, 0.0)), ((24, 48, 24), (0.0, 0.0, 0.0)),
+                                         ((36, 24, 48), (0.01, -0.02, 0.015))])
+def test_noise_and_density_pinned(wl, grid, strain):
+    """genNoiseOrbitalReal (gen-noise.c) and rhoCalcRealStoHybrid
+    (density.c) of the reference against the oracle, cubic and non-cubic."""
+    s = wl.make_system(1, grid, strain=strain)
+    r, o = R.RefSys(s, 6), O.OracleSys(s)
+    a = r.noise(5, 10.0)
+    b = o.noise(5, 10.0)
+    assert rel_l2(np.concatenate(b), np.concatenate(a)) < 1e-14
+    rho_r = r.density(*b)
+    rho_o = o.density(*b)
+    assert rel_l2(rho_o, rho_r) < 1e-14

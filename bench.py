@@ -340,7 +340,7 @@ def run_ours(args):
         "metric": "filtered stochastic orbitals/s (512-atom Si, mixed vs FP64 GPU); p50/p99 latency",
         "value": value, "unit": "orbitals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "mixed(fp32 fft, fp64-dmma kb gemm, fp64 recurrence)" if prec == pkg.SDFT_PREC_MIXED else "f64",
+        "dtype": "mixed(fp32 fft, int8-ozaki kb gemm, fp64 recurrence)" if prec == pkg.SDFT_PREC_MIXED else "f64",
         "data": "synthetic (seeded Si supercell, Gaussian V_loc, Gaussian s+p KB, +-1 noise)",
         "config": {"workload": f"{args.config}: {s['natm']}-atom Si, grid {s['grid'][0]}x{s['grid'][1]}x{s['grid'][2]}, "
                                f"{nsto} orbitals/GPU, Chebyshev L={L}, ncoef={s['ncoef']}, P={s['_P']}",

@@ -44,8 +44,11 @@ extern "C" {
 
 /* ---- precision modes ------------------------------------------------- */
 #define SDFT_PREC_FP64  0      /* everything FP64 (plain form)               */
-#define SDFT_PREC_MIXED 1      /* FP32 FFT + V multiply, TF32x3 KB GEMM,
-                                  FP64 recurrence / accumulators / reductions */
+#define SDFT_PREC_MIXED 1      /* FP32 FFT + V multiply, KB GEMMs on INT8
+                                  tensor cores in the Ozaki digit scheme
+                                  (about 28-bit operands, exact products and
+                                  sums), FP64 recurrence / accumulators /
+                                  reductions */
 
 typedef struct sdft_ctx sdft_ctx;
 

@@ -118,7 +118,7 @@ static int build_columns(sdft_ctx *ctx, std::vector<int> &cp_gstart, std::vector
 }
 
 static int ensure_x(sdft_ctx *ctx, int npairs) {
-  const size_t csz = ctx->prec == SDFT_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t csz = ctx->fft64 ? sizeof(double2) : sizeof(float2);
   const size_t need = (size_t)npairs * ctx->n3 * ctx->cols.ncols_pad * csz;
   if (need <= ctx->x_bytes) return SDFT_OK;
   if (ctx->d_x) { cudaFree(ctx->d_x); ctx->dev_bytes -= (long long)ctx->x_bytes; ctx->d_x = nullptr; }
@@ -168,41 +168,43 @@ static int download_block(sdft_ctx *ctx, const double *src, int nstate, double *
   return SDFT_OK;
 }
 
-static bool is_fp64(const sdft_ctx *c) { return c->prec == SDFT_PREC_FP64; }
+static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 
 // Nonlocal projection Z = Pj C and back projection FNL = Bk Z for `nstate`
-// orbitals held in `vec`.
-static int run_kb_tc(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
-  const int K1 = 2 * ctx->ngp;
+// orbitals held in `vec`, mixed precision: INT8 Ozaki GEMMs on the digit
+// form of the orbitals; Z = Pj C is split over K with FP64 partial sums, the
+// reduction also produces the digit form of Z for FNL = Bk Z.
+static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
+  const int K1 = 2 * ctx->ngp, S = ctx->s_oz, Ppad = ctx->Ppad;
   const int N = (nstate + 127) / 128 * 128;
   {
     TScope ts(ctx, 7);
-    launch_split_tf32(vec, K1, ctx->d_c_hi, ctx->d_c_lo, K1, nstate, K1, ctx->st);
-    ctx->launches++;
+    launch_oz_slice_rows(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,
+                         ctx->d_c_sc, ctx->st);
+    ctx->launches += 2;
   }
-  TcGemm g1 = ctx->gm1, g2 = ctx->gm2;
+  OzGemm g1 = ctx->om1, g2 = ctx->om2;
   g1.N = N; g1.Nst = nstate;
   g2.N = N; g2.Nst = nstate;
-  // split K so that the projection has >= ~3 waves of CTAs; partials are
-  // summed in FP64
-  const int tiles = (g1.M / 128) * (N / 128);
-  int split = 1;
-  while (tiles * split < 3 * 148 && split < 32 && (size_t)(2 * split) * N * ctx->Ppad <= ctx->tc_part_elems) split *= 2;
+  const size_t stride = (size_t)N * Ppad;
+  const int max_split = (int)std::min<size_t>(32, ctx->oz_part_elems / stride);
+  const int split = oz_choose_split((Ppad / 128) * (N / 128), ctx->kp_oz / 64, max_split);
   int r;
   {
     TScope ts(ctx, 3);
-    r = run_gemm_tf32x3(g1, split, ctx->d_tc_part, ctx->tc_part_elems, ctx->d_z, ctx->d_z_hi, ctx->d_z_lo,
-                        ctx->d_err, ctx->st);
+    r = run_gemm_oz(g1, split, ctx->d_oz_part, stride, ctx->d_err, ctx->st);
+    if (r) return r;
+    launch_oz_reduce_slice(ctx->d_oz_part, split, stride, Ppad, ctx->P, nstate, ctx->d_z, ctx->d_z_dig,
+                           (size_t)S * Ppad, ctx->d_z_sc, ctx->st);
     ctx->launches += 2;
   }
-  if (r) return r;
   if (want_enl) {
-    launch_enl(ctx->d_z, ctx->Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
+    launch_enl(ctx->d_z, Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
     ctx->launches++;
   }
   {
     TScope ts(ctx, 4);
-    r = run_gemm_tf32x3(g2, 1, nullptr, 0, ctx->d_fnl, nullptr, nullptr, ctx->d_err, ctx->st);
+    r = run_gemm_oz(g2, 1, ctx->d_fnl, 0, ctx->d_err, ctx->st);
     ctx->launches++;
   }
   return r;
@@ -210,7 +212,7 @@ static int run_kb_tc(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
 
 static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
   if (ctx->P == 0) return SDFT_OK;
-  if (ctx->tc) return run_kb_tc(ctx, vec, nstate, want_enl);
+  if (ctx->oz) return run_kb_oz(ctx, vec, nstate, want_enl);
   const int spad = (int)rup(nstate, 64);
   const int K1 = 2 * ctx->ngp;
   // split K of the projection so that >= ~2 waves of CTAs exist
@@ -427,6 +429,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   auto fail = [&](int code) { sdft_ctx_destroy(ctx); return code; };
   ctx->device = device;
   ctx->prec = precision;
+  ctx->fft64 = (precision == SDFT_PREC_FP64);
   ctx->n1 = n1; ctx->n2 = n2; ctx->n3 = n3;
   ctx->N = n1 * n2 * n3;
   ctx->ncoef = ncoef;
@@ -527,8 +530,9 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
                   ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
                   ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_enl,
-                  ctx->d_err, ctx->d_pj_hi, ctx->d_pj_lo, ctx->d_bk_hi, ctx->d_bk_lo, ctx->d_c_hi, ctx->d_c_lo,
-                  ctx->d_z_hi, ctx->d_z_lo, ctx->d_tc_part};
+                  ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
+                  ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
+                  ctx->d_oz_part};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &t : ctx->tev_pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }

@@ -4,7 +4,7 @@
 #include <vector>
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
-#include "sdft_gemm_tc.cuh"
+#include "sdft_gemm_oz.cuh"
 
 struct sdft_ctx {
   int device = 0;
@@ -56,13 +56,17 @@ struct sdft_ctx {
   long long dev_bytes = 0;
   double gcut = 0.0;
   bool fast = false;  // compile-time-edge FFT kernels available
-  // mixed precision KB GEMMs (TF32x3 tensor cores)
-  bool tc = false;
-  int s_tc = 0;                    // orbital rows of the TF32 operands (multiple of 128)
-  float *d_pj_hi = nullptr, *d_pj_lo = nullptr, *d_bk_hi = nullptr, *d_bk_lo = nullptr;
-  float *d_c_hi = nullptr, *d_c_lo = nullptr, *d_z_hi = nullptr, *d_z_lo = nullptr, *d_tc_part = nullptr;
-  size_t tc_part_elems = 0;
-  sdft::TcGemm gm1{}, gm2{};
+  bool fft64 = true;  // FFT scratch / V_KS in FP64 (plain form)
+  // mixed precision KB GEMMs (Ozaki scheme on INT8 tensor cores)
+  bool oz = false;
+  int s_oz = 0;                                   // orbital rows of the digit arrays (multiple of 128)
+  int kp_oz = 0;                                  // K1 rounded up to 64 (digit row pitch)
+  int8_t *d_pj_dig = nullptr, *d_bk_dig = nullptr, *d_c_dig = nullptr, *d_z_dig = nullptr;
+  double *d_pj_sc = nullptr, *d_bk_sc = nullptr, *d_c_sc = nullptr, *d_z_sc = nullptr;
+  unsigned long long *d_rowmax = nullptr;
+  double *d_oz_part = nullptr;
+  size_t oz_part_elems = 0;
+  sdft::OzGemm om1{}, om2{};
   int *d_err = nullptr;
   // per-kind event timing (sdft_ctx_set_timing)
   bool timing = false;

@@ -1,0 +1,371 @@
+// sdft_gemm_oz.cu -- FP64-accurate GEMM from INT8 tcgen05 tensor cores
+// (Ozaki scheme: split each operand into int8 digits under a per-row
+// power-of-two scale, multiply digit slices exactly, recombine exactly).
+//
+// CTA = 6 warps over one 128 x 128 output tile and one K range:
+//   warp 0    TMA producer: per 64-wide K tile one 3-D box per operand
+//             carrying all four digit slices (64 B rows, 64B swizzle),
+//             three-stage ring of 64 KB stages;
+//   warp 1    TMEM owner (512 columns = four int32 accumulators of 128
+//             columns, one per digit order q = s + t) and single-thread
+//             issuer of tcgen05.mma.kind::i8 (10 slice pairs x 2 K steps
+//             of 32 per stage);
+//   warps 2-5 epilogue: tcgen05.ld 32x32b of the four accumulators,
+//             exact int64 combination acc0 2^21 + acc1 2^14 + acc2 2^7 +
+//             acc3, one conversion to FP64 (exact: |value| < 2^53 for K
+//             ranges below 2^20), scaling by 2^(Ea+Eb-33), coalesced store.
+// int32 accumulation cannot overflow while (K range) * 4 * 64^2 < 2^31,
+// i.e. K ranges up to 131072 (checked on the host).
+// All mbarrier waits are bounded (sdft_tc_common.cuh).  No TMA multicast.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cmath>
+#include "sdft_internal.h"
+#include "sdft_tc_common.cuh"
+#include "sdft_gemm_oz.cuh"
+
+namespace sdft {
+
+constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 64, OZ_STAGES = 3;
+constexpr int OZ_MAX_KRANGE = 131072;
+
+struct OzSmem {
+  static constexpr int A_SLICE = OZ_BM * OZ_BK;          // 8 KB
+  static constexpr int B_SLICE = OZ_BN * OZ_BK;          // 8 KB
+  static constexpr int A_BYTES = kOzSlices * A_SLICE;    // 32 KB
+  static constexpr int B_BYTES = kOzSlices * B_SLICE;    // 32 KB
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 64 KB
+  static constexpr int BAR_OFF = OZ_STAGES * STAGE_BYTES;
+  static constexpr int TOTAL = BAR_OFF + 8 * (2 * OZ_STAGES + 1) + 16 + 1024;  // + alignment slack
+  static constexpr int TMEM_COLS = 4 * OZ_BN;                                   // 512
+};
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+
+__global__ void __launch_bounds__(192, 1)
+k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int ktiles_total,
+           int ktiles_per_split, const double *__restrict__ sa, const double *__restrict__ sb,
+           double *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
+  using S = OzSmem;
+  extern __shared__ __align__(1024) unsigned char smem_dyn[];
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t bar_full = sbase + S::BAR_OFF;
+  const uint32_t bar_empty = bar_full + 8 * OZ_STAGES;
+  const uint32_t bar_tmem = bar_empty + 8 * OZ_STAGES;
+  uint32_t *tmem_slot = (uint32_t *)(smem + S::BAR_OFF + 8 * (2 * OZ_STAGES + 1));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * OZ_BN, m0 = blockIdx.y * OZ_BM;
+  const int kt0 = blockIdx.z * ktiles_per_split;
+  const int nkt = max(0, min(ktiles_total, kt0 + ktiles_per_split) - kt0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < OZ_STAGES; s++) {
+      mbar_init(bar_full + 8 * s, 1);
+      mbar_init(bar_empty + 8 * s, 1);
+    }
+    mbar_init(bar_tmem, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(S::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      for (int it = 0; it < nkt; it++) {
+        const int s = it % OZ_STAGES;
+        const uint32_t par = ((it / OZ_STAGES) & 1) ^ 1;
+        if (!mbar_wait(bar_empty + 8 * s, par, err)) break;
+        const uint32_t st = sbase + s * S::STAGE_BYTES;
+        mbar_expect_tx(bar_full + 8 * s, S::STAGE_BYTES);
+        const int kx = (kt0 + it) * OZ_BK;
+        tma_load_3d(st, &tA, kx, m0, 0, bar_full + 8 * s);
+        tma_load_3d(st + S::A_BYTES, &tB, kx, n0, 0, bar_full + 8 * s);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      // D = S32, A = B = signed 8-bit, K-major, N = 128, M = 128
+      constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
+                                 ((uint32_t)(OZ_BM >> 4) << 24);
+      uint32_t started = 0;  // bit q: accumulator q holds data
+      for (int it = 0; it < nkt; it++) {
+        const int s = it % OZ_STAGES;
+        if (!mbar_wait(bar_full + 8 * s, (it / OZ_STAGES) & 1, err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = sbase + s * S::STAGE_BYTES;
+#pragma unroll
+        for (int ks = 0; ks < OZ_BK / 32; ks++) {
+#pragma unroll
+          for (int sa_ = 0; sa_ < kOzSlices; sa_++) {
+#pragma unroll
+            for (int tb = 0; tb + sa_ < kOzSlices; tb++) {
+              const int q = sa_ + tb;
+              const uint64_t ad = smem_desc<64>(st + sa_ * S::A_SLICE + ks * 32);
+              const uint64_t bd = smem_desc<64>(st + S::A_BYTES + tb * S::B_SLICE + ks * 32);
+              mma_i8(tmem + (uint32_t)(q * OZ_BN), ad, bd, idesc, (started >> q) & 1u);
+              started |= 1u << q;
+            }
+          }
+        }
+        mma_commit(bar_empty + 8 * s);  // stage free once these MMAs retire
+      }
+      mma_commit(bar_tmem);  // accumulators complete (also fires when nkt == 0)
+    }
+  } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
+    const int qd = warp & 3;
+    const bool ok = mbar_wait(bar_tmem, 0, err);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int m = m0 + 32 * qd + lane;
+    const bool row_ok = ok && m < Mst && nkt > 0;
+    const double fa = row_ok ? sa[m] * 0x1p-33 : 0.0;
+    const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
+#pragma unroll 1
+    for (int c = 0; c < OZ_BN / 16; c++) {
+      uint32_t r0[16], r1[16], r2[16], r3[16];
+      tmem_ld16(tl + 0 * OZ_BN + c * 16, r0);
+      tmem_ld16(tl + 1 * OZ_BN + c * 16, r1);
+      tmem_ld16(tl + 2 * OZ_BN + c * 16, r2);
+      tmem_ld16(tl + 3 * OZ_BN + c * 16, r3);
+      tmem_ld_wait();
+      if (!(ok && m < Mst)) continue;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int n = n0 + c * 16 + j;
+        if (n < Nst) {
+          const long long v = ((long long)(int)r0[j] << 21) + ((long long)(int)r1[j] << 14) +
+                              ((long long)(int)r2[j] << 7) + (long long)(int)r3[j];
+          out[(size_t)blockIdx.z * split_stride + (size_t)n * ldo + m] = row_ok ? (double)v * fa * sb[n] : 0.0;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// digit extraction
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double absmax_key(double a) { return isfinite(a) ? fabs(a) : INFINITY; }
+
+// rowmax[row] = max |x[row][:]| (as the bit pattern of a non-negative double,
+// whose integer order is its numeric order); +inf if any entry is not finite.
+__global__ void k_row_absmax(const double *__restrict__ x, int ldx, int cols, unsigned long long *rowmax) {
+  const int row = blockIdx.x;
+  double m = 0.0;
+  for (int c = blockIdx.y * blockDim.x + threadIdx.x; c < cols; c += gridDim.y * blockDim.x)
+    m = fmax(m, absmax_key(x[(size_t)row * ldx + c]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
+    atomicMax(rowmax + row, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// Exponent E with max < 2^E (E = 0 for an all-zero row, clamped below so
+// that 2^(6-E) stays finite).
+__device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
+  if (maxbits == 0) return 0;
+  const int field = (int)(maxbits >> 52) & 0x7ff;
+  return max(-1000, max(field, 1) - 1022);
+}
+
+// four digits of x * 2^(6-E) (|.| < 64), each a round-to-nearest integer
+// of the running remainder times 2^7; all steps exact in FP64.
+__device__ __forceinline__ void digits4(double r, int *d) {
+#pragma unroll
+  for (int s = 0; s < kOzSlices; s++) {
+    const double q = rint(r);
+    d[s] = (int)q;
+    r = (r - q) * 128.0;
+  }
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+  return (uint32_t)(a & 0xff) | ((uint32_t)(b & 0xff) << 8) | ((uint32_t)(c & 0xff) << 16) |
+         ((uint32_t)(d & 0xff) << 24);
+}
+
+// digits of rows x cols doubles; 4 consecutive columns per thread, zero
+// digits for cols <= k < ld.
+__global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, int cols,
+                             const unsigned long long *__restrict__ rowmax, int8_t *__restrict__ dig, int ld,
+                             size_t sstride, double *__restrict__ scale) {
+  const int g4 = ld >> 2;
+  const size_t tot = (size_t)rows * g4;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(i / g4), c4 = (int)(i - (size_t)row * g4) * 4;
+    const unsigned long long mb = rowmax[row];
+    const bool bad = mb >= 0x7ff0000000000000ull;
+    const int E = bad ? 0 : row_exponent(mb);
+    const double p = ldexp(1.0, 6 - E);
+    int d[4][kOzSlices];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int c = c4 + e;
+      const double v = (c < cols && !bad) ? x[(size_t)row * ldx + c] : 0.0;
+      digits4(v * p, d[e]);
+    }
+#pragma unroll
+    for (int s = 0; s < kOzSlices; s++)
+      *(uint32_t *)(dig + s * sstride + (size_t)row * ld + c4) = pack4(d[0][s], d[1][s], d[2][s], d[3][s]);
+    if (c4 == 0) scale[row] = bad ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, E);
+  }
+}
+
+// Sum of split-K partials for one row per CTA, then the digit form of the
+// row (second sweep over the just-written row, which is L2 resident).
+__global__ void k_reduce_slice(const double *__restrict__ part, int split, size_t stride, int ldo, int Mst,
+                               double *__restrict__ out, int8_t *__restrict__ dig, size_t dig_stride,
+                               double *__restrict__ scale) {
+  const int n = blockIdx.x;
+  double mx = 0.0;
+  for (int m = threadIdx.x; m < ldo; m += blockDim.x) {
+    double s = 0.0;
+    if (m < Mst)
+      for (int z = 0; z < split; z++) s += part[z * stride + (size_t)n * ldo + m];
+    out[(size_t)n * ldo + m] = s;
+    mx = fmax(mx, absmax_key(s));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  __shared__ double red[32];
+  __shared__ unsigned long long mbits;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mx = fmax(mx, red[w]);
+    mbits = (unsigned long long)__double_as_longlong(mx);
+  }
+  __syncthreads();
+  const bool bad = mbits >= 0x7ff0000000000000ull;
+  const int E = bad ? 0 : row_exponent(mbits);
+  const double p = ldexp(1.0, 6 - E);
+  for (int m4 = threadIdx.x * 4; m4 < ldo; m4 += blockDim.x * 4) {
+    int d[4][kOzSlices];
+#pragma unroll
+    for (int e = 0; e < 4; e++) digits4(bad ? 0.0 : out[(size_t)n * ldo + m4 + e] * p, d[e]);
+#pragma unroll
+    for (int s = 0; s < kOzSlices; s++)
+      *(uint32_t *)(dig + s * dig_stride + (size_t)n * ldo + m4) = pack4(d[0][s], d[1][s], d[2][s], d[3][s]);
+  }
+  if (threadIdx.x == 0) scale[n] = bad ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, E);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*PFN_encodeTiledOz)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                      CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                      CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiledOz get_encode_oz() {
+  static PFN_encodeTiledOz fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encodeTiledOz)p;
+  }
+  return fn;
+}
+
+bool gemm_oz_available() { return get_encode_oz() != nullptr; }
+
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld) {
+  PFN_encodeTiledOz enc = get_encode_oz();
+  if (!enc) return set_error(SDFT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  if (((uintptr_t)dig & 15) || ld % OZ_BK || rows % 128) return set_error(SDFT_ERR_ARG, "oz tensor map alignment");
+  cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)kOzSlices};
+  cuuint64_t strides[2] = {(cuuint64_t)ld, (cuuint64_t)ld * rows};
+  cuuint32_t box[3] = {(cuuint32_t)OZ_BK, 128u, (cuuint32_t)kOzSlices};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void *)dig, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(SDFT_ERR_CUDA, "cuTensorMapEncodeTiled failed (oz)");
+  return SDFT_OK;
+}
+
+int oz_choose_split(int tiles, int ktiles, int max_split) {
+  // cost model in MMA-stage units: waves x K tiles per CTA, plus the
+  // partial-tile write + read of each extra split (about 8 stages' worth of
+  // one CTA's time, spread over the 148 SMs)
+  const int nsm = 148;
+  int best = 1;
+  double best_cost = 1e300;
+  const int lim = max_split < 1 ? 1 : max_split;
+  for (int s = 1; s <= lim && s <= ktiles; s++) {
+    const int kps = (ktiles + s - 1) / s;
+    if (kps * OZ_BK > OZ_MAX_KRANGE) continue;
+    const int se = (ktiles + kps - 1) / kps;
+    const int waves = (tiles * se + nsm - 1) / nsm;
+    const double cost = (double)waves * kps + (se > 1 ? 8.0 * se * tiles / nsm : 0.0);
+    if (cost < best_cost - 1e-9) { best_cost = cost; best = se; }
+  }
+  return best;
+}
+
+int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st) {
+  const int ktiles = (g.K + OZ_BK - 1) / OZ_BK;
+  if (g.M % OZ_BM || g.N % OZ_BN || ktiles < 1) return set_error(SDFT_ERR_ARG, "oz gemm: shape");
+  if (split < 1) split = 1;
+  if (split > ktiles) split = ktiles;
+  const int kps = (ktiles + split - 1) / split;
+  if (kps * OZ_BK > OZ_MAX_KRANGE) return set_error(SDFT_ERR_ARG, "oz gemm: K range per CTA too long");
+  split = (ktiles + kps - 1) / kps;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_gemm_oz8, cudaFuncAttributeMaxDynamicSharedMemorySize, OzSmem::TOTAL);
+    attr = true;
+  }
+  dim3 grid(g.N / OZ_BN, g.M / OZ_BM, split);
+  k_gemm_oz8<<<grid, 192, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
+                                                 g.Mst, g.Nst, err);
+  return SDFT_OK;
+}
+
+void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
+                          int ld, size_t slice_stride, double *scale, cudaStream_t st) {
+  cudaMemsetAsync(rowmax, 0, (size_t)rows * sizeof(unsigned long long), st);
+  int chunks = (cols + 255) / 256;  // grid = rows x chunks (rows on x: up to 2^31 - 1)
+  if (chunks > 64) chunks = 64;
+  if (chunks < 1) chunks = 1;
+  k_row_absmax<<<dim3(rows, chunks), 256, 0, st>>>(x, ldx, cols, rowmax);
+  const size_t tot = (size_t)rows * (ld / 4);
+  int blocks = (int)((tot + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_slice_rows<<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
+}
+
+void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
+                            int8_t *dig, size_t dig_stride, double *scale, cudaStream_t st) {
+  k_reduce_slice<<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale);
+}
+
+}  // namespace sdft

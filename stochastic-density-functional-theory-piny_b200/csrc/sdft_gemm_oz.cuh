@@ -1,0 +1,52 @@
+// sdft_gemm_oz.cuh -- FP64-accurate GEMM on INT8 tensor cores (Ozaki
+// scheme) for the Kleinman-Bylander projection and back projection of the
+// mixed-precision filter.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace sdft {
+
+// A matrix of `rows` x K doubles in digit form: every row carries a
+// power-of-two scale 2^E (E chosen so that all |x| < 2^E) and four signed
+// 8-bit digits per value,
+//     x ~= 2^E * 2^-27 * (d0 2^21 + d1 2^14 + d2 2^7 + d3),  d_s in [-64, 64],
+// i.e. 28 bits relative to the row's largest element (the representation
+// error is below 2^-28 of it).  Digits are stored slice-major:
+// dig[s*rows*ld + row*ld + k], ld a multiple of 64, zero for k >= K.
+constexpr int kOzSlices = 4;
+
+// out[n*ldo + m] = sum_k A[m][k] B[n][k] over the digit products with
+// s + t <= 3 (10 of the 16; the rest lie below 2^-28 of the leading term).
+// Every product is an exact int8 x int8 -> int32 tensor-core MMA; the four
+// digit orders are accumulated exactly in four TMEM accumulators and
+// combined exactly in 64-bit integers, so a K range contributes
+// an exactly representable FP64 value and the only rounding is the
+// FP64 sum of split-K partials.  A: M x K (M multiple of 128), B: N x K
+// (N multiple of 128); only m < Mst, n < Nst are stored.
+struct OzGemm {
+  CUtensorMap tA, tB;
+  int M, N, K, ldo, Mst, Nst;
+  const double *sa, *sb;  // row scales 2^E of A (M) and B (N)
+};
+
+bool gemm_oz_available();
+// tensor map of a digit array [kOzSlices][rows][ld] (int8, K-major)
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld);
+// split == 1: out = result; split > 1: FP64 partial z at out + z*split_stride.
+int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st);
+// split count for `tiles` output tiles over `ktiles` K tiles (<= max_split)
+int oz_choose_split(int tiles, int ktiles, int max_split);
+// digits (row pitch ld, slice pitch slice_stride bytes) + scales of
+// rows x cols doubles (row pitch ldx); rowmax: `rows` words of scratch
+void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
+                          int ld, size_t slice_stride, double *scale, cudaStream_t st);
+// out[n*ldo+m] = sum_z part[z*stride + n*ldo + m] (m < Mst, else 0) for
+// n < Nst, plus the digit form of each row n (ld = ldo, slice pitch
+// dig_stride bytes).
+void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
+                            int8_t *dig, size_t dig_stride, double *scale, cudaStream_t st);
+
+}  // namespace sdft

@@ -20,6 +20,8 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <algorithm>
+#include <cstdlib>
 #include "sdft_ctx.h"
 
 namespace sdft {
@@ -154,12 +156,16 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl};
   for (double **p : old)
     if (*p) { cudaFree(*p); *p = nullptr; }
-  float **oldf[] = {&ctx->d_pj_hi, &ctx->d_pj_lo, &ctx->d_bk_hi, &ctx->d_bk_lo, &ctx->d_c_hi,
-                    &ctx->d_c_lo,  &ctx->d_z_hi,  &ctx->d_z_lo,  &ctx->d_tc_part};
-  for (float **p : oldf)
-    if (*p) { cudaFree(*p); *p = nullptr; }
+  void *oldo[] = {ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig, ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc,
+                  ctx->d_c_sc,   ctx->d_z_sc,   ctx->d_rowmax, ctx->d_oz_part};
+  for (void *p : oldo)
+    if (p) cudaFree(p);
+  ctx->d_pj_dig = ctx->d_bk_dig = ctx->d_c_dig = ctx->d_z_dig = nullptr;
+  ctx->d_pj_sc = ctx->d_bk_sc = ctx->d_c_sc = ctx->d_z_sc = nullptr;
+  ctx->d_rowmax = nullptr;
+  ctx->d_oz_part = nullptr;
   ctx->P = 0;
-  ctx->tc = false;
+  ctx->oz = false;
   if (!kb || kb->natm == 0) return SDFT_OK;
   if (!kb->pos || !kb->type || !kb->lmax_type || !kb->vps || !kb->vpsnorm || !kb->gzvps0 || kb->ntype < 1 ||
       kb->nsplin_g < 1 || kb->dg_spl <= 0.0)
@@ -275,42 +281,52 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->P = P;
   ctx->Ppad = Ppad;
   ctx->Mpad2 = Mpad2;
-  if (ctx->prec == SDFT_PREC_MIXED && gemm_tf32x3_available() && !getenv("SDFT_NO_TC")) {
-    // TF32 hi/lo operands for the tensor-core GEMMs
+  if (ctx->prec == SDFT_PREC_MIXED && gemm_oz_available()) {
+    // digit form of the projector matrices for the INT8 tensor-core GEMMs
     const int S = (ctx->max_states + 127) / 128 * 128;
-    ctx->s_tc = S;
+    const int Kp = (K1 + 63) / 64 * 64;
+    ctx->s_oz = S;
+    ctx->kp_oz = Kp;
     int r;
-    const size_t pjn = (size_t)Ppad * K1, bkn = (size_t)Mpad2 * Ppad, cn = (size_t)S * K1, zn = (size_t)S * Ppad;
-    ctx->tc_part_elems = (size_t)32 * S * Ppad;
-    float **bufs[] = {&ctx->d_pj_hi, &ctx->d_pj_lo, &ctx->d_bk_hi, &ctx->d_bk_lo, &ctx->d_c_hi, &ctx->d_c_lo,
-                      &ctx->d_z_hi,  &ctx->d_z_lo,  &ctx->d_tc_part};
-    size_t ns[] = {pjn, pjn, bkn, bkn, cn, cn, zn, zn, ctx->tc_part_elems};
-    for (int i = 0; i < 9; i++)
-      if ((r = dmalloc(ctx, (void **)bufs[i], ns[i] * sizeof(float)))) { rc = r; goto done; }
-    CKB(cudaMemset(ctx->d_c_hi, 0, cn * sizeof(float)));
-    CKB(cudaMemset(ctx->d_c_lo, 0, cn * sizeof(float)));
-    CKB(cudaMemset(ctx->d_z_hi, 0, zn * sizeof(float)));
-    CKB(cudaMemset(ctx->d_z_lo, 0, zn * sizeof(float)));
-    launch_split_tf32(ctx->d_pj, K1, ctx->d_pj_hi, ctx->d_pj_lo, K1, Ppad, K1, ctx->st);
-    launch_split_tf32(ctx->d_bk, Ppad, ctx->d_bk_hi, ctx->d_bk_lo, Ppad, Mpad2, Ppad, ctx->st);
-    ctx->launches += 2;
-    CKB(cudaStreamSynchronize(ctx->st));
-    TcGemm &g1 = ctx->gm1, &g2 = ctx->gm2;
-    if ((r = make_tmap(&g1.tAh, ctx->d_pj_hi, Ppad, K1, K1, 128)) || (r = make_tmap(&g1.tAl, ctx->d_pj_lo, Ppad, K1, K1, 128)) ||
-        (r = make_tmap(&g1.tBh, ctx->d_c_hi, S, K1, K1, 128)) || (r = make_tmap(&g1.tBl, ctx->d_c_lo, S, K1, K1, 128)) ||
-        (r = make_tmap(&g2.tAh, ctx->d_bk_hi, Mpad2, Ppad, Ppad, 128)) ||
-        (r = make_tmap(&g2.tAl, ctx->d_bk_lo, Mpad2, Ppad, Ppad, 128)) ||
-        (r = make_tmap(&g2.tBh, ctx->d_z_hi, S, Ppad, Ppad, 128)) || (r = make_tmap(&g2.tBl, ctx->d_z_lo, S, Ppad, Ppad, 128))) {
+    const size_t pjd = (size_t)kOzSlices * Ppad * Kp, bkd = (size_t)kOzSlices * Mpad2 * Ppad;
+    const size_t cd = (size_t)kOzSlices * S * Kp, zd = (size_t)kOzSlices * S * Ppad;
+    const int maxrows = std::max(std::max(Ppad, Mpad2), S);
+    ctx->oz_part_elems = (size_t)32 * S * Ppad;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_pj_dig, pjd)) || (r = dmalloc(ctx, (void **)&ctx->d_bk_dig, bkd)) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_c_dig, cd)) || (r = dmalloc(ctx, (void **)&ctx->d_z_dig, zd)) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_pj_sc, Ppad * sizeof(double))) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_bk_sc, Mpad2 * sizeof(double))) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_c_sc, S * sizeof(double))) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_z_sc, S * sizeof(double))) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_rowmax, maxrows * sizeof(unsigned long long))) ||
+        (r = dmalloc(ctx, (void **)&ctx->d_oz_part, ctx->oz_part_elems * sizeof(double)))) {
       rc = r;
       goto done;
     }
-    g1.M = Ppad; g1.K = K1; g1.ldo = Ppad; g1.Mst = P; g1.bn = 128;
-    g2.M = Mpad2; g2.K = Ppad; g2.ldo = K1; g2.Mst = K1; g2.bn = 128;
+    CKB(cudaMemset(ctx->d_c_dig, 0, cd));
+    CKB(cudaMemset(ctx->d_z_dig, 0, zd));
+    CKB(cudaMemset(ctx->d_c_sc, 0, S * sizeof(double)));
+    CKB(cudaMemset(ctx->d_z_sc, 0, S * sizeof(double)));
+    launch_oz_slice_rows(ctx->d_pj, K1, Ppad, K1, ctx->d_rowmax, ctx->d_pj_dig, Kp, (size_t)Ppad * Kp, ctx->d_pj_sc,
+                         ctx->st);
+    launch_oz_slice_rows(ctx->d_bk, Ppad, Mpad2, Ppad, ctx->d_rowmax, ctx->d_bk_dig, Ppad, (size_t)Mpad2 * Ppad,
+                         ctx->d_bk_sc, ctx->st);
+    ctx->launches += 4;
+    CKB(cudaGetLastError());
+    CKB(cudaStreamSynchronize(ctx->st));
+    OzGemm &g1 = ctx->om1, &g2 = ctx->om2;
+    if ((r = make_tmap_oz(&g1.tA, ctx->d_pj_dig, Ppad, Kp)) || (r = make_tmap_oz(&g1.tB, ctx->d_c_dig, S, Kp)) ||
+        (r = make_tmap_oz(&g2.tA, ctx->d_bk_dig, Mpad2, Ppad)) || (r = make_tmap_oz(&g2.tB, ctx->d_z_dig, S, Ppad))) {
+      rc = r;
+      goto done;
+    }
+    g1.M = Ppad; g1.K = Kp; g1.ldo = Ppad; g1.Mst = P; g1.sa = ctx->d_pj_sc; g1.sb = ctx->d_c_sc;
+    g2.M = Mpad2; g2.K = Ppad; g2.ldo = K1; g2.Mst = K1; g2.sa = ctx->d_bk_sc; g2.sb = ctx->d_z_sc;
     // the FP64 projector copies are not used by the mixed path
     cudaFree(ctx->d_pj); ctx->d_pj = nullptr;
     cudaFree(ctx->d_bk); ctx->d_bk = nullptr;
-    ctx->dev_bytes -= (long long)(pjn + bkn) * 8;
-    ctx->tc = true;
+    ctx->dev_bytes -= (long long)((size_t)Ppad * K1 + (size_t)Mpad2 * Ppad) * 8;
+    ctx->oz = true;
   }
 done:
   cudaFree(d_kv); cudaFree(d_rs); cudaFree(d_rcnt); cudaFree(d_frac);

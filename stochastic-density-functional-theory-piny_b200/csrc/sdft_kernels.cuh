@@ -101,7 +101,4 @@ void launch_scale_copy(const double *src, double *dst, double a, size_t n, cudaS
 template <typename T>
 void launch_vks_transpose(const double *v, T *Vp, int n1, int n2, int n3, cudaStream_t st);
 
-// TF32x3 tcgen05 GEMM (mixed precision); returns false if not available.
-bool gemm_tf32x3_available();
-
 }  // namespace sdft

@@ -225,16 +225,17 @@ def test_noncubic_and_generic_grids(pkg, wl, grid, strain):
 
 @pytest.mark.parametrize("which,ns", [("sys1", 5), ("sys2", 130)])
 def test_mixed_hpsi_tensor_core(pkg, which, ns, request):
-    """Mixed context: FP32 FFT + TF32x3 tcgen05 KB GEMMs vs the FP64 oracle."""
+    """Mixed context: FP32 FFT + INT8 Ozaki tcgen05 KB GEMMs vs the FP64 oracle."""
     s = request.getfixturevalue(which)
     c = _ctx(pkg, s, ns, prec=1)
     o = O.OracleSys(s)
     cr, ci = _rand(s["ncoef"], ns, 17)
     fr, fi, e = c.calc_coef_force(cr, ci, want_enl=True)
     orr, oi, oe = o.hpsi(cr, ci, want_enl=True)
-    assert rel_l2(np.concatenate([fr, fi]), np.concatenate([orr, oi])) < 2e-6
-    # E_NL sums +0.5 (s) and -0.5 (p) channel terms; the partial cancellation
-    # amplifies the ~1e-6 relative error of the TF32x3 projections
-    assert abs(e - oe) < 1e-5 * abs(oe)
+    # FP32 FFTs bound the force error (~2e-8 measured); the digit GEMMs keep
+    # the nonlocal energy within ~1e-8 (E_NL partly cancels between the
+    # +0.5 s and -0.5 p channels)
+    assert rel_l2(np.concatenate([fr, fi]), np.concatenate([orr, oi])) < 2e-7
+    assert abs(e - oe) < 1e-6 * abs(oe)
     c.sync()
     c.close()

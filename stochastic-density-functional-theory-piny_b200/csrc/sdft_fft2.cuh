@@ -114,37 +114,62 @@ struct Lines2 {  // two contiguous groups of lines (rows 0..n1-1 and the top one
   __device__ __forceinline__ int base(int l) const { return (l < nl1) ? l * ls : off2 + (l - nl1) * ls; }
 };
 
+// Unit (line l, index j) enumeration for the passes below: lines vary
+// fastest across threads, so a warp touches 32 consecutive lines at the same
+// j.  With line pitches of N+1 complex (odd) or unit pitch, consecutive lines
+// fall in distinct banks (no shared-memory bank conflicts) and the twiddle
+// index j is uniform across most of a warp (broadcast loads).  The stepping
+// avoids a runtime division per unit.
+struct UnitIter {
+  int l, j, dl, dj, nl;
+  __device__ __forceinline__ UnitIter(int tid, int nthr, int nlines) : nl(nlines) {
+    dj = nthr / nl;
+    dl = nthr - dj * nl;
+    j = tid / nl;
+    l = tid - j * nl;
+  }
+  __device__ __forceinline__ void next() {
+    l += dl;
+    j += dj;
+    if (l >= nl) { l -= nl; j++; }
+  }
+};
+
 // natural -> permuted.  twN: exp(-2 pi i t/N) in shared memory.
 template <int N, int ES, int DIR, typename C, typename LM>
 __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+  if (nl > 0) {
 #pragma unroll 1
-  for (int u = tid; u < nl * R2; u += nthr) {
-    const int l = u / R2, j2 = u - l * R2;
-    C *p = buf + lm.base(l);
-    C v[R1];
+    for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {
+      const int l = it.l, j2 = it.j;
+      C *p = buf + lm.base(l);
+      C v[R1];
 #pragma unroll
-    for (int j1 = 0; j1 < R1; j1++) v[j1] = p[(j2 + R2 * j1) * ES];
-    dftr<R1, DIR>(v);
-    p[j2 * ES] = v[0];
+      for (int j1 = 0; j1 < R1; j1++) v[j1] = p[(j2 + R2 * j1) * ES];
+      dftr<R1, DIR>(v);
+      p[j2 * ES] = v[0];
 #pragma unroll
-    for (int k1 = 1; k1 < R1; k1++) {
-      C w = lds_tw(twN + j2 * k1);
-      if (DIR > 0) w.y = -w.y;
-      p[(j2 + R2 * k1) * ES] = cmul(v[k1], w);
+      for (int k1 = 1; k1 < R1; k1++) {
+        C w = lds_tw(twN + j2 * k1);
+        if (DIR > 0) w.y = -w.y;
+        p[(j2 + R2 * k1) * ES] = cmul(v[k1], w);
+      }
     }
   }
   __syncthreads();
+  if (nl > 0) {
 #pragma unroll 1
-  for (int u = tid; u < nl * R1; u += nthr) {
-    const int l = u / R1, k1 = u - l * R1;
-    C *p = buf + lm.base(l) + R2 * k1 * ES;
-    C v[R2];
+    for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {
+      const int l = it.l, k1 = it.j;
+      C *p = buf + lm.base(l) + R2 * k1 * ES;
+      C v[R2];
 #pragma unroll
-    for (int j = 0; j < R2; j++) v[j] = p[j * ES];
-    dftr<R2, DIR>(v);
+      for (int j = 0; j < R2; j++) v[j] = p[j * ES];
+      dftr<R2, DIR>(v);
 #pragma unroll
-    for (int j = 0; j < R2; j++) p[j * ES] = v[j];
+      for (int j = 0; j < R2; j++) p[j * ES] = v[j];
+    }
   }
   __syncthreads();
 }
@@ -153,33 +178,37 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, 
 template <int N, int ES, int DIR, typename C, typename LM>
 __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+  if (nl > 0) {
 #pragma unroll 1
-  for (int u = tid; u < nl * R1; u += nthr) {
-    const int l = u / R1, k1 = u - l * R1;
-    C *p = buf + lm.base(l) + R2 * k1 * ES;
-    C v[R2];
+    for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {
+      const int l = it.l, k1 = it.j;
+      C *p = buf + lm.base(l) + R2 * k1 * ES;
+      C v[R2];
 #pragma unroll
-    for (int j = 0; j < R2; j++) v[j] = p[j * ES];
-    dftr<R2, DIR>(v);
-    p[0] = v[0];
+      for (int j = 0; j < R2; j++) v[j] = p[j * ES];
+      dftr<R2, DIR>(v);
+      p[0] = v[0];
 #pragma unroll
-    for (int j2 = 1; j2 < R2; j2++) {
-      C w = lds_tw(twN + j2 * k1);
-      if (DIR > 0) w.y = -w.y;
-      p[j2 * ES] = cmul(v[j2], w);
+      for (int j2 = 1; j2 < R2; j2++) {
+        C w = lds_tw(twN + j2 * k1);
+        if (DIR > 0) w.y = -w.y;
+        p[j2 * ES] = cmul(v[j2], w);
+      }
     }
   }
   __syncthreads();
+  if (nl > 0) {
 #pragma unroll 1
-  for (int u = tid; u < nl * R2; u += nthr) {
-    const int l = u / R2, j2 = u - l * R2;
-    C *p = buf + lm.base(l);
-    C v[R1];
+    for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {
+      const int l = it.l, j2 = it.j;
+      C *p = buf + lm.base(l);
+      C v[R1];
 #pragma unroll
-    for (int k1 = 0; k1 < R1; k1++) v[k1] = p[(R2 * k1 + j2) * ES];
-    dftr<R1, DIR>(v);
+      for (int k1 = 0; k1 < R1; k1++) v[k1] = p[(R2 * k1 + j2) * ES];
+      dftr<R1, DIR>(v);
 #pragma unroll
-    for (int j1 = 0; j1 < R1; j1++) p[(j2 + R2 * j1) * ES] = v[j1];
+      for (int j1 = 0; j1 < R1; j1++) p[(j2 + R2 * j1) * ES] = v[j1];
+    }
   }
   __syncthreads();
 }

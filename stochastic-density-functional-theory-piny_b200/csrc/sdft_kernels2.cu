@@ -146,7 +146,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
 }
 
 template <typename T, int N3>
-__global__ void __launch_bounds__(kColThreads)
+__global__ void __launch_bounds__(kColThreads, 4)
 kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
   using C2 = typename CT<T>::type;
   constexpr int P3 = N3 + 1;
@@ -247,6 +247,77 @@ template <int N1> struct RowsPerm {  // rows given in permuted-a order
   }
 };
 
+// a-direction transform pair of one plane with the V multiply fused in:
+// forward a-FFT (natural -> permuted) of the N2 columns, times V (stored in
+// the permuted order, Vpl[pa*N2 + pb]), inverse a-FFT (permuted -> natural).
+// The second forward pass and the first inverse pass work on the same
+// R2-blocks of a column, so one register-resident unit does
+// DFT -> x V -> inverse DFT without a round trip through shared memory.
+// Rows with kamax < ka < N1 - kamax are zero on input (outside the sphere)
+// and not needed on output: they are neither read nor written.
+template <int N1, typename C2, typename T>
+__device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, const T *__restrict__ Vpl, int kamax,
+                                             const C2 *tw1, int tid, int nthr) {
+  constexpr int R1 = Plan<N1>::R1, R2 = Plan<N1>::R2;
+  auto active = [&](int ka) { return ka <= kamax || ka >= N1 - kamax; };
+#pragma unroll 1
+  for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {  // forward pass 1
+    const int l = it.l, j2 = it.j;
+    C2 *p = pl + l;
+    C2 v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; j1++) {
+      const int ka = j2 + R2 * j1;
+      v[j1] = active(ka) ? p[ka * P2] : cmk<C2>(0.0, 0.0);
+    }
+    dftr<R1, +1>(v);
+    p[j2 * P2] = v[0];
+#pragma unroll
+    for (int k1 = 1; k1 < R1; k1++) {
+      C2 w = lds_tw(tw1 + j2 * k1);
+      w.y = -w.y;
+      p[(j2 + R2 * k1) * P2] = cmul(v[k1], w);
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {  // forward pass 2, x V, inverse pass 1
+    const int l = it.l, k1 = it.j;
+    C2 *p = pl + R2 * k1 * P2 + l;
+    const T *vp = Vpl + (size_t)R2 * k1 * N2 + l;
+    C2 v[R2];
+#pragma unroll
+    for (int j = 0; j < R2; j++) v[j] = p[j * P2];
+    dftr<R2, +1>(v);
+#pragma unroll
+    for (int j = 0; j < R2; j++) {
+      const T w = vp[(size_t)j * N2];
+      v[j].x *= w;
+      v[j].y *= w;
+    }
+    dftr<R2, -1>(v);
+    p[0] = v[0];
+#pragma unroll
+    for (int j2 = 1; j2 < R2; j2++) p[j2 * P2] = cmul(v[j2], lds_tw(tw1 + j2 * k1));
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {  // inverse pass 2
+    const int l = it.l, j2 = it.j;
+    C2 *p = pl + l;
+    C2 v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) v[k1] = p[(R2 * k1 + j2) * P2];
+    dftr<R1, -1>(v);
+#pragma unroll
+    for (int j1 = 0; j1 < R1; j1++) {
+      const int ka = j2 + R2 * j1;
+      if (active(ka)) p[ka * P2] = v[j1];
+    }
+  }
+  __syncthreads();
+}
+
 template <typename T, int N1, int N2>
 __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
 kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict__ Vp) {
@@ -263,7 +334,13 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
     for (int t = tid; t < N1; t += NT) tw1[t] = t1[t];
     for (int t = tid; t < N2; t += NT) tw2[t] = t2[t];
   }
-  for (int i = tid; i < N1 * P2; i += NT) pl[i] = cmk<C2>(0.0, 0.0);
+  const int ka = g.kamax;
+  const Lines2 rows{ka + 1, P2, (N1 - ka) * P2};
+  // zero only the 2 kamax + 1 rows inside the sphere's a-range
+  for (int i = tid; i < (2 * ka + 1) * N2; i += NT) {
+    const int l = i / N2, b = i - l * N2;
+    pl[rows.base(l) + b] = cmk<C2>(0.0, 0.0);
+  }
   __syncthreads();
   C2 *Xrow = X + ((size_t)blockIdx.y * g.n3 + r) * g.ncols_pad;
   for (int col = tid; col < g.ncols; col += NT) {
@@ -271,20 +348,8 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
     pl[(ab >> 16) * P2 + (ab & 0xffff)] = Xrow[col];
   }
   __syncthreads();
-  const int ka = g.kamax;
-  const Lines2 rows{ka + 1, P2, (N1 - ka) * P2};
   dif<N2, 1, +1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
-  dif<N1, P2, +1>(pl, Lines1{1}, N2, tw1, tid, NT);
-  const T *Vpl = Vp + (size_t)r * N1 * N2;
-  for (int e = tid; e < N1 * N2; e += NT) {
-    const int pa = e / N2, pb = e - pa * N2;
-    C2 v = pl[pa * P2 + pb];
-    const T w = Vpl[e];
-    v.x *= w; v.y *= w;
-    pl[pa * P2 + pb] = v;
-  }
-  __syncthreads();
-  dit<N1, P2, -1>(pl, Lines1{1}, N2, tw1, tid, NT);
+  plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, tw1, tid, NT);
   dit<N2, 1, -1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
   for (int col = tid; col < g.ncols; col += NT) {
     const int ab = g.col_ab[col];

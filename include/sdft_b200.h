@@ -165,7 +165,8 @@ int sdft_filter_newton_dev(sdft_ctx *ctx, int nstate, int L, int num_chem_pot,
 int sdft_cheby_moments_dev(sdft_ctx *ctx, int nstate, int L, double scale,
                            double energy_mean, double *moments);
 /* Density of the filtered orbitals of chem-pot imu, result stays on device
- * unless rho != NULL.  occ_over_nsto scales it (aveFactUp).            */
+ * unless rho != NULL (host or device memory; copied, then synchronised).
+ * occ_over_nsto scales it (aveFactUp).                                   */
 int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double occ_over_nsto,
                      double *rho);
 int sdft_download_filtered(sdft_ctx *ctx, int nstate, int imu, double *re, double *im);

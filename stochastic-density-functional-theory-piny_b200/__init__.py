@@ -388,7 +388,13 @@ class Context:
         _chk(lib.sdft_cheby_moments_dev(self._p, nstate, L, scale, energy_mean, _d(m)))
         return m
 
-    def density_dev(self, nstate, imu=0, scale=1.0, want=True):
+    def density_dev(self, nstate, imu=0, scale=1.0, want=True, out_ptr=None):
+        """Density of the filtered orbitals; returned as a host array (want),
+        or copied to the device address out_ptr (e.g. a torch tensor's
+        data_ptr()), or left on the device."""
+        if out_ptr is not None:
+            _chk(lib.sdft_density_dev(self._p, nstate, imu, scale, C.cast(C.c_void_p(out_ptr), _dp)))
+            return None
         rho = np.zeros(self.n[0] * self.n[1] * self.n[2]) if want else None
         _chk(lib.sdft_density_dev(self._p, nstate, imu, scale, _d(rho) if want else None))
         return rho

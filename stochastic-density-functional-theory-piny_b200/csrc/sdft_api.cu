@@ -869,7 +869,8 @@ extern "C" int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double scale
   int r = density_core(ctx, ctx->d_acc + (size_t)imu * ctx->vec_elems, nstate, scale);
   if (r) return r;
   if (rho) {
-    CK(cudaMemcpyAsync(rho, ctx->d_rho, (size_t)ctx->N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    // host or device destination (unified addressing)
+    CK(cudaMemcpyAsync(rho, ctx->d_rho, (size_t)ctx->N * sizeof(double), cudaMemcpyDefault, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
   }
   return SDFT_OK;

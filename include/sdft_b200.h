@@ -182,6 +182,22 @@ long long sdft_launch_count(const sdft_ctx *ctx);
 int sdft_ctx_set_timing(sdft_ctx *ctx, int enable);
 int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count);
 
+/* ---- allocation-free device helper ------------------------------------ */
+/* No counterpart in the reference.  Per-orbital half-sphere inner products
+ *   out[s] = sum_{G!=0} 2 (a_re b_re + a_im b_im) + a_re(G0) b_re(G0)
+ * of nstate orbitals of ncoef coefficients (G0 last), all five arrays in
+ * device memory of the calling thread's current device; queued on `stream`
+ * (a cudaStream_t, NULL = default stream) and asynchronous.  Allocates
+ * nothing: for callers whose device memory is fully owned by their own pool
+ * or fixed in size.  Partial sums live in a static 64 KB device array
+ * compiled into the library; nstate above 1024 is rejected
+ * (SDFT_ERR_ARG).  The first call on a device looks that array up and
+ * should come before any stream capture.  Calls that may overlap on one
+ * device race on the array: order them on one stream.                    */
+int sdft_half_dots_noalloc(const double *a_re, const double *a_im,
+                           const double *b_re, const double *b_im,
+                           int ncoef, int nstate, double *out, void *stream);
+
 /* ---- host FP64 helpers (no device) ------------------------------------ */
 int sdft_round_fft(int n);
 /* fun_flag 1: F, 2: sqrt(F) (Fermi-Dirac 1/(1+exp(beta(x-mu)))).        */

@@ -115,6 +115,7 @@ _sig("sdft_sync", C.c_int, [_vp])
 _sig("sdft_launch_count", C.c_longlong, [_vp])
 _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
+_sig("sdft_half_dots_noalloc", C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
 KERNEL_KINDS = ("stage_a_pack_cfft", "stage_b_plane_fft_vks", "stage_c_cfft_unpack_recur", "kb_proj_gemm",
                 "kb_back_gemm", "density_planes", "noise_planes", "other")
 _sig("sdft_round_fft", C.c_int, [C.c_int])

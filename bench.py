@@ -168,14 +168,10 @@ def run_ours(args):
     chi_h = ctx.genNoiseOrbitalReal(nsto, seed=10.0, np_states=world, myid=rank)
     noise_s = time.time() - t1
     # chemical potential from the moments (calcChemPotCheby), summed over ranks
+    states = __import__(pkg.__name__ + ".states", fromlist=["StateGroup"])
+    grp = states.StateGroup(dist, device=f"cuda:{local}")
     mom = ctx.moments_dev(nsto, L, scale, emean)
-    if world > 1:
-        mt = torch.tensor(mom, device=f"cuda:{local}")
-        dist.all_reduce(mt)
-        mom = mt.cpu().numpy()
-    mom_n = mom / (nsto * world)
-    ne_true = s["num_elec"]
-    mu, ne = pkg.calcChemPotCheby(L, ediff, emean, wl.BETA, wl.OCC, mom_n, ne_true, 0.2, 0.05)
+    mu, ne = grp.chem_pot(pkg, mom, nsto * world, L, ediff, emean, wl.BETA, wl.OCC, s["num_elec"], 0.2, 0.05)
     ec = pkg.calcChebyCoeff(L, ediff, emean, wl.BETA, mu, fun_flag=2)
     setup_s = time.time() - t0
     occ_over = wl.OCC / (nsto * world)
@@ -188,7 +184,7 @@ def run_ours(args):
             # this rank's density into a device buffer, then the path's one
             # exchange step: the sum of the density over the state ranks
             ctx.density_dev(nsto, 0, occ_over, out_ptr=rho_t.data_ptr())
-            dist.all_reduce(rho_t)
+            grp.sum_tensor_(rho_t)
         else:
             ctx.density_dev(nsto, 0, occ_over, want=False)
 

@@ -336,7 +336,7 @@ def run_ours(args):
                     timing.values()))} for k, v in timing.items() if v[1]}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # reported at N=1 only
         cpu = cpu_baseline(s, nsto, L, scale, emean, ec, args)
     lat = sorted(step_ms)
     out = {

@@ -179,9 +179,14 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   const int N = (nstate + 127) / 128 * 128;
   {
     TScope ts(ctx, 7);
-    launch_oz_slice_rows(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,
-                         ctx->d_c_sc, ctx->st);
-    ctx->launches += 2;
+    // row maxima: from the stage C that wrote `vec`, else one pass over it
+    if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {
+      launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);
+      ctx->launches++;
+    }
+    launch_oz_slice(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,
+                    ctx->d_c_sc, ctx->st);
+    ctx->launches++;
   }
   OzGemm g1 = ctx->om1, g2 = ctx->om2;
   g1.N = N; g1.Nst = nstate;
@@ -194,9 +199,13 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
     TScope ts(ctx, 3);
     r = run_gemm_oz(g1, split, ctx->d_oz_part, stride, ctx->d_err, ctx->st);
     if (r) return r;
+    // also zeroes d_rowmax[0, nstate) for the next stage C (the slice above
+    // has consumed it)
     launch_oz_reduce_slice(ctx->d_oz_part, split, stride, Ppad, ctx->P, nstate, ctx->d_z, ctx->d_z_dig,
-                           (size_t)S * Ppad, ctx->d_z_sc, ctx->st);
+                           (size_t)S * Ppad, ctx->d_z_sc, ctx->d_rowmax, ctx->st);
     ctx->launches += 2;
+    ctx->rowmax_zero_n = nstate;
+    ctx->omax_vec = nullptr;
   }
   if (want_enl) {
     launch_enl(ctx->d_z, Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
@@ -251,6 +260,10 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
   e.C = cur;
   e.FNL = ctx->P ? ctx->d_fnl : nullptr;
   e.invN = 1.0 / (double)ctx->N;
+  if (ctx->oz && ctx->track_omax && e.OUT) {
+    if (ctx->rowmax_zero_n < nstate) CK(cudaMemsetAsync(ctx->d_rowmax, 0, (size_t)nstate * 8, ctx->st));
+    e.omax = ctx->d_rowmax;
+  }
   if (ctx->fast) {
     if (is_fp64(ctx)) {
       { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
@@ -272,8 +285,20 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
   }
   ctx->launches += 3;
   CK(cudaGetLastError());
+  if (e.omax) {
+    ctx->omax_vec = e.OUT;
+    ctx->omax_n = nstate;
+    ctx->rowmax_zero_n = 0;
+  }
   return SDFT_OK;
 }
+
+// Row-maximum tracking for the duration of one filter / moments loop.
+struct OmaxScope {
+  sdft_ctx *c;
+  explicit OmaxScope(sdft_ctx *ctx) : c(ctx) { c->track_omax = c->oz; c->omax_vec = nullptr; }
+  ~OmaxScope() { c->track_omax = false; c->omax_vec = nullptr; }
+};
 
 static int check_ready(sdft_ctx *ctx, int nstate) {
   if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
@@ -295,6 +320,7 @@ static EpiArgs base_epi(sdft_ctx *ctx) {
 static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double scale, double emean,
                              bool store_moments) {
   int r;
+  OmaxScope om(ctx);
   if ((r = ensure_acc(ctx, nmu))) return r;
   const double prefact = -scale * emean, s1 = -scale * 0.25, s2 = -scale * 0.5;
   double *cur = ctx->d_chi, *prev = nullptr;
@@ -335,6 +361,7 @@ static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double s
 static int filter_newton_core(sdft_ctx *ctx, int nstate, int L, int nmu, const double *samp, double scale,
                               double emean) {
   int r;
+  OmaxScope om(ctx);
   if ((r = ensure_acc(ctx, nmu))) return r;
   const double s1 = -scale * 0.25, s2 = -scale * 0.5;
   double *cur = ctx->d_chi;
@@ -357,6 +384,7 @@ static int filter_newton_core(sdft_ctx *ctx, int nstate, int L, int nmu, const d
 // Moments by the doubling identities (calcChebyMoments).
 static int moments_core(sdft_ctx *ctx, int nstate, int L, double scale, double emean, double *mom_host) {
   int r;
+  OmaxScope om(ctx);
   const int M = (L % 2 == 0) ? (L / 2 + 1) : ((L + 1) / 2);
   if ((r = ensure_mom(ctx, (size_t)(M + 1) * 3))) return r;
   const double prefact = -scale * emean, s1 = -scale * 0.25, s2 = -scale * 0.5;

@@ -67,6 +67,13 @@ struct sdft_ctx {
   double *d_oz_part = nullptr;
   size_t oz_part_elems = 0;
   sdft::OzGemm om1{}, om2{};
+  // Inside a filter / moments loop, stage C records the per-orbital max of
+  // the vector it writes (d_rowmax), so the next projection can form that
+  // vector's digits without another pass over it.
+  bool track_omax = false;
+  const double *omax_vec = nullptr;  // vector whose row maxima d_rowmax holds
+  int omax_n = 0;
+  int rowmax_zero_n = 0;             // d_rowmax[0, n) known to be zero
   int *d_err = nullptr;
   // per-kind event timing (sdft_ctx_set_timing)
   bool timing = false;

@@ -239,8 +239,9 @@ __global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, in
 // row (second sweep over the just-written row, which is L2 resident).
 __global__ void k_reduce_slice(const double *__restrict__ part, int split, size_t stride, int ldo, int Mst,
                                double *__restrict__ out, int8_t *__restrict__ dig, size_t dig_stride,
-                               double *__restrict__ scale) {
+                               double *__restrict__ scale, unsigned long long *__restrict__ zero_rowmax) {
   const int n = blockIdx.x;
+  if (zero_rowmax && threadIdx.x == 0) zero_rowmax[n] = 0ull;
   double mx = 0.0;
   for (int m = threadIdx.x; m < ldo; m += blockDim.x) {
     double s = 0.0;
@@ -350,22 +351,32 @@ int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, in
   return SDFT_OK;
 }
 
-void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
-                          int ld, size_t slice_stride, double *scale, cudaStream_t st) {
+void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {
   cudaMemsetAsync(rowmax, 0, (size_t)rows * sizeof(unsigned long long), st);
   int chunks = (cols + 255) / 256;  // grid = rows x chunks (rows on x: up to 2^31 - 1)
   if (chunks > 64) chunks = 64;
   if (chunks < 1) chunks = 1;
   k_row_absmax<<<dim3(rows, chunks), 256, 0, st>>>(x, ldx, cols, rowmax);
+}
+
+void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
+                     int ld, size_t slice_stride, double *scale, cudaStream_t st) {
   const size_t tot = (size_t)rows * (ld / 4);
   int blocks = (int)((tot + 255) / 256);
   if (blocks > 148 * 32) blocks = 148 * 32;
   k_slice_rows<<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
 }
 
+void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
+                          int ld, size_t slice_stride, double *scale, cudaStream_t st) {
+  launch_oz_rowmax(x, ldx, rows, cols, rowmax, st);
+  launch_oz_slice(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale, st);
+}
+
 void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
-                            int8_t *dig, size_t dig_stride, double *scale, cudaStream_t st) {
-  k_reduce_slice<<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale);
+                            int8_t *dig, size_t dig_stride, double *scale, unsigned long long *zero_rowmax,
+                            cudaStream_t st) {
+  k_reduce_slice<<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale, zero_rowmax);
 }
 
 }  // namespace sdft

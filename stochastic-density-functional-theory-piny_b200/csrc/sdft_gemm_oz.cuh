@@ -39,14 +39,20 @@ int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld);
 int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st);
 // split count for `tiles` output tiles over `ktiles` K tiles (<= max_split)
 int oz_choose_split(int tiles, int ktiles, int max_split);
-// digits (row pitch ld, slice pitch slice_stride bytes) + scales of
-// rows x cols doubles (row pitch ldx); rowmax: `rows` words of scratch
+// rowmax[r] = bits of max_k |x[r][k]| (zeroed first); rows x cols, pitch ldx
+void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st);
+// digits (row pitch ld, slice pitch slice_stride bytes) + scales of rows x
+// cols doubles under the row maxima in rowmax
+void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
+                     int ld, size_t slice_stride, double *scale, cudaStream_t st);
+// both of the above
 void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
                           int ld, size_t slice_stride, double *scale, cudaStream_t st);
 // out[n*ldo+m] = sum_z part[z*stride + n*ldo + m] (m < Mst, else 0) for
 // n < Nst, plus the digit form of each row n (ld = ldo, slice pitch
-// dig_stride bytes).
+// dig_stride bytes).  zero_rowmax (nullable): words [0, Nst) set to 0.
 void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
-                            int8_t *dig, size_t dig_stride, double *scale, cudaStream_t st);
+                            int8_t *dig, size_t dig_stride, double *scale, unsigned long long *zero_rowmax,
+                            cudaStream_t st);
 
 }  // namespace sdft

@@ -327,6 +327,7 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     cudaFree(ctx->d_bk); ctx->d_bk = nullptr;
     ctx->dev_bytes -= (long long)((size_t)Ppad * K1 + (size_t)Mpad2 * Ppad) * 8;
     ctx->oz = true;
+    ctx->rowmax_zero_n = 0;  // the projector slicing above left row maxima behind
   }
 done:
   cudaFree(d_kv); cudaFree(d_rs); cudaFree(d_rcnt); cudaFree(d_frac);

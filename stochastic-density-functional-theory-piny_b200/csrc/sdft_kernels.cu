@@ -224,11 +224,12 @@ k_stage_b_noise(DevGeom g, const unsigned char *__restrict__ neg, int nstate, in
 struct Dots { double d0, d1, d2; };
 
 __device__ __forceinline__ void epilogue(const DevGeom &g, const EpiArgs &e, int s, int gi, bool g0,
-                                         double fr, double fi, Dots &dt) {
+                                         double fr, double fi, Dots &dt, double &mx) {
   const size_t o = (size_t)s * 2 * g.ngp + gi;
   if (e.mode == EPI_NOISE) {
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
+    mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
     return;
   }
   const double cr = e.C[o], ci = e.C[o + g.ngp];
@@ -246,6 +247,7 @@ __device__ __forceinline__ void epilogue(const DevGeom &g, const EpiArgs &e, int
   if (e.mode == EPI_HPSI) {
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
+    mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
     return;
   }
   const double sc = g0 ? e.s2 : e.s1;
@@ -257,6 +259,7 @@ __device__ __forceinline__ void epilogue(const DevGeom &g, const EpiArgs &e, int
   }
   e.OUT[o] = nr;
   e.OUT[o + g.ngp] = ni;
+  mx = fmax(mx, fmax(absmax_key_d(nr), absmax_key_d(ni)));
   if (e.ACC) {
     for (int imu = 0; imu < e.nmu; imu++) {
       double *A = e.ACC + imu * e.acc_stride;
@@ -312,6 +315,7 @@ k_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
   LineMap lmap{ncl, ncl, P3, 0, 1};
   fft_lines<-1, (2 * kCPB * kMaxEdge + kColThreads - 1) / kColThreads>(buf, g.n3, lmap, tw, blockDim.x, tid);
   Dots dt{0.0, 0.0, 0.0};
+  double mx1 = 0.0, mx2 = 0.0;
   const int warp = tid >> 5, lane = tid & 31;
   const double invN = e.invN;
   const bool noise = (e.mode == EPI_NOISE);
@@ -342,17 +346,21 @@ k_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
           f2r = -0.5 * (ti + tic);
           f2i = -0.5 * (trc - tr);
         }
-        epilogue(g, e, s1, gi, false, f1r, f1i, dt);
-        if (has2) epilogue(g, e, s2, gi, false, f2r, f2i, dt);
+        epilogue(g, e, s1, gi, false, f1r, f1i, dt, mx1);
+        if (has2) epilogue(g, e, s2, gi, false, f2r, f2i, dt, mx2);
       } else {
         const int g0 = g.ncoef - 1;
         const C2 F = buf[lc * P3];
         const double tr = (double)F.x * invN, ti = (double)F.y * invN;
         const double m = noise ? -1.0 : -2.0;
-        epilogue(g, e, s1, g0, true, m * tr, 0.0, dt);
-        if (has2) epilogue(g, e, s2, g0, true, m * ti, 0.0, dt);
+        epilogue(g, e, s1, g0, true, m * tr, 0.0, dt, mx1);
+        if (has2) epilogue(g, e, s2, g0, true, m * ti, 0.0, dt, mx2);
       }
     }
+  }
+  if (e.omax) {
+    __shared__ double mred[kColThreads / 32][2];
+    omax_flush(e.omax, s1, s2, has2, mx1, mx2, mred);
   }
   if (e.dots) {
 #pragma unroll

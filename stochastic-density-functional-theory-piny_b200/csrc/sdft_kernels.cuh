@@ -55,7 +55,31 @@ struct EpiArgs {
   double *dots;          // per-CTA partials [pairs][nbatch][3] or nullptr
   int ndots;             // 1 (filter moments) or 3 (doubling)
   double invN;
+  unsigned long long *omax;  // per orbital: atomicMax of max|OUT| (bits of a
+                             // non-negative double; +inf if not finite), or nullptr
 };
+
+// |x| as an order-preserving key for atomicMax on the bit pattern; non-finite -> +inf
+__device__ __forceinline__ double absmax_key_d(double a) { return isfinite(a) ? fabs(a) : INFINITY; }
+
+// Block-wide max of two per-thread values, then one atomicMax per orbital
+// (blockDim.x = kColThreads).
+__device__ __forceinline__ void omax_flush(unsigned long long *omax, int s1, int s2, bool has2, double m1, double m2,
+                                           double (*red)[2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+  }
+  if (lane == 0) { red[warp][0] = m1; red[warp][1] = m2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) { m1 = fmax(m1, red[w][0]); m2 = fmax(m2, red[w][1]); }
+    atomicMax(omax + s1, (unsigned long long)__double_as_longlong(m1));
+    if (has2) atomicMax(omax + s2, (unsigned long long)__double_as_longlong(m2));
+  }
+}
 
 // ----- launches (all on `st`) ---------------------------------------------
 // Column stage A: pack pairs of orbitals into columns, backward c-FFT.

@@ -170,6 +170,9 @@ int sdft_cheby_moments_dev(sdft_ctx *ctx, int nstate, int L, double scale,
 int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double occ_over_nsto,
                      double *rho);
 int sdft_download_filtered(sdft_ctx *ctx, int nstate, int imu, double *re, double *im);
+/* The last density computed on the context (by sdft_density_dev or a batch
+ * replay), copied to host or device memory without recomputing it. */
+int sdft_download_density(sdft_ctx *ctx, double *rho);
 int sdft_sync(sdft_ctx *ctx);
 /* Kernel launches issued by the context since creation (own kernels only). */
 long long sdft_launch_count(const sdft_ctx *ctx);
@@ -181,6 +184,31 @@ long long sdft_launch_count(const sdft_ctx *ctx);
 #define SDFT_NKIND 8
 int sdft_ctx_set_timing(sdft_ctx *ctx, int enable);
 int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count);
+
+/* ---- tuning and batched systems ---------------------------------------- */
+/* No counterpart in the reference (it filters one system per run).
+ * Split-K of the nonlocal projection GEMM: 0 = built-in cost model,
+ * 1..64 = fixed (chosen by the autotuner in tuner.py).                    */
+int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split);
+/* One CUDA graph running, for every context i (orbitals resident, V and KB
+ * set), the Chebyshev filter of nstate[i] orbitals with the L[i]
+ * coefficients coeffs[i] (one chemical potential) followed by the density
+ * of the result scaled by occ_over_nsto[i].  Each context's stream is one
+ * branch of the graph, so systems of different grids run concurrently.
+ * Creation sizes every buffer, uploads the coefficients and captures;
+ * sdft_batch_launch replays the whole batch with a single graph launch
+ * (asynchronous; refilters whatever orbitals are resident).  Afterwards each
+ * context's result is read with sdft_density_dev / sdft_download_filtered. */
+typedef struct sdft_batch sdft_batch;
+int sdft_batch_create(int n, sdft_ctx *const *ctxs, const int *nstate, const int *L,
+                      const double *const *coeffs, const double *scale, const double *emean,
+                      const double *occ_over_nsto, sdft_batch **out);
+int sdft_batch_launch(sdft_batch *b);
+int sdft_batch_sync(sdft_batch *b);
+void *sdft_batch_stream(sdft_batch *b);
+/* own kernels + memsets issued by one replay */
+long long sdft_batch_kernel_count(const sdft_batch *b);
+int sdft_batch_destroy(sdft_batch *b);
 
 /* ---- allocation-free device helper ------------------------------------ */
 /* No counterpart in the reference.  Per-orbital half-sphere inner products

@@ -115,6 +115,14 @@ _sig("sdft_sync", C.c_int, [_vp])
 _sig("sdft_launch_count", C.c_longlong, [_vp])
 _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
+_sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
+_sig("sdft_download_density", C.c_int, [_vp, _dp])
+_sig("sdft_batch_create", C.c_int, [C.c_int, C.POINTER(_vp), _ip, _ip, C.POINTER(_dp), _dp, _dp, _dp, C.POINTER(_vp)])
+_sig("sdft_batch_launch", C.c_int, [_vp])
+_sig("sdft_batch_sync", C.c_int, [_vp])
+_sig("sdft_batch_stream", _vp, [_vp])
+_sig("sdft_batch_kernel_count", C.c_longlong, [_vp])
+_sig("sdft_batch_destroy", C.c_int, [_vp])
 _sig("sdft_half_dots_noalloc", C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
 KERNEL_KINDS = ("stage_a_pack_cfft", "stage_b_plane_fft_vks", "stage_c_cfft_unpack_recur", "kb_proj_gemm",
                 "kb_back_gemm", "density_planes", "noise_planes", "other")
@@ -400,8 +408,65 @@ class Context:
         _chk(lib.sdft_density_dev(self._p, nstate, imu, scale, _d(rho) if want else None))
         return rho
 
+    def download_density(self):
+        """The last density computed on this context (no recomputation)."""
+        rho = np.zeros(self.n[0] * self.n[1] * self.n[2])
+        _chk(lib.sdft_download_density(self._p, _d(rho)))
+        return rho
+
+    def set_gemm_split(self, split):
+        """Split-K of the nonlocal projection GEMM (0 = cost model)."""
+        _chk(lib.sdft_ctx_set_gemm_split(self._p, int(split)))
+
+    @property
+    def stream_ptr(self):
+        return int(lib.sdft_ctx_stream(self._p) or 0)
+
     def download_filtered(self, nstate, imu=0):
         re = np.zeros(nstate * self.ncoef)
         im = np.zeros(nstate * self.ncoef)
         _chk(lib.sdft_download_filtered(self._p, nstate, imu, _d(re), _d(im)))
         return re, im
+
+
+class Batch:
+    """Filters + densities of several contexts (systems) captured as one CUDA
+    graph (sdft_batch_*): every context is a concurrent branch and
+    launch() replays the whole batch with one graph launch."""
+
+    def __init__(self, ctxs, nstate, L, coeffs, scale, emean, occ_over_nsto):
+        n = len(ctxs)
+        self._ctxs = list(ctxs)
+        self._coeffs = [_f64(c) for c in coeffs]
+        arr = (_vp * n)(*[c._p for c in ctxs])
+        cptr = (_dp * n)(*[_d(c) for c in self._coeffs])
+        ns, Ls = _i32(nstate), _i32(L)
+        sc, em, oc = _f64(scale), _f64(emean), _f64(occ_over_nsto)
+        p = _vp()
+        _chk(lib.sdft_batch_create(n, arr, _i(ns), _i(Ls), cptr, _d(sc), _d(em), _d(oc), C.byref(p)))
+        self._p = p
+
+    def launch(self):
+        _chk(lib.sdft_batch_launch(self._p))
+
+    def sync(self):
+        _chk(lib.sdft_batch_sync(self._p))
+
+    @property
+    def stream_ptr(self):
+        return int(lib.sdft_batch_stream(self._p) or 0)
+
+    @property
+    def kernels_per_launch(self):
+        return int(lib.sdft_batch_kernel_count(self._p))
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib.sdft_batch_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

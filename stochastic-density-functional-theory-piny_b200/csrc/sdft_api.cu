@@ -193,7 +193,8 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   g2.N = N; g2.Nst = nstate;
   const size_t stride = (size_t)N * Ppad;
   const int max_split = (int)std::min<size_t>(32, ctx->oz_part_elems / stride);
-  const int split = oz_choose_split((Ppad / 128) * (N / 128), ctx->kp_oz / 64, max_split);
+  const int split = ctx->gemm_split > 0 ? std::min(ctx->gemm_split, std::max(1, max_split))
+                                        : oz_choose_split((Ppad / 128) * (N / 128), ctx->kp_oz / 64, max_split);
   int r;
   {
     TScope ts(ctx, 3);
@@ -230,6 +231,10 @@ static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
   while (tiles * split < 2 * 148 && split < 64 && (K1 / 16) / (split * 2) >= 8 &&
          (size_t)(split * 2) * spad * ctx->Ppad <= ctx->zwork_elems)
     split *= 2;
+  if (ctx->gemm_split > 0) {  // tuned override, within the workspace and K
+    split = std::min(ctx->gemm_split, std::max(1, K1 / 16));
+    while (split > 1 && (size_t)split * spad * ctx->Ppad > ctx->zwork_elems) split--;
+  }
   {
     TScope ts(ctx, 3);
     launch_gemm_nt_f64(ctx->d_pj, K1, vec, K1, ctx->d_z, ctx->Ppad, ctx->Ppad, spad, K1, ctx->P, nstate,
@@ -965,6 +970,156 @@ extern "C" int sdft_noise_real(sdft_ctx *ctx, int nstate, double seed, int np_st
   int r = noise_core(ctx, nstate, seed, np_states, myid);
   if (r) return r;
   if ((r = download_block(ctx, ctx->d_chi, nstate, cre, cim))) return r;
+  CK(cudaStreamSynchronize(ctx->st));
+  return SDFT_OK;
+}
+
+// ============================================================================
+// Tuning knob and batched filters (one CUDA graph over several contexts)
+// ============================================================================
+extern "C" int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (split < 0 || split > 64) return set_error(SDFT_ERR_ARG, "gemm_split: 0 (cost model) or 1..64");
+  ctx->gemm_split = split;
+  return SDFT_OK;
+}
+
+struct sdft_batch {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<sdft_ctx *> ctxs;
+  std::vector<int> nstate;
+  std::vector<cudaEvent_t> evs;  // [0] fork, [1..n] joins
+  long long launches_per_replay = 0;
+};
+
+namespace sdft {
+// Every buffer the filter + density path touches, sized up front (no
+// allocation may happen while the stream is captured).
+static int prepare_filter(sdft_ctx *ctx, int nstate, int L) {
+  int r;
+  if ((r = ensure_coef(ctx, (size_t)L))) return r;
+  if ((r = ensure_acc(ctx, 1))) return r;
+  const int npairs = (nstate + 1) / 2;
+  if ((r = ensure_x(ctx, npairs))) return r;
+  if (npairs > ctx->rho_split) {
+    if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
+    ctx->d_rho_part = nullptr;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_rho_part, (size_t)npairs * ctx->N * sizeof(double)))) return r;
+    ctx->rho_split = npairs;
+  }
+  if (!ctx->d_rho && (r = dmalloc(ctx, (void **)&ctx->d_rho, (size_t)ctx->N * sizeof(double)))) return r;
+  return SDFT_OK;
+}
+}  // namespace sdft
+
+extern "C" int sdft_batch_destroy(sdft_batch *b) {
+  if (!b) return SDFT_OK;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : b->evs) cudaEventDestroy(e);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_batch_create(int n, sdft_ctx *const *ctxs, const int *nstate, const int *L,
+                                 const double *const *coeffs, const double *scale, const double *emean,
+                                 const double *occ_over_nsto, sdft_batch **out) {
+  if (!out || n < 1 || !ctxs || !nstate || !L || !coeffs || !scale || !emean || !occ_over_nsto)
+    return set_error(SDFT_ERR_ARG, "batch_create: bad argument");
+  *out = nullptr;
+  const int dev = ctxs[0] ? ctxs[0]->device : 0;
+  for (int i = 0; i < n; i++) {
+    sdft_ctx *c = ctxs[i];
+    if (!c || c->device != dev) return set_error(SDFT_ERR_ARG, "batch_create: contexts must share one device");
+    int r = check_ready(c, nstate[i]);
+    if (r) return r;
+    if (L[i] < 2 || !coeffs[i]) return set_error(SDFT_ERR_ARG, "batch_create: L >= 2 and coefficients required");
+    if (nstate[i] > c->resident) return set_error(SDFT_ERR_STATE, "batch_create: orbitals not resident");
+    for (int j = 0; j < i; j++)
+      if (ctxs[j] == c) return set_error(SDFT_ERR_ARG, "batch_create: a context appears twice");
+  }
+  cudaSetDevice(dev);
+  sdft_batch *b = new sdft_batch;
+  b->device = dev;
+  auto fail = [&](int code) { sdft_batch_destroy(b); return code; };
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? SDFT_OK : set_error(SDFT_ERR_CUDA, cudaGetErrorString(e)); };
+  int r;
+  if ((r = ck(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)))) return fail(r);
+  b->evs.resize(n + 1, nullptr);
+  for (auto &e : b->evs)
+    if ((r = ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return fail(r);
+  // buffers and coefficients, outside the capture
+  for (int i = 0; i < n; i++) {
+    sdft_ctx *c = ctxs[i];
+    if ((r = prepare_filter(c, nstate[i], L[i]))) return fail(r);
+    if ((r = ck(cudaMemcpy(c->d_coef, coeffs[i], (size_t)L[i] * sizeof(double), cudaMemcpyHostToDevice))))
+      return fail(r);
+    if ((r = ck(cudaStreamSynchronize(c->st)))) return fail(r);
+    b->ctxs.push_back(c);
+    b->nstate.push_back(nstate[i]);
+  }
+  // capture: fork every context's stream from the batch stream, record its
+  // filter + density, join back
+  std::vector<bool> timing(n);
+  long long l0 = 0;
+  for (int i = 0; i < n; i++) { timing[i] = ctxs[i]->timing; ctxs[i]->timing = false; l0 += ctxs[i]->launches; }
+  if ((r = ck(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal)))) return fail(r);
+  int rc = ck(cudaEventRecord(b->evs[0], b->st));
+  for (int i = 0; i < n && rc == SDFT_OK; i++) {
+    sdft_ctx *c = ctxs[i];
+    if ((rc = ck(cudaStreamWaitEvent(c->st, b->evs[0], 0)))) break;
+    if ((rc = filter_cheby_core(c, nstate[i], L[i], 1, scale[i], emean[i], false))) break;
+    if ((rc = density_core(c, c->d_acc, nstate[i], occ_over_nsto[i]))) break;
+    if ((rc = ck(cudaEventRecord(b->evs[i + 1], c->st)))) break;
+    if ((rc = ck(cudaStreamWaitEvent(b->st, b->evs[i + 1], 0)))) break;
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(b->st, &g);
+  for (int i = 0; i < n; i++) ctxs[i]->timing = timing[i];
+  b->graph = g;
+  if (rc) return fail(rc);
+  if ((r = ck(ee))) return fail(r);
+  if ((r = ck(cudaGraphInstantiate(&b->exec, b->graph, 0)))) return fail(r);
+  long long l1 = 0;
+  for (int i = 0; i < n; i++) { l1 += ctxs[i]->launches; ctxs[i]->filtered = nstate[i]; }
+  b->launches_per_replay = l1 - l0;
+  *out = b;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_batch_launch(sdft_batch *b) {
+  if (!b || !b->exec) return set_error(SDFT_ERR_ARG, "batch_launch: no batch");
+  cudaSetDevice(b->device);
+  CK(cudaGraphLaunch(b->exec, b->st));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_batch_sync(sdft_batch *b) {
+  if (!b) return set_error(SDFT_ERR_ARG, "batch_sync: no batch");
+  cudaSetDevice(b->device);
+  CK(cudaStreamSynchronize(b->st));
+  for (sdft_ctx *c : b->ctxs) {
+    int e = 0;
+    CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
+  }
+  return SDFT_OK;
+}
+
+extern "C" void *sdft_batch_stream(sdft_batch *b) { return b ? (void *)b->st : nullptr; }
+extern "C" long long sdft_batch_kernel_count(const sdft_batch *b) { return b ? b->launches_per_replay : 0; }
+
+extern "C" int sdft_download_density(sdft_ctx *ctx, double *rho) {
+  if (!ctx || !rho) return set_error(SDFT_ERR_ARG, "download_density: null");
+  if (!ctx->d_rho) return set_error(SDFT_ERR_STATE, "download_density: no density computed yet");
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(rho, ctx->d_rho, (size_t)ctx->N * sizeof(double), cudaMemcpyDefault, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   return SDFT_OK;
 }

@@ -70,6 +70,7 @@ struct sdft_ctx {
   // Inside a filter / moments loop, stage C records the per-orbital max of
   // the vector it writes (d_rowmax), so the next projection can form that
   // vector's digits without another pass over it.
+  int gemm_split = 0;                // projection split-K override (0: cost model)
   bool track_omax = false;
   const double *omax_vec = nullptr;  // vector whose row maxima d_rowmax holds
   int omax_n = 0;

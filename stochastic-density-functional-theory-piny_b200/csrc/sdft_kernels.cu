@@ -600,23 +600,23 @@ void launch_stage_c(const DevGeom &g, const void *X, const EpiArgs &e, int npair
     const size_t sm = plane_smem<T>(g);                                                  \
     if (E <= 512 * 2) {                                                                  \
       auto k = KERNEL<T, 512, 2>;                                                        \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);  \
+      static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), true); (void)attr_once;  \
       k<<<grid, 512, sm, st>>>(__VA_ARGS__);                                             \
     } else if (E <= 512 * 5) {                                                           \
       auto k = KERNEL<T, 512, 5>;                                                        \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);  \
+      static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), true); (void)attr_once;  \
       k<<<grid, 512, sm, st>>>(__VA_ARGS__);                                             \
     } else if (E <= 512 * 11) {                                                          \
       auto k = KERNEL<T, 512, 11>;                                                       \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);  \
+      static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), true); (void)attr_once;  \
       k<<<grid, 512, sm, st>>>(__VA_ARGS__);                                             \
     } else if (E <= 512 * 18) {                                                          \
       auto k = KERNEL<T, 512, 18>;                                                       \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);  \
+      static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), true); (void)attr_once;  \
       k<<<grid, 512, sm, st>>>(__VA_ARGS__);                                             \
     } else {                                                                             \
       auto k = KERNEL<T, 512, 24>;                                                       \
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);  \
+      static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), true); (void)attr_once;  \
       k<<<grid, 512, sm, st>>>(__VA_ARGS__);                                             \
     }                                                                                    \
   } while (0)

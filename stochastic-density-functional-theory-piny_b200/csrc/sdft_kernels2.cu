@@ -539,7 +539,7 @@ bool fast_stage_b(const DevGeom &g, void *X, const T *Vp, int npairs, cudaStream
 #define LB(A, B)                                                                               \
   do {                                                                                         \
     auto k = kf_stage_b<T, A, B>;                                                              \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);             \
+    static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true); (void)attr_once;             \
     k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, (typename CT<T>::type *)X, Vp);                    \
   } while (0)
   SDFT_FOR_PLANE(LB);
@@ -556,7 +556,7 @@ bool fast_stage_b_density(const DevGeom &g, const void *X, int npairs, double *r
 #define LD(A, B)                                                                               \
   do {                                                                                         \
     auto k = kf_stage_b_density<T, A, B>;                                                      \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);             \
+    static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true); (void)attr_once;             \
     k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, (const typename CT<T>::type *)X, rho_pair, r1, r2); \
   } while (0)
   SDFT_FOR_PLANE(LD);
@@ -574,7 +574,7 @@ bool fast_stage_b_noise(const DevGeom &g, const unsigned char *neg, int nstate, 
 #define LN(A, B)                                                                                        \
   do {                                                                                                  \
     auto k = kf_stage_b_noise<T, A, B>;                                                                 \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                      \
+    static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true); (void)attr_once;                      \
     k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, neg, nstate, pair0, (typename CT<T>::type *)X, r1, r2);   \
   } while (0)
   SDFT_FOR_PLANE(LN);

@@ -1,0 +1,204 @@
+"""Filter + density requests served with continuous batching on one GPU.
+
+A request names a system (a batch spec from workload.batch_specs), its
+number of stochastic orbitals, the polynomial order and a noise seed.  For
+every request the server
+
+1. waits until a slot is free and its device memory fits in the HBM budget
+   (admission); memory is reserved from an estimate and corrected to the
+   context's measured footprint once it exists;
+2. prepares it on its own context: V_KS, KB projectors, 20-step Lanczos
+   bounds, noise orbitals generated on the device, Chebyshev moments, mu by
+   the FP64 bisection (calcChemPotCheby) and the filter coefficients;
+3. captures its Chebyshev filter + density as a one-context CUDA graph
+   (sdft_batch) and launches it on the request's own stream, so requests
+   admitted while others run overlap on the device;
+4. when the graph's completion event fires, downloads the density, frees the
+   context and returns its memory to the budget.
+
+Requests are independent and every kernel is deterministic, so a request's
+result does not depend on what else runs beside it.
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+
+import numpy as np
+
+
+def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None):
+    """Context with resident noise orbitals and filter coefficients for one
+    system (steps 2 of the request life cycle).  mu, if given, replaces the
+    bisection result (the moments are still computed)."""
+    ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=precision, max_states=nsto,
+                      device=device)
+    ctx.set_vks(s["vks"])
+    ctx.set_kb(s["kb_desc"])
+    emin, emax = wl.lanczos_bounds(lambda r, i: ctx.calc_coef_force(r, i), s["ncoef"])
+    ediff, emean = emax - emin, 0.5 * (emin + emax)
+    scale = 2.0 / ediff
+    ctx.noise_dev(nsto, seed=seed)
+    mom = ctx.moments_dev(nsto, L, scale, emean)
+    mu_b, ne = pkg.calcChemPotCheby(L, ediff, emean, wl.BETA, wl.OCC, mom / nsto, s["num_elec"], 0.2, 0.05)
+    mu = mu_b if mu is None else mu
+    ec = pkg.calcChebyCoeff(L, ediff, emean, wl.BETA, mu, fun_flag=2)
+    if tuner is not None:  # times short filters of the resident noise (accumulators only)
+        tuner.tune(ctx, nsto, 4 * s["natm"], scale, emean)
+    return dict(ctx=ctx, ec=ec, scale=scale, emean=emean, mu=mu, num_elec=ne, occ_over=wl.OCC / nsto, nsto=nsto, L=L)
+
+
+def estimate_spec_bytes(spec, nsto, ecut=10.0, a0=10.26):
+    """estimate_bytes before the system is built: G-sphere and sphere-column
+    counts from the cell volume and cutoff (x 1.15 margin)."""
+    import math
+    rep = spec["nrep"]
+    Lc = [a0 * rep[i] * (1.0 + spec["strain"][i]) for i in range(3)]
+    vol = Lc[0] * Lc[1] * Lc[2]
+    gmax = math.sqrt(2.0 * ecut)
+    ncoef = int(vol * gmax ** 3 / (6.0 * math.pi ** 2) / 2.0) + 1
+    area = Lc[0] * Lc[1]
+    cols = int(area * gmax ** 2 / (4.0 * math.pi)) + 1
+    natm = 8 * rep[0] * rep[1] * rep[2]
+    return int(1.15 * _bytes(spec["grid"], ncoef, cols, natm, nsto))
+
+
+def _bytes(grid, ncoef, cols, natm, nsto):
+    n1, n2, n3 = grid
+    spad = (nsto + 127) // 128 * 128
+    vec = spad * 2 * ncoef * 8
+    npairs = (nsto + 1) // 2
+    P = 4 * natm
+    ppad = (P + 127) // 128 * 128
+    kp = (2 * ncoef + 63) // 64 * 64
+    mpad = (2 * ncoef + 127) // 128 * 128
+    return int(5 * vec + npairs * n3 * cols * 8 + npairs * n1 * n2 * n3 * 8 + 4 * (ppad * kp + mpad * ppad)
+               + 4 * spad * (kp + ppad) + 32 * spad * ppad * 8 + 64 * 2 ** 20)
+
+
+def estimate_bytes(s, nsto):
+    """Device footprint of one request's context (mixed precision), from the
+    sizes the library allocates: orbital blocks, FFT column scratch, density
+    partials, KB digit arrays and split-K partials."""
+    cols = len(set(zip(s["ka"][:-1].tolist(), s["kb"][:-1].tolist()))) * 2 + 1
+    return _bytes(s["grid"], s["ncoef"], cols, s["natm"], nsto)
+
+
+class Server:
+    """Continuous-batching loop over a list of timed requests.  Admission and
+    completion run on the calling thread; preparation (host set-up, moments,
+    capture, launch) runs on a pool of `workers` threads, so the host work of
+    new requests overlaps the device work of running ones (the library's calls
+    release the interpreter lock)."""
+
+    def __init__(self, pkg, wl, precision, hbm_budget=150e9, slots=16, device=0, tuner=None, workers=4):
+        self.pkg, self.wl = pkg, wl
+        self.precision = precision
+        self.budget = float(hbm_budget)
+        self.slots = int(slots)
+        self.device = device
+        self.tuner = tuner
+        self.workers = int(workers)
+
+    def _start(self, i, r, t0, t0_ev):
+        import torch
+        torch.cuda.set_device(self.device)
+        t_adm = time.perf_counter() - t0
+        s = self.wl.build_spec(r["spec"])
+        p = prepare(self.pkg, self.wl, s, r["nsto"], r["L"], self.precision, r["seed"], self.device, self.tuner,
+                    mu=r.get("mu"))
+        ctx = p["ctx"]
+        b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
+        st = torch.cuda.ExternalStream(b.stream_ptr)
+        b.launch()
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(st)
+        return dict(i=i, ctx=ctx, batch=b, ev=ev, mem=ctx.device_bytes, t_adm=t_adm, prep=p, natm=s["natm"])
+
+    def run(self, requests, keep_density=True):
+        """requests: list of dicts with arrival (s), spec, nsto, L, seed and
+        optionally mu.  Returns per-request records (latency, orbitals,
+        density ...) and a summary.  Times are seconds from the start of the
+        run: arrivals and admissions on the host clock, completions from CUDA
+        events."""
+        import torch
+        from concurrent.futures import ThreadPoolExecutor
+        order = sorted(range(len(requests)), key=lambda i: requests[i]["arrival"])
+        pending = deque(order)
+        waiting = deque()
+        starting, active = [], []
+        used = 0.0
+        rec = [None] * len(requests)
+        side = torch.cuda.Stream(device=self.device)
+        t0_ev = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        t0_ev.record(side)
+        peak_active, peak_used = 0, 0.0
+        pool = ThreadPoolExecutor(max_workers=self.workers)
+        try:
+            while pending or waiting or starting or active:
+                now = time.perf_counter() - t0
+                while pending and requests[pending[0]]["arrival"] <= now:
+                    waiting.append(pending.popleft())
+                # admission: FIFO while a slot and memory are free
+                while waiting and len(active) + len(starting) < self.slots:
+                    i = waiting[0]
+                    r = requests[i]
+                    est = estimate_spec_bytes(r["spec"], r["nsto"])
+                    if used + est > self.budget and (active or starting):
+                        break
+                    waiting.popleft()
+                    used += est
+                    starting.append((est, pool.submit(self._start, i, r, t0, t0_ev)))
+                # started requests become active (reservation -> measured footprint)
+                keep = []
+                for est, fut in starting:
+                    if fut.done():
+                        a = fut.result()
+                        used += a["mem"] - est
+                        active.append(a)
+                    else:
+                        keep.append((est, fut))
+                starting = keep
+                peak_active = max(peak_active, len(active))
+                peak_used = max(peak_used, used)
+                # completions
+                still = []
+                for a in active:
+                    if a["ev"].query():
+                        a["batch"].sync()
+                        i = a["i"]
+                        rho = a["ctx"].download_density() if keep_density else None
+                        t_done = t0_ev.elapsed_time(a["ev"]) / 1e3
+                        r = requests[i]
+                        rec[i] = dict(arrival=r["arrival"], admitted=a["t_adm"], done=t_done,
+                                      latency=t_done - r["arrival"], nsto=r["nsto"], L=r["L"], natm=a["natm"],
+                                      mu=a["prep"]["mu"],
+                                      num_elec=float(rho.sum() / rho.size) if rho is not None else None, density=rho)
+                        a["batch"].close()
+                        a["ctx"].close()
+                        used -= a["mem"]
+                    else:
+                        still.append(a)
+                active = still
+                time.sleep(0.0005)
+        finally:
+            pool.shutdown(wait=True)
+        lat = np.array([r["latency"] for r in rec])
+        span = max(r["done"] for r in rec) - min(r["arrival"] for r in rec)
+        summary = dict(requests=len(rec), orbitals=int(sum(r["nsto"] for r in rec)),
+                       orbitals_per_s=float(sum(r["nsto"] for r in rec) / span), span_s=float(span),
+                       p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                       mean_ms=float(lat.mean() * 1e3), peak_active=peak_active, peak_reserved_gb=peak_used / 1e9,
+                       workers=self.workers, slots=self.slots)
+        return rec, summary
+
+
+def poisson_requests(wl, n, rate, seed=5, big_fraction=0.1):
+    """n requests with seeded Poisson arrivals at `rate` per second drawn from
+    the batch distribution with `big_fraction` 512-atom systems."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    specs = wl.batch_specs(nsys=n, seed=seed + 1, big_fraction=big_fraction)
+    return [dict(arrival=float(t[i]), spec=specs[i], nsto=specs[i]["nsto"], L=specs[i]["L"], seed=10.0 + i)
+            for i in range(n)]

@@ -1,0 +1,70 @@
+"""Autotuner for the per-system launch shapes of the filter.
+
+The tunable shape is the split-K factor of the nonlocal projection GEMM
+(Z = Pj C: M = projectors, N = orbitals, K = 2 ncoef): few-orbital, small
+systems have only a handful of output tiles, so the K range per CTA decides
+how many of the 148 SMs work.  The built-in wave-quantisation cost model
+(choice 0) is one candidate; fixed splits are the others.  Each candidate is
+timed on a short Chebyshev filter of the context's resident orbitals (the
+filter kernels themselves, device time by CUDA events on the context
+stream), and the fastest is set on the context.  Results are cached per
+problem shape (grid, projectors, orbital tiles of 128, precision), in
+memory and optionally in a JSON file.
+
+Tuning overwrites the context's filter accumulators: run it before the real
+filter.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+CANDIDATES = (0, 1, 2, 4, 8, 16, 32)
+
+
+class Tuner:
+    def __init__(self, pkg, path=None, steps=6, candidates=CANDIDATES):
+        self.pkg = pkg
+        self.path = path
+        self.steps = int(steps)
+        self.candidates = tuple(candidates)
+        self.cache = {}
+        if path and os.path.exists(path):
+            with open(path) as f:
+                self.cache = json.load(f)
+
+    @staticmethod
+    def key(ctx, nstate, nproj):
+        # the GEMM tile grid depends on the projector count and the orbitals
+        # in 128-wide tiles; K (2 ncoef) follows from the grid
+        return f"{ctx.n[0]}x{ctx.n[1]}x{ctx.n[2]}/P{nproj}/N{(nstate + 127) // 128}/prec{ctx.precision}"
+
+    def _time(self, ctx, nstate, split, scale, emean):
+        import torch
+        ctx.set_gemm_split(split)
+        ec = np.full(self.steps + 1, 1.0 / (self.steps + 1))
+        ext = torch.cuda.ExternalStream(ctx.stream_ptr)
+        ctx.filter_cheby_dev(nstate, ec, 1, scale, emean)  # warm (buffers, caches)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        ctx.filter_cheby_dev(nstate, ec, 1, scale, emean)
+        b.record(ext)
+        ctx.sync()
+        return a.elapsed_time(b)
+
+    def tune(self, ctx, nstate, nproj, scale=0.1, emean=0.0):
+        """Pick and set the projection split-K for (ctx, nstate); returns it."""
+        k = self.key(ctx, nstate, nproj)
+        if k not in self.cache:
+            times = {str(c): self._time(ctx, nstate, c, scale, emean) for c in self.candidates}
+            best = min(times, key=times.get)
+            self.cache[k] = {"split": int(best), "ms": times}
+            if self.path:
+                with open(self.path, "w") as f:
+                    json.dump(self.cache, f, indent=1, sort_keys=True)
+        split = int(self.cache[k]["split"])
+        ctx.set_gemm_split(split)
+        return split

@@ -35,26 +35,38 @@ CONFIGS = {
     "cfg2": dict(nrep=2, grid=(48, 48, 48), nsto=128, L=256, poly="cheby", mu=None),
     "cfg3": dict(nrep=4, grid=(96, 96, 96), nsto=512, L=512, poly="cheby", mu=None),
 }
+# Batched uneven systems: supercells of 1..3 conventional cells per axis
+# (8..216 atoms), uniform +-2 % strain per axis, N(0, 0.05 bohr) displacements,
+# grid 24 per cell and axis (24..72), 16..256 orbitals, order 128..512.
+BATCH = dict(nsys=32, seed=4, strain=0.02, disp=0.05, nsto=(16, 256), L=(128, 512))
 BETA = 1000.0          # 1/Ha
 ELEC_PER_8 = 32.0      # electrons per 8 Si atoms (4 e/atom)
 OCC = 2.0              # spin-unpolarised occupation
 
 
+def _reps(nrep):
+    return (int(nrep),) * 3 if np.isscalar(nrep) else tuple(int(x) for x in nrep)
+
+
 def diamond_positions(nrep, a0=A0_SI):
+    """Fractional coordinates of an n1 x n2 x n3 (or n^3) diamond supercell."""
+    r = _reps(nrep)
     base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]], dtype=np.float64)
     basis = np.concatenate([base, base + 0.25])
-    cells = np.array([[i, j, k] for i in range(nrep) for j in range(nrep) for k in range(nrep)], dtype=np.float64)
-    frac = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) / nrep
+    cells = np.array([[i, j, k] for i in range(r[0]) for j in range(r[1]) for k in range(r[2])], dtype=np.float64)
+    frac = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) / np.array(r, dtype=np.float64)
     return frac
 
 
 def make_system(nrep=1, grid=(24, 24, 24), a0=A0_SI, strain=(0.0, 0.0, 0.0), disp_sigma=0.0, seed=0,
                 ecut=ECUT_HA, with_kb=True):
-    """Orthorhombic Si supercell.  Returns a dict with the cell, G sphere,
-    V_KS (filter layout), KB description and electron count."""
+    """Orthorhombic Si supercell (nrep: n or (n1, n2, n3) conventional cells).
+    Returns a dict with the cell, G sphere, V_KS (filter layout), KB
+    description and electron count."""
     from . import setkvec3d_sm  # noqa: PLC0415  (package-relative)
     rng = np.random.default_rng(seed)
-    L = np.array([a0 * nrep * (1.0 + s) for s in strain])
+    r = _reps(nrep)
+    L = np.array([a0 * r[i] * (1.0 + strain[i]) for i in range(3)])
     hmat = np.diag(L)
     frac = diamond_positions(nrep, a0)
     pos = frac * L
@@ -161,3 +173,32 @@ def lanczos_bounds(hpsi, ncoef, nstep=20, seed=15, margin=0.1):
     T = np.diag(alphas) + np.diag(betas[:k - 1], 1) + np.diag(betas[:k - 1], -1)
     ev = np.linalg.eigvalsh(T)
     return float(ev[0] - margin), float(ev[-1] + margin)
+
+
+def batch_specs(nsys=BATCH["nsys"], seed=BATCH["seed"], big_fraction=0.0, big_nsto=256, big_L=512):
+    """Seeded specs of uneven systems: dicts with nrep (per axis), grid,
+    strain, disp_seed, nsto (even), L (even).  The supercell shape is drawn
+    uniformly from the 27 shapes with 1..3 cells per axis (8..216 atoms).
+    With big_fraction > 0 that fraction of specs is the 512-atom 4x4x4 cell
+    on the 96^3 grid with big_nsto orbitals and order big_L."""
+    rng = np.random.default_rng(seed)
+    shapes = [(a, b, c) for a in (1, 2, 3) for b in (1, 2, 3) for c in (1, 2, 3)]
+    out = []
+    for i in range(nsys):
+        if big_fraction > 0 and rng.random() < big_fraction:
+            rep = (4, 4, 4)
+            nsto, L = big_nsto, big_L
+        else:
+            rep = shapes[int(rng.integers(len(shapes)))]
+            nsto = 2 * int(rng.integers(BATCH["nsto"][0] // 2, BATCH["nsto"][1] // 2 + 1))
+            L = 2 * int(rng.integers(BATCH["L"][0] // 2, BATCH["L"][1] // 2 + 1))
+        strain = tuple(float(x) for x in rng.uniform(-BATCH["strain"], BATCH["strain"], size=3))
+        out.append(dict(nrep=rep, grid=tuple(24 * r for r in rep), strain=strain, disp_seed=int(rng.integers(1 << 30)),
+                        nsto=nsto, L=L))
+    return out
+
+
+def build_spec(spec):
+    """The system of one batch spec."""
+    return make_system(spec["nrep"], spec["grid"], strain=spec["strain"], disp_sigma=BATCH["disp"],
+                       seed=spec["disp_seed"])

@@ -635,7 +635,9 @@ def run_serve(args):
         "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"], "mean": m["mean_ms"]},
         "mixed": m, "fp64": out_runs["fp64"],
         "mixed_speedup": m["orbitals_per_s"] / out_runs["fp64"]["orbitals_per_s"],
-        "density_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+        "density_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                                         "per_request": [[int(recs["mixed"][i]["natm"]), int(reqs[i]["nsto"]),
+                                                          int(reqs[i]["L"]), float(e)] for i, e in enumerate(errs)]},
     }
     print(json.dumps(out))
 
@@ -656,7 +658,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
-    ap.add_argument("--workers", type=int, default=4, help="cfg5: host threads preparing requests")
+    ap.add_argument("--workers", type=int, default=8, help="cfg5: host threads preparing requests")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

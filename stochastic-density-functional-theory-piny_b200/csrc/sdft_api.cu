@@ -127,6 +127,17 @@ static int ensure_x(sdft_ctx *ctx, int npairs) {
   return SDFT_OK;
 }
 
+// Pairs per chunk when the column scratch holds FP64 data (the one-off
+// transforms -- noise, density -- run in FP64 in every context); the
+// scratch is grown to at least two FP32 pairs so a chunk is never empty.
+static int fp64_chunk(sdft_ctx *ctx, int npairs, int *chunk) {
+  int r = ensure_x(ctx, std::max(npairs, 2));
+  if (r) return r;
+  const size_t per = (size_t)ctx->n3 * ctx->cols.ncols_pad * sizeof(double2);
+  *chunk = (int)std::min<size_t>((size_t)npairs, ctx->x_bytes / per);
+  return *chunk >= 1 ? SDFT_OK : set_error(SDFT_ERR_STATE, "column scratch too small");
+}
+
 static int ensure_coef(sdft_ctx *ctx, size_t n) {
   if (n <= ctx->coef_cap) return SDFT_OK;
   if (ctx->d_coef) { cudaFree(ctx->d_coef); ctx->dev_bytes -= (long long)(ctx->coef_cap * 8); }
@@ -851,9 +862,9 @@ extern "C" int sdft_cheby_moments(sdft_ctx *ctx, int nstate, const double *cre, 
 
 // Density of the orbitals held in `vec`.
 static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double scale) {
-  int r;
+  int r, chunk;
   const int npairs = (nstate + 1) / 2;
-  if ((r = ensure_x(ctx, npairs))) return r;
+  if ((r = fp64_chunk(ctx, npairs, &chunk))) return r;
   const int nsplit = npairs;  // one |psi|^2 plane set per pair, summed in pair order
   if (nsplit > ctx->rho_split) {
     if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
@@ -861,23 +872,22 @@ static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double sca
     ctx->rho_split = nsplit;
   }
   if (!ctx->d_rho) DM(ctx->d_rho, (size_t)ctx->N * sizeof(double));
-  if (ctx->fast) {
-    if (is_fp64(ctx)) {
-      { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
-      { TScope ts(ctx, 5); fast_stage_b_density<double>(ctx->g, ctx->d_x, npairs, ctx->d_rho_part, ctx->st); }
+  // one transform per pair (against 2 per pair per filter step): FP64 in
+  // every precision, in chunks of pairs that fit the column scratch
+  for (int p0 = 0; p0 < npairs; p0 += chunk) {
+    const int np = std::min(chunk, npairs - p0);
+    double *part = ctx->d_rho_part + (size_t)p0 * ctx->N;
+    if (ctx->fast) {
+      { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, vec, nstate, p0, np, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 5); fast_stage_b_density<double>(ctx->g, ctx->d_x, np, part, ctx->st); }
     } else {
-      { TScope ts(ctx, 0); fast_stage_a<float>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
-      { TScope ts(ctx, 5); fast_stage_b_density<float>(ctx->g, ctx->d_x, npairs, ctx->d_rho_part, ctx->st); }
+      { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, vec, nstate, p0, np, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 5); launch_stage_b_density<double>(ctx->g, ctx->d_x, np, np, part, ctx->st); }
     }
-  } else if (is_fp64(ctx)) {
-    { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
-    { TScope ts(ctx, 5); launch_stage_b_density<double>(ctx->g, ctx->d_x, npairs, nsplit, ctx->d_rho_part, ctx->st); }
-  } else {
-    { TScope ts(ctx, 0); launch_stage_a<float>(ctx->g, vec, nstate, 0, npairs, ctx->d_x, ctx->st); }
-    { TScope ts(ctx, 5); launch_stage_b_density<float>(ctx->g, ctx->d_x, npairs, nsplit, ctx->d_rho_part, ctx->st); }
+    ctx->launches += 2;
   }
   { TScope ts(ctx, 7); launch_density_reduce(ctx->d_rho_part, nsplit, ctx->N, scale, ctx->d_rho, ctx->st); }
-  ctx->launches += 3;
+  ctx->launches += 1;
   CK(cudaGetLastError());
   return SDFT_OK;
 }
@@ -925,30 +935,27 @@ static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int
   }
   CK(cudaMemcpyAsync(ctx->d_neg, neg.data(), n, cudaMemcpyHostToDevice, ctx->st));
   const int npairs = (nstate + 1) / 2;
-  int r;
-  if ((r = ensure_x(ctx, npairs))) return r;
+  int r, chunk;
+  if ((r = fp64_chunk(ctx, npairs, &chunk))) return r;
   CK(cudaMemsetAsync(ctx->d_chi, 0, ctx->vec_elems * sizeof(double), ctx->st));
-  EpiArgs e = base_epi(ctx);
-  e.mode = EPI_NOISE;
-  e.nstate = nstate;
-  e.OUT = ctx->d_chi;
-  e.invN = 1.0 / (double)ctx->N;
-  if (ctx->fast) {
-    if (is_fp64(ctx)) {
-      { TScope ts(ctx, 6); fast_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
-      { TScope ts(ctx, 2); fast_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+  // the noise orbitals are input data: FP64 transforms in every precision
+  for (int p0 = 0; p0 < npairs; p0 += chunk) {
+    const int np = std::min(chunk, npairs - p0);
+    EpiArgs e = base_epi(ctx);
+    e.mode = EPI_NOISE;
+    e.nstate = nstate;
+    e.pair0 = p0;
+    e.OUT = ctx->d_chi;
+    e.invN = 1.0 / (double)ctx->N;
+    if (ctx->fast) {
+      { TScope ts(ctx, 6); fast_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, p0, np, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 2); fast_stage_c<double>(ctx->g, ctx->d_x, e, np, ctx->st); }
     } else {
-      { TScope ts(ctx, 6); fast_stage_b_noise<float>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
-      { TScope ts(ctx, 2); fast_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+      { TScope ts(ctx, 6); launch_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, p0, np, ctx->d_x, ctx->st); }
+      { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, np, ctx->st); }
     }
-  } else if (is_fp64(ctx)) {
-    { TScope ts(ctx, 6); launch_stage_b_noise<double>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
-    { TScope ts(ctx, 2); launch_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
-  } else {
-    { TScope ts(ctx, 6); launch_stage_b_noise<float>(ctx->g, ctx->d_neg, nstate, 0, npairs, ctx->d_x, ctx->st); }
-    { TScope ts(ctx, 2); launch_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
+    ctx->launches += 2;
   }
-  ctx->launches += 2;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->st));
   ctx->resident = nstate;
@@ -1003,7 +1010,7 @@ static int prepare_filter(sdft_ctx *ctx, int nstate, int L) {
   if ((r = ensure_coef(ctx, (size_t)L))) return r;
   if ((r = ensure_acc(ctx, 1))) return r;
   const int npairs = (nstate + 1) / 2;
-  if ((r = ensure_x(ctx, npairs))) return r;
+  if ((r = ensure_x(ctx, std::max(npairs, 2)))) return r;  // as fp64_chunk needs it
   if (npairs > ctx->rho_split) {
     if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
     ctx->d_rho_part = nullptr;

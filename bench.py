@@ -131,6 +131,66 @@ def algorithmic(kind, s, nsto, csz):
     return "hbm", None
 
 
+# DRAM bytes from ncu captures (profiles/): kf_stage_b<float,96,96> per
+# orbital pair (136.5 + 74.8 MB for 64 pairs, scaled by pairs); the KB GEMMs
+# per launch at 512 orbitals (full-size capture, mean of the projection
+# 1.14 GB + 63.8 MB and the back projection 865.8 + 398.0 MB)
+PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 74.8e6) / 64}
+PROFILED_GEMM_TRAFFIC = {((96, 96, 96), True, 512): (1.14e9 + 63.8e6 + 865.8e6 + 398.0e6) / 2}
+
+KERNEL_OF = {"stage_a_pack_cfft": "kf_stage_a", "stage_b_plane_fft_vks": "kf_stage_b",
+             "stage_c_cfft_unpack_recur": "kf_stage_c", "kb_proj_gemm": "kb_gemm", "kb_back_gemm": "kb_gemm",
+             "density_planes": "kf_stage_b_density"}
+
+
+def rooflines(timing, s, nsto, mixed):
+    """Roofline of every kernel function with an algorithmic model, largest
+    total time first.  Tensor: the KB GEMMs (projection and back projection,
+    one kernel) -- mixed: int8 tcgen05 ops (10 digit products per FP64-
+    equivalent multiply-add) against 2 x the measured bf16 burst peak (B200's
+    dense int8 rate is twice its bf16 rate); FP64: DMMA flops against the
+    nominal 40 TFLOP/s FP64 tensor rate.  HBM: algorithmic bytes (algorithmic())
+    against the measured copy bandwidth."""
+    pk, src = peaks()
+    csz = 8 if mixed else 16
+    agg = {}
+    for kind, (ms, n) in timing.items():
+        kern = KERNEL_OF.get(kind)
+        if kern is None or n == 0:
+            continue
+        bound, work = algorithmic(kind, s, nsto, csz)
+        a = agg.setdefault(kern, [bound, 0.0, 0, 0.0])
+        a[1] += ms
+        a[2] += n
+        a[3] += work * n
+    out = []
+    for kern, (bound, ms, n, work) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+        t = ms / 1e3
+        if bound == "hbm":
+            ach = work / t / 1e9
+            peak = pk["hbm_gbs"]
+            tr = PROFILED_TRAFFIC.get((kern, tuple(s["grid"]), mixed))
+            out.append({"kernel": kern, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                        "frac": ach / peak, "traffic": tr * ((nsto + 1) // 2) if tr else None,
+                        "peak_source": src, "ms_total": ms, "launches": n})
+        else:
+            if mixed:
+                ach = 10.0 * work / t / 1e12
+                peak = 2.0 * pk["bf16_tflops"]
+                psrc = f"int8 dense = 2 x {src} bf16 burst ({pk['bf16_tflops']})"
+                name = "kb_gemm (k_gemm_oz8, int8 tcgen05)"
+            else:
+                ach = work / t / 1e12
+                peak = 40.0
+                psrc = "nominal FP64 tensor (DMMA) rate"
+                name = "kb_gemm (k_gemm_nt_f64, DMMA)"
+            out.append({"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                        "frac": ach / peak, "traffic": PROFILED_GEMM_TRAFFIC.get((tuple(s["grid"]), mixed, nsto)),
+                        "peak_source": psrc, "ms_total": ms, "launches": n,
+                        "fp64_equivalent_tflops": work / t / 1e12})
+    return out
+
+
 def ncols_of(s):
     ka, kb = s["ka"][:-1], s["kb"][:-1]
     cols = set(zip(ka.tolist(), kb.tolist()))
@@ -221,10 +281,39 @@ def run_ours(args):
         t = torch.tensor([tot_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
-    clocks = clk.stop() if rank == 0 else None
+    clocks = None
     launches = ctx.launches - launches0
     timing = ctx.read_timing()
     ctx.set_timing(False)
+    eager = {"orbitals_per_s": args.steps * nsto * world / (tot_ms / 1e3), "ms_per_step": tot_ms / args.steps,
+             "launches_per_step": launches / args.steps, "note": "per-kernel event timing on"}
+    # ---- the same step as one CUDA-graph launch (sdft_batch of this context);
+    # the small configurations are launch-bound when issued kernel by kernel
+    graph = None
+    if world == 1 and not args.no_graph:
+        bt = pkg.Batch([ctx], [nsto], [L], [ec], [scale], [emean], [occ_over])
+        gst = torch.cuda.ExternalStream(bt.stream_ptr, device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            bt.launch()
+        bt.sync()
+        gevs = []
+        for _ in range(args.steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(gst)
+            bt.launch()
+            b.record(gst)
+            gevs.append((a, b))
+        bt.sync()
+        g_ms = [a.elapsed_time(b) for a, b in gevs]
+        graph = {"ms": g_ms, "kernels_per_launch": bt.kernels_per_launch}
+        bt.close()
+    if rank == 0:
+        clocks = clk.stop()
+    if graph:
+        step_ms = graph["ms"]
+        tot_ms = sum(step_ms)
+        launches = graph["kernels_per_launch"] * args.steps
     value = args.steps * nsto * world / (tot_ms / 1e3)
 
     # ---- e2e: the public host-buffer API, H2D of chi and D2H of results
@@ -274,15 +363,30 @@ def run_ours(args):
         c64.set_kb(s["kb_desc"])
         c64.upload(*chi_h)
         ctx.upload(*chi_h)
-        ext64 = torch.cuda.ExternalStream(pkg.lib.sdft_ctx_stream(c64._p), device=f"cuda:{local}")
-        c64.filter_cheby_dev(nsto, ec, 1, scale, emean)  # warm-up
+        # timed the same way as the mixed step (one graph launch, or eager)
+        if graph:
+            b64 = pkg.Batch([c64], [nsto], [L], [ec], [scale], [emean], [occ_over])
+            ext64 = torch.cuda.ExternalStream(b64.stream_ptr, device=f"cuda:{local}")
+            run64 = b64.launch
+        else:
+            b64 = None
+            ext64 = torch.cuda.ExternalStream(pkg.lib.sdft_ctx_stream(c64._p), device=f"cuda:{local}")
+
+            def run64():
+                c64.filter_cheby_dev(nsto, ec, 1, scale, emean)
+                c64.density_dev(nsto, 0, occ_over, want=False)
+        run64()  # warm-up
         c64.sync()
+        if b64:
+            b64.sync()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(ext64)
-        c64.filter_cheby_dev(nsto, ec, 1, scale, emean)
-        r64 = c64.density_dev(nsto, 0, occ_over, want=False)
+        run64()
         b.record(ext64)
+        if b64:
+            b64.sync()
+            b64.close()
         c64.sync()
         ms64 = a.elapsed_time(b)
         rho64 = c64.density_dev(nsto, 0, occ_over)
@@ -313,25 +417,9 @@ def run_ours(args):
                 "num_elec_density": float(rho64.sum() / rho64.size)}
         c64.close()
 
-    # ---- roofline for the dominant kernel
-    pk, src = peaks()
-    csz = 8 if prec == pkg.SDFT_PREC_MIXED else 16
-    dom = max(timing.items(), key=lambda kv: kv[1][0])
-    kind, (kms, kn) = dom
-    bound, work = algorithmic(kind, s, nsto, csz)
-    roof = None
-    if work is not None and kn > 0:
-        per_launch_s = kms / 1e3 / kn
-        if bound == "hbm":
-            ach = work / per_launch_s / 1e9
-            peak = pk["hbm_gbs"]
-            roof = {"kernel": kind, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "traffic": None, "peak_source": src}
-        else:
-            ach = work / per_launch_s / 1e12
-            peak = pk["bf16_tflops_sustained"]
-            roof = {"kernel": kind, "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                    "frac": ach / peak, "traffic": None, "peak_source": src + " bf16 sustained"}
+    # ---- roofline: per kernel function, the dominant one first
+    roof_all = rooflines(timing, s, nsto, prec == pkg.SDFT_PREC_MIXED)
+    roof = roof_all[0] if roof_all else None
     kernel_table = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / max(1e-9, sum(x[0] for x in
                     timing.values()))} for k, v in timing.items() if v[1]}
 
@@ -351,7 +439,8 @@ def run_ours(args):
                    "emin": emin, "emax": emax, "l2": "inputs (orbitals 0.43 GB/GPU) larger than L2; no flush",
                    "setup_s": setup_s, "noise_host_s": noise_s, "parallelism": f"state-parallel x{world}"},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)]},
-        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "kernels": kernel_table, "fp64": fp64,
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "roofline_kernels": roof_all,
+        "kernels": kernel_table, "eager": eager, "step_launch": "one CUDA graph" if graph else "eager", "fp64": fp64,
         "cpu_baseline": cpu, "clocks": clocks,
     }
     ctx.close()
@@ -656,6 +745,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="time the eager step only")
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
     ap.add_argument("--workers", type=int, default=8, help="cfg5: host threads preparing requests")

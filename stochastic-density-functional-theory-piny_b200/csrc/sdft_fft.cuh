@@ -22,16 +22,53 @@ template <> struct CT<float> { using type = float2; };
 template <typename C> __device__ __forceinline__ C cmk(double r, double i) {
   C c; c.x = (decltype(c.x))r; c.y = (decltype(c.y))i; return c;
 }
+// FP32 complex arithmetic on the packed f32x2 pipe (sm_100): one
+// instruction per complex add/sub/scale, two per complex multiply.
+__device__ __forceinline__ unsigned long long pk2(float x, float y) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a.x, a.y)), "l"(pk2(b.x, b.y)), "l"(pk2(c.x, c.y)));
+  return upk2(r);
+}
+
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return add2(a, b); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return sub2(a, b); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// (a.x b.x - a.y b.y, a.x b.y + a.y b.x) = a.x (b.x, b.y) + a.y (-b.y, b.x)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return fma2(make_float2(a.y, a.y), make_float2(-b.y, b.x), mul2(make_float2(a.x, a.x), b));
 }
+// s * (a.x, a.y) for a real s
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return mul2(a, make_float2(s, s)); }
 // multiply by (dir * i): dir=-1 -> -i, dir=+1 -> +i
 template <int DIR, typename C> __device__ __forceinline__ C mul_i(C a) {
   C r;
@@ -56,8 +93,8 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft_small(
     const T hs = (T)0.86602540378443864676372317075294;  // sqrt(3)/2
     C s = cadd(v[1], v[2]);
     C d = csub(v[1], v[2]);
-    C m; m.x = v[0].x - (T)0.5 * s.x; m.y = v[0].y - (T)0.5 * s.y;
-    C rot = mul_i<DIR>(d); rot.x *= hs; rot.y *= hs;
+    const C m = csub(v[0], cscale(s, (T)0.5));
+    const C rot = cscale(mul_i<DIR>(d), hs);
     v[0] = cadd(v[0], s);
     v[1] = cadd(m, rot);
     v[2] = csub(m, rot);

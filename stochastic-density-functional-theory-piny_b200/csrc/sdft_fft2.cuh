@@ -108,10 +108,21 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dftr(C *v)
 struct Lines1 {  // lines at l*ls
   int ls;
   __device__ __forceinline__ int base(int l) const { return l * ls; }
+  __device__ __forceinline__ bool valid(int) const { return true; }
 };
 struct Lines2 {  // two contiguous groups of lines (rows 0..n1-1 and the top ones)
   int nl1, ls, off2;
   __device__ __forceinline__ int base(int l) const { return (l < nl1) ? l * ls : off2 + (l - nl1) * ls; }
+  __device__ __forceinline__ bool valid(int) const { return true; }
+};
+// Two groups of rows (n1r rows from row 0, n2r rows from offset off2), each
+// enumerated over a multiple of 16 lanes (g1, g2): every half-warp then
+// touches 16 consecutive rows of one group, which with an odd row pitch
+// (in complex elements) hit disjoint banks.  Padding lanes are not valid.
+struct Lines2P {
+  int n1r, g1, n2r, ls, off2;
+  __device__ __forceinline__ int base(int l) const { return (l < g1) ? l * ls : off2 + (l - g1) * ls; }
+  __device__ __forceinline__ bool valid(int l) const { return (l < g1) ? (l < n1r) : (l - g1 < n2r); }
 };
 
 // Unit (line l, index j) enumeration for the passes below: lines vary
@@ -143,6 +154,7 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, 
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {
       const int l = it.l, j2 = it.j;
+      if (!lm.valid(l)) continue;
       C *p = buf + lm.base(l);
       C v[R1];
 #pragma unroll
@@ -162,6 +174,7 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, 
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {
       const int l = it.l, k1 = it.j;
+      if (!lm.valid(l)) continue;
       C *p = buf + lm.base(l) + R2 * k1 * ES;
       C v[R2];
 #pragma unroll
@@ -182,6 +195,7 @@ __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, 
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {
       const int l = it.l, k1 = it.j;
+      if (!lm.valid(l)) continue;
       C *p = buf + lm.base(l) + R2 * k1 * ES;
       C v[R2];
 #pragma unroll
@@ -201,6 +215,7 @@ __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, 
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {
       const int l = it.l, j2 = it.j;
+      if (!lm.valid(l)) continue;
       C *p = buf + lm.base(l);
       C v[R1];
 #pragma unroll

@@ -253,6 +253,7 @@ template <int N1> struct RowsPerm {  // rows given in permuted-a order
     const int ka = (l <= kamax) ? l : N1 - (2 * kamax + 1) + l;
     return pos<N1>(ka) * ls;
   }
+  __device__ __forceinline__ bool valid(int) const { return true; }
 };
 
 // a-direction transform pair of one plane with the V multiply fused in:
@@ -298,11 +299,7 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
     for (int j = 0; j < R2; j++) v[j] = p[j * P2];
     dftr<R2, +1>(v);
 #pragma unroll
-    for (int j = 0; j < R2; j++) {
-      const T w = vp[(size_t)j * N2];
-      v[j].x *= w;
-      v[j].y *= w;
-    }
+    for (int j = 0; j < R2; j++) v[j] = cscale(v[j], vp[(size_t)j * N2]);
     dftr<R2, -1>(v);
     p[0] = v[0];
 #pragma unroll
@@ -356,9 +353,12 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
     pl[(ab >> 16) * P2 + (ab & 0xffff)] = Xrow[col];
   }
   __syncthreads();
-  dif<N2, 1, +1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
+  // b-transforms over the sphere rows, each row group padded to 16 lanes
+  const int g1 = (ka + 1 + 15) & ~15, g2 = (ka + 15) & ~15;
+  const Lines2P rowsp{ka + 1, g1, ka, P2, (N1 - ka) * P2};
+  dif<N2, 1, +1>(pl, rowsp, g1 + g2, tw2, tid, NT);
   plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, tw1, tid, NT);
-  dit<N2, 1, -1>(pl, rows, 2 * ka + 1, tw2, tid, NT);
+  dit<N2, 1, -1>(pl, rowsp, g1 + g2, tw2, tid, NT);
   for (int col = tid; col < g.ncols; col += NT) {
     const int ab = g.col_ab[col];
     Xrow[col] = pl[(ab >> 16) * P2 + (ab & 0xffff)];

@@ -225,7 +225,9 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   }
   {
     TScope ts(ctx, 4);
-    r = run_gemm_oz(g2, 1, ctx->d_fnl, 0, ctx->d_err, ctx->st);
+    // FNL in FP32 (its rounding is below the FP32 transforms' error in the
+    // same force); stage C reads it through EpiArgs::FNLf
+    r = run_gemm_oz(g2, 1, reinterpret_cast<float *>(ctx->d_fnl), 0, ctx->d_err, ctx->st);
     ctx->launches++;
   }
   return r;
@@ -274,7 +276,8 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
   e.nstate = nstate;
   e.pair0 = 0;
   e.C = cur;
-  e.FNL = ctx->P ? ctx->d_fnl : nullptr;
+  if (ctx->P && ctx->oz) e.FNLf = reinterpret_cast<const float *>(ctx->d_fnl);
+  else e.FNL = ctx->P ? ctx->d_fnl : nullptr;
   e.invN = 1.0 / (double)ctx->N;
   if (ctx->oz && ctx->track_omax && e.OUT) {
     if (ctx->rowmax_zero_n < nstate) CK(cudaMemsetAsync(ctx->d_rowmax, 0, (size_t)nstate * 8, ctx->st));
@@ -331,6 +334,20 @@ static EpiArgs base_epi(sdft_ctx *ctx) {
   return e;
 }
 
+// The filter sum acc = sum_k a_k v_k is updated every other step: step k
+// (odd, >= 3) adds a_{k-1} v_{k-1} + a_k v_k -- v_{k-1} is the step's input
+// vector, which the epilogue reads anyway -- and even steps skip the
+// accumulator, except the last step (then only a_k v_k).  Same terms, half
+// the accumulator traffic.
+static void pair_accumulation(sdft_ctx *ctx, EpiArgs &e, int k, int L, int nmu) {
+  if (k < 2) return;
+  if (k % 2 == 0) {
+    if (k != L - 1) e.ACC = nullptr;
+  } else {
+    e.acoefp = ctx->d_coef + (size_t)(k - 1) * nmu;
+  }
+}
+
 // Chebyshev filter on resident chi (d_chi) -> d_acc.  moments (device, may
 // be null): per step dots written to d_mom[k*3 .. k*3+2].
 static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double scale, double emean,
@@ -350,6 +367,7 @@ static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double s
     e.nmu = nmu;
     e.acoef = ctx->d_coef + (size_t)k * nmu;
     e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
+    pair_accumulation(ctx, e, k, L, nmu);
     e.CHI = ctx->d_chi;
     if (k == 1) {
       e.mode = EPI_CHEB1;
@@ -389,6 +407,7 @@ static int filter_newton_core(sdft_ctx *ctx, int nstate, int L, int nmu, const d
     e.nmu = nmu;
     e.acoef = ctx->d_coef + (size_t)k * nmu;
     e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
+    pair_accumulation(ctx, e, k, L, nmu);
     e.s1 = s1; e.s2 = s2;
     e.pre = -scale * emean - samp[k - 1];
     if ((r = apply_h(ctx, cur, nstate, e, false))) return r;

@@ -48,10 +48,11 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, 
       "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
 }
 
+template <typename OutT>
 __global__ void __launch_bounds__(192, 1)
 k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int ktiles_total,
            int ktiles_per_split, const double *__restrict__ sa, const double *__restrict__ sb,
-           double *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
+           OutT *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
   using S = OzSmem;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
@@ -149,7 +150,7 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
         if (n < Nst) {
           const long long v = ((long long)(int)r0[j] << 21) + ((long long)(int)r1[j] << 14) +
                               ((long long)(int)r2[j] << 7) + (long long)(int)r3[j];
-          out[(size_t)blockIdx.z * split_stride + (size_t)n * ldo + m] = row_ok ? (double)v * fa * sb[n] : 0.0;
+          out[(size_t)blockIdx.z * split_stride + (size_t)n * ldo + m] = (OutT)(row_ok ? (double)v * fa * sb[n] : 0.0);
         }
       }
     }
@@ -332,7 +333,8 @@ int oz_choose_split(int tiles, int ktiles, int max_split) {
   return best;
 }
 
-int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st) {
+template <typename OutT>
+static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_stride, int *err, cudaStream_t st) {
   const int ktiles = (g.K + OZ_BK - 1) / OZ_BK;
   if (g.M % OZ_BM || g.N % OZ_BN || ktiles < 1) return set_error(SDFT_ERR_ARG, "oz gemm: shape");
   if (split < 1) split = 1;
@@ -340,15 +342,20 @@ int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, in
   const int kps = (ktiles + split - 1) / split;
   if (kps * OZ_BK > OZ_MAX_KRANGE) return set_error(SDFT_ERR_ARG, "oz gemm: K range per CTA too long");
   split = (ktiles + kps - 1) / kps;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_gemm_oz8, cudaFuncAttributeMaxDynamicSharedMemorySize, OzSmem::TOTAL);
-    attr = true;
-  }
+  static const bool attr_once =
+      (cudaFuncSetAttribute(k_gemm_oz8<OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, OzSmem::TOTAL), true);
+  (void)attr_once;
   dim3 grid(g.N / OZ_BN, g.M / OZ_BM, split);
-  k_gemm_oz8<<<grid, 192, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
-                                                 g.Mst, g.Nst, err);
+  k_gemm_oz8<OutT><<<grid, 192, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
+                                                       g.Mst, g.Nst, err);
   return SDFT_OK;
+}
+
+int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st) {
+  return run_gemm_oz_t<double>(g, split, out, split_stride, err, st);
+}
+int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st) {
+  return run_gemm_oz_t<float>(g, split, out, split_stride, err, st);
 }
 
 void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {

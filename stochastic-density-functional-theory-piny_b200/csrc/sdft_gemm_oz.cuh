@@ -37,6 +37,8 @@ bool gemm_oz_available();
 int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld);
 // split == 1: out = result; split > 1: FP64 partial z at out + z*split_stride.
 int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st);
+// the same with FP32 output (rounded once from the exact FP64 tile value)
+int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st);
 // split count for `tiles` output tiles over `ktiles` K tiles (<= max_split)
 int oz_choose_split(int tiles, int ktiles, int max_split);
 // rowmax[r] = bits of max_k |x[r][k]| (zeroed first); rows x cols, pitch ldx

@@ -46,9 +46,12 @@ struct EpiArgs {
   double *OUT;           // output vector (may alias PREV or C)
   const double *CHI;     // chi (moment dots)
   const double *FNL;     // nonlocal force or nullptr
+  const float *FNLf;     // the same in FP32 (mixed precision), or nullptr
   double *ACC;           // [nmu][S][2][ngp] or nullptr
   const double *acoef;   // device: a[k*nmu + imu] of this step (nmu values)
   const double *acoef0;  // device: a[imu] (k = 0) when initialising ACC, else nullptr
+  const double *acoefp;  // device: a[(k-1)*nmu + imu] when this step also adds the
+                         // previous vector (C): ACC += a_{k-1} C + a_k OUT; else nullptr
   int nmu;
   size_t acc_stride;     // elements between ACC chem-pot blocks
   double s1, s2, pre;    // G!=0 scale, G=0 scale, c coefficient

@@ -97,6 +97,9 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
   if (e.FNL) {
     fr += e.FNL[o];
     fi += e.FNL[o + g.ngp];
+  } else if (e.FNLf) {
+    fr += (double)e.FNLf[o];
+    fi += (double)e.FNLf[o + g.ngp];
   }
   if (!g0) {
     const double k2 = 2.0 * g.ak2[gi];
@@ -129,6 +132,10 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
         const double a0 = e.acoef0[imu];
         A[o] = a0 * cr + a * nr;
         A[o + g.ngp] = a0 * ci + a * ni;
+      } else if (e.acoefp) {
+        const double ap = e.acoefp[imu];
+        A[o] += ap * cr + a * nr;
+        A[o + g.ngp] += ap * ci + a * ni;
       } else {
         A[o] += a * nr;
         A[o + g.ngp] += a * ni;

@@ -191,7 +191,7 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   {
     TScope ts(ctx, 7);
     // row maxima: from the stage C that wrote `vec`, else one pass over it
-    if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {
+    if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
       launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);
       ctx->launches++;
     }
@@ -279,20 +279,28 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
   if (ctx->P && ctx->oz) e.FNLf = reinterpret_cast<const float *>(ctx->d_fnl);
   else e.FNL = ctx->P ? ctx->d_fnl : nullptr;
   e.invN = 1.0 / (double)ctx->N;
-  if (ctx->oz && ctx->track_omax && e.OUT) {
+  if (ctx->oz && ctx->track_omax && e.OUT) {  // (row maxima exist only for the digit GEMMs)
     if (ctx->rowmax_zero_n < nstate) CK(cudaMemsetAsync(ctx->d_rowmax, 0, (size_t)nstate * 8, ctx->st));
     e.omax = ctx->d_rowmax;
   }
+  // inside a loop the previous stage C already packed and c-transformed `cur`
+  // into the column scratch; this step's stage C does the same for OUT when
+  // another application follows
+  const bool fuse = ctx->fast && ctx->track_omax && !is_fp64(ctx);
+  const bool have_x = fuse && ctx->x_vec == cur && ctx->x_n == nstate;
+  e.Xnext = (fuse && e.pack_next && e.OUT) ? ctx->d_x : nullptr;
+  int nl = 3;
   if (ctx->fast) {
     if (is_fp64(ctx)) {
-      { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      if (!have_x) { TScope ts(ctx, 0); fast_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
       { TScope ts(ctx, 1); fast_stage_b<double>(ctx->g, ctx->d_x, (const double *)ctx->d_vp, npairs, ctx->st); }
       { TScope ts(ctx, 2); fast_stage_c<double>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
     } else {
-      { TScope ts(ctx, 0); fast_stage_a<float>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
+      if (!have_x) { TScope ts(ctx, 0); fast_stage_a<float>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
       { TScope ts(ctx, 1); fast_stage_b<float>(ctx->g, ctx->d_x, (const float *)ctx->d_vp, npairs, ctx->st); }
       { TScope ts(ctx, 2); fast_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
     }
+    if (have_x) nl = 2;
   } else if (is_fp64(ctx)) {
     { TScope ts(ctx, 0); launch_stage_a<double>(ctx->g, cur, nstate, 0, npairs, ctx->d_x, ctx->st); }
     { TScope ts(ctx, 1); launch_stage_b<double>(ctx->g, ctx->d_x, (const double *)ctx->d_vp, npairs, ctx->st); }
@@ -302,21 +310,24 @@ static int apply_h(sdft_ctx *ctx, const double *cur, int nstate, EpiArgs e, bool
     { TScope ts(ctx, 1); launch_stage_b<float>(ctx->g, ctx->d_x, (const float *)ctx->d_vp, npairs, ctx->st); }
     { TScope ts(ctx, 2); launch_stage_c<float>(ctx->g, ctx->d_x, e, npairs, ctx->st); }
   }
-  ctx->launches += 3;
+  ctx->launches += nl;
   CK(cudaGetLastError());
   if (e.omax) {
     ctx->omax_vec = e.OUT;
     ctx->omax_n = nstate;
     ctx->rowmax_zero_n = 0;
   }
+  ctx->x_vec = e.Xnext ? e.OUT : nullptr;
+  ctx->x_n = nstate;
   return SDFT_OK;
 }
 
-// Row-maximum tracking for the duration of one filter / moments loop.
+// For the duration of one filter / moments loop: row-maximum tracking (mixed
+// precision) and the stage A fused into the previous stage C (fast path).
 struct OmaxScope {
   sdft_ctx *c;
-  explicit OmaxScope(sdft_ctx *ctx) : c(ctx) { c->track_omax = c->oz; c->omax_vec = nullptr; }
-  ~OmaxScope() { c->track_omax = false; c->omax_vec = nullptr; }
+  explicit OmaxScope(sdft_ctx *ctx) : c(ctx) { c->track_omax = true; c->omax_vec = nullptr; c->x_vec = nullptr; }
+  ~OmaxScope() { c->track_omax = false; c->omax_vec = nullptr; c->x_vec = nullptr; }
 };
 
 static int check_ready(sdft_ctx *ctx, int nstate) {
@@ -368,6 +379,7 @@ static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double s
     e.acoef = ctx->d_coef + (size_t)k * nmu;
     e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
     pair_accumulation(ctx, e, k, L, nmu);
+    e.pack_next = k + 1 < L;
     e.CHI = ctx->d_chi;
     if (k == 1) {
       e.mode = EPI_CHEB1;
@@ -408,6 +420,7 @@ static int filter_newton_core(sdft_ctx *ctx, int nstate, int L, int nmu, const d
     e.acoef = ctx->d_coef + (size_t)k * nmu;
     e.acoef0 = (k == 1) ? ctx->d_coef : nullptr;
     pair_accumulation(ctx, e, k, L, nmu);
+    e.pack_next = k + 1 < L;
     e.s1 = s1; e.s2 = s2;
     e.pre = -scale * emean - samp[k - 1];
     if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
@@ -432,6 +445,7 @@ static int moments_core(sdft_ctx *ctx, int nstate, int L, double scale, double e
     e.OUT = out;
     e.CHI = ctx->d_chi;
     e.dots = ctx->d_dots;
+    e.pack_next = k + 1 < std::max(M, 2);
     if (k == 1) {
       e.mode = EPI_CHEB1;
       e.ndots = 2;

@@ -75,6 +75,8 @@ struct sdft_ctx {
   const double *omax_vec = nullptr;  // vector whose row maxima d_rowmax holds
   int omax_n = 0;
   int rowmax_zero_n = 0;             // d_rowmax[0, n) known to be zero
+  const double *x_vec = nullptr;     // vector whose packed columns d_x holds (fast path, in loops)
+  int x_n = 0;
   int *d_err = nullptr;
   // per-kind event timing (sdft_ctx_set_timing)
   bool timing = false;

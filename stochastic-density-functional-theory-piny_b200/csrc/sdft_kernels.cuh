@@ -58,6 +58,9 @@ struct EpiArgs {
   double *dots;          // per-CTA partials [pairs][nbatch][3] or nullptr
   int ndots;             // 1 (filter moments) or 3 (doubling)
   double invN;
+  void *Xnext;           // column scratch to receive the packed, c-transformed OUT
+                         // (stage A of the next H application; fast path), or nullptr
+  bool pack_next;        // set by the loops: a next application follows this step
   unsigned long long *omax;  // per orbital: atomicMax of max|OUT| (bits of a
                              // non-negative double; +inf if not finite), or nullptr
 };

@@ -84,13 +84,16 @@ kf_stage_a(DevGeom g, const double *__restrict__ C, int nstate, int pair0, typen
 // ---------------------------------------------------------------------------
 struct Dots2 { double d0, d1, d2; };
 
+// Writes OUT for orbital s at G index gi and returns the written pair in
+// (wr, wi).
 __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, int s, int gi, bool g0, double fr,
-                                          double fi, Dots2 &dt, double &mx) {
+                                          double fi, Dots2 &dt, double &mx, double &wr, double &wi) {
   const size_t o = (size_t)s * 2 * g.ngp + gi;
   if (e.mode == EPI_NOISE) {
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
     mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
+    wr = fr; wi = fi;
     return;
   }
   const double cr = e.C[o], ci = e.C[o + g.ngp];
@@ -112,6 +115,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
     mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
+    wr = fr; wi = fi;
     return;
   }
   const double sc = g0 ? e.s2 : e.s1;
@@ -124,6 +128,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
   e.OUT[o] = nr;
   e.OUT[o + g.ngp] = ni;
   mx = fmax(mx, fmax(absmax_key_d(nr), absmax_key_d(ni)));
+  wr = nr; wi = ni;
   if (e.ACC) {
     for (int imu = 0; imu < e.nmu; imu++) {
       double *A = e.ACC + imu * e.acc_stride;
@@ -155,13 +160,19 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
   }
 }
 
+// X is not __restrict__: with e.Xnext the CTA overwrites its own columns of
+// the same scratch (read into shared memory at the start) for the next step.
 template <typename T, int N3>
 __global__ void __launch_bounds__(kColThreads, 4)
-kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
+kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   using C2 = typename CT<T>::type;
   constexpr int P3 = N3 + 1;
   __shared__ __align__(16) C2 tw[N3];
   __shared__ __align__(16) C2 buf[2 * kCPB * P3];
+  // packed OUT columns for the next step (e.Xnext; FP32 columns only: the
+  // FP64 instance has no room for a second buffer in static shared memory)
+  constexpr bool kCanPack = sizeof(T) == 4;
+  __shared__ __align__(16) C2 nbuf[kCanPack ? 2 * kCPB * P3 : 1];
   __shared__ double red[kColThreads / 32][3];
   const int tid = threadIdx.x;
   const int cp0 = blockIdx.x * kCPB;
@@ -178,6 +189,9 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
     const int r = i / ncl, cl = i - r * ncl;
     buf[cl * P3 + r] = Xp[(size_t)r * g.ncols_pad + col0 + cl];
   }
+  const bool pack = kCanPack && e.Xnext != nullptr;
+  if (pack)
+    for (int i = tid; i < ncl * P3; i += kColThreads) nbuf[i] = cmk<C2>(0.0, 0.0);
   __syncthreads();
   dit<N3, 1, -1>(buf, Lines1{P3}, ncl, tw, tid, kColThreads);
   Dots2 dt{0.0, 0.0, 0.0};
@@ -212,15 +226,22 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
           f2r = -0.5 * (ti + tic);
           f2i = -0.5 * (trc - tr);
         }
-        epilogue2(g, e, s1, gi, false, f1r, f1i, dt, mx1);
-        if (has2) epilogue2(g, e, s2, gi, false, f2r, f2i, dt, mx2);
+        double ar, ai, cr2 = 0.0, ci2 = 0.0;
+        epilogue2(g, e, s1, gi, false, f1r, f1i, dt, mx1, ar, ai);
+        if (has2) epilogue2(g, e, s2, gi, false, f2r, f2i, dt, mx2, cr2, ci2);
+        if (pack) {  // stage A's packing of the pair (c1 + i c2) at +kc and -kc
+          nbuf[lc * P3 + kd] = cmk<C2>(ar - ci2, ai + cr2);
+          nbuf[lm * P3 + km] = cmk<C2>(ar + ci2, -ai + cr2);
+        }
       } else {
         const int g0 = g.ncoef - 1;
         const C2 F = buf[lc * P3];
         const double tr = (double)F.x * invN, ti = (double)F.y * invN;
         const double m = noise ? -1.0 : -2.0;
-        epilogue2(g, e, s1, g0, true, m * tr, 0.0, dt, mx1);
-        if (has2) epilogue2(g, e, s2, g0, true, m * ti, 0.0, dt, mx2);
+        double ar, ai, cr2 = 0.0, ci2 = 0.0;
+        epilogue2(g, e, s1, g0, true, m * tr, 0.0, dt, mx1, ar, ai);
+        if (has2) epilogue2(g, e, s2, g0, true, m * ti, 0.0, dt, mx2, cr2, ci2);
+        if (pack) nbuf[lc * P3] = cmk<C2>(ar, cr2);
       }
     }
   }
@@ -242,6 +263,15 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *__restrict__ X, EpiArgs e) {
       for (int w = 0; w < kColThreads / 32; w++) { a += red[w][0]; b += red[w][1]; c += red[w][2]; }
       double *dst = e.dots + ((size_t)p * g.nbatch + blockIdx.x) * 3;
       dst[0] = a; dst[1] = b; dst[2] = c;
+    }
+  }
+  if (pack) {  // the next application's stage A: forward c-transform, store columns
+    __syncthreads();
+    dif<N3, 1, +1>(nbuf, Lines1{P3}, ncl, tw, tid, kColThreads);
+    C2 *Xn = reinterpret_cast<C2 *>(e.Xnext) + (size_t)blockIdx.y * N3 * g.ncols_pad;
+    for (int i = tid; i < N3 * ncl; i += kColThreads) {
+      const int r = i / ncl, cl = i - r * ncl;
+      Xn[(size_t)r * g.ncols_pad + col0 + cl] = nbuf[cl * P3 + r];
     }
   }
 }

@@ -86,10 +86,14 @@ struct Dots2 { double d0, d1, d2; };
 
 // Writes OUT for orbital s at G index gi and returns the written pair in
 // (wr, wi).
+// HOT: a filter step (Chebyshev or Newton, no moment dots): the noise,
+// H-psi and dot branches are compiled out, which keeps the hot instance
+// within 64 registers without spills.
+template <bool HOT>
 __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, int s, int gi, bool g0, double fr,
                                           double fi, Dots2 &dt, double &mx, double &wr, double &wi) {
   const size_t o = (size_t)s * 2 * g.ngp + gi;
-  if (e.mode == EPI_NOISE) {
+  if (!HOT && e.mode == EPI_NOISE) {
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
     mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
@@ -111,7 +115,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
   } else {
     fi = 0.0;
   }
-  if (e.mode == EPI_HPSI) {
+  if (!HOT && e.mode == EPI_HPSI) {
     e.OUT[o] = fr;
     e.OUT[o + g.ngp] = fi;
     mx = fmax(mx, fmax(absmax_key_d(fr), absmax_key_d(fi)));
@@ -147,7 +151,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
       }
     }
   }
-  if (e.dots) {
+  if (!HOT && e.dots) {
     const double wr = g0 ? 1.0 : 2.0;
     const double xr = e.CHI[o], xi = e.CHI[o + g.ngp];
     dt.d0 += wr * xr * nr + 2.0 * xi * ni;
@@ -162,7 +166,7 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
 
 // X is not __restrict__: with e.Xnext the CTA overwrites its own columns of
 // the same scratch (read into shared memory at the start) for the next step.
-template <typename T, int N3>
+template <typename T, int N3, bool HOT>
 __global__ void __launch_bounds__(kColThreads, 4)
 kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   using C2 = typename CT<T>::type;
@@ -198,7 +202,7 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   double mx1 = 0.0, mx2 = 0.0;
   const int warp = tid >> 5, lane = tid & 31;
   const double invN = e.invN;
-  const bool noise = (e.mode == EPI_NOISE);
+  const bool noise = !HOT && (e.mode == EPI_NOISE);
   for (int cp = cp0 + warp; cp < cp1; cp += kColThreads / 32) {
     const int lc = 2 * (cp - cp0);
     const bool zc = (cp == g.ncp - 1);
@@ -227,8 +231,8 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
           f2i = -0.5 * (trc - tr);
         }
         double ar, ai, cr2 = 0.0, ci2 = 0.0;
-        epilogue2(g, e, s1, gi, false, f1r, f1i, dt, mx1, ar, ai);
-        if (has2) epilogue2(g, e, s2, gi, false, f2r, f2i, dt, mx2, cr2, ci2);
+        epilogue2<HOT>(g, e, s1, gi, false, f1r, f1i, dt, mx1, ar, ai);
+        if (has2) epilogue2<HOT>(g, e, s2, gi, false, f2r, f2i, dt, mx2, cr2, ci2);
         if (pack) {  // stage A's packing of the pair (c1 + i c2) at +kc and -kc
           nbuf[lc * P3 + kd] = cmk<C2>(ar - ci2, ai + cr2);
           nbuf[lm * P3 + km] = cmk<C2>(ar + ci2, -ai + cr2);
@@ -239,8 +243,8 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
         const double tr = (double)F.x * invN, ti = (double)F.y * invN;
         const double m = noise ? -1.0 : -2.0;
         double ar, ai, cr2 = 0.0, ci2 = 0.0;
-        epilogue2(g, e, s1, g0, true, m * tr, 0.0, dt, mx1, ar, ai);
-        if (has2) epilogue2(g, e, s2, g0, true, m * ti, 0.0, dt, mx2, cr2, ci2);
+        epilogue2<HOT>(g, e, s1, g0, true, m * tr, 0.0, dt, mx1, ar, ai);
+        if (has2) epilogue2<HOT>(g, e, s2, g0, true, m * ti, 0.0, dt, mx2, cr2, ci2);
         if (pack) nbuf[lc * P3] = cmk<C2>(ar, cr2);
       }
     }
@@ -249,7 +253,7 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
     __shared__ double mred[kColThreads / 32][2];
     omax_flush(e.omax, s1, s2, has2, mx1, mx2, mred);
   }
-  if (e.dots) {
+  if (!HOT && e.dots) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       dt.d0 += __shfl_down_sync(0xffffffffu, dt.d0, off);
@@ -563,7 +567,12 @@ bool fast_stage_a(const DevGeom &g, const double *C, int nstate, int pair0, int 
 template <typename T>
 bool fast_stage_c(const DevGeom &g, const void *X, const EpiArgs &e, int npairs, cudaStream_t st) {
   dim3 grid(g.nbatch, npairs);
-#define LC(N) kf_stage_c<T, N><<<grid, kColThreads, 0, st>>>(g, (const typename CT<T>::type *)X, e)
+  const bool hot = e.dots == nullptr && (e.mode == EPI_CHEB1 || e.mode == EPI_CHEBK || e.mode == EPI_NEWTON);
+#define LC(N)                                                                                \
+  do {                                                                                       \
+    if (hot) kf_stage_c<T, N, true><<<grid, kColThreads, 0, st>>>(g, (const typename CT<T>::type *)X, e);  \
+    else kf_stage_c<T, N, false><<<grid, kColThreads, 0, st>>>(g, (const typename CT<T>::type *)X, e);     \
+  } while (0)
   SDFT_FOR_N3(LC);
 #undef LC
   return true;

@@ -239,3 +239,24 @@ def test_mixed_hpsi_tensor_core(pkg, which, ns, request):
     assert abs(e - oe) < 1e-6 * abs(oe)
     c.sync()
     c.close()
+
+
+def test_mixed_newton_and_moments_close_to_fp64(pkg, sys1):
+    """Mixed-precision Newton filter (in-place recurrence, paired accumulation,
+    fused packing of the next step) and Chebyshev moments against FP64."""
+    cd = _ctx(pkg, sys1, 6, prec=0)
+    cm = _ctx(pkg, sys1, 6, prec=1)
+    emin, emax = -1.0, 45.0
+    scale = 4.0 / (emax - emin)
+    samp, unsc = pkg.genSampNewtonHermit(48, -2.0, 2.0, scale, emin)
+    ec = pkg.genCoeffNewtonHermit(48, 0.2, 1000.0, samp, unsc)
+    cr, ci = cd.genNoiseOrbitalReal(6, seed=12.0)
+    (a,), (b,) = cd.filterNewtonPolyHerm(cr, ci, ec, samp, 1, scale, 0.5 * (emin + emax))
+    (x,), (y,) = cm.filterNewtonPolyHerm(cr, ci, ec, samp, 1, scale, 0.5 * (emin + emax))
+    assert rel_l2(np.concatenate([x, y]), np.concatenate([a, b])) < 1e-5
+    s2, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    md = cd.calcChebyMoments(cr, ci, 33, s2, em)
+    mm = cm.calcChebyMoments(cr, ci, 33, s2, em)
+    assert np.max(np.abs(mm - md)) < 1e-6 * np.max(np.abs(md))
+    cd.close()
+    cm.close()

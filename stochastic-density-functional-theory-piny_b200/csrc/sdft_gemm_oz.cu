@@ -2,7 +2,7 @@
 // (Ozaki scheme: split each operand into int8 digits under a per-row
 // power-of-two scale, multiply digit slices exactly, recombine exactly).
 //
-// CTA = 6 warps over one 128 x 128 output tile and one K range:
+// CTA = 10 warps over one 128 x 128 output tile and one K range:
 //   warp 0    TMA producer: per 64-wide K tile one 3-D box per operand
 //             carrying all four digit slices (64 B rows, 64B swizzle),
 //             three-stage ring of 64 KB stages;
@@ -10,7 +10,8 @@
 //             columns, one per digit order q = s + t) and single-thread
 //             issuer of tcgen05.mma.kind::i8 (10 slice pairs x 2 K steps
 //             of 32 per stage);
-//   warps 2-5 epilogue: tcgen05.ld 32x32b of the four accumulators,
+//   warps 2-9 epilogue (two per TMEM lane quadrant, one column half each):
+//             tcgen05.ld 32x32b of the four accumulators,
 //             exact int64 combination acc0 2^21 + acc1 2^14 + acc2 2^7 +
 //             acc3, one conversion to FP64 (exact: |value| < 2^53 for K
 //             ranges below 2^20), scaling by 2^(Ea+Eb-33), coalesced store.
@@ -48,8 +49,11 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, 
       "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
 }
 
+constexpr int OZ_EPI_WARPS = 8;                 // two per TMEM lane quadrant
+constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
+
 template <typename OutT>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(OZ_THREADS, 1)
 k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int ktiles_total,
            int ktiles_per_split, const double *__restrict__ sa, const double *__restrict__ sb,
            OutT *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
@@ -127,16 +131,18 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
       }
       mma_commit(bar_tmem);  // accumulators complete (also fires when nkt == 0)
     }
-  } else {  // epilogue warps 2..5: TMEM lane quadrant = warp % 4
+  } else {  // epilogue warps 2..9: TMEM lane quadrant = warp % 4, column half = (warp - 2) / 4
     const int qd = warp & 3;
+    const int half = (warp - 2) >> 2;
     const bool ok = mbar_wait(bar_tmem, 0, err);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int m = m0 + 32 * qd + lane;
     const bool row_ok = ok && m < Mst && nkt > 0;
     const double fa = row_ok ? sa[m] * 0x1p-33 : 0.0;
     const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
+    constexpr int CH = OZ_BN / 16 / 2;  // 16-column chunks per epilogue warp
 #pragma unroll 1
-    for (int c = 0; c < OZ_BN / 16; c++) {
+    for (int c = half * CH; c < (half + 1) * CH; c++) {
       uint32_t r0[16], r1[16], r2[16], r3[16];
       tmem_ld16(tl + 0 * OZ_BN + c * 16, r0);
       tmem_ld16(tl + 1 * OZ_BN + c * 16, r1);
@@ -346,7 +352,7 @@ static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_str
       (cudaFuncSetAttribute(k_gemm_oz8<OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, OzSmem::TOTAL), true);
   (void)attr_once;
   dim3 grid(g.N / OZ_BN, g.M / OZ_BM, split);
-  k_gemm_oz8<OutT><<<grid, 192, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
+  k_gemm_oz8<OutT><<<grid, OZ_THREADS, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
                                                        g.Mst, g.Nst, err);
   return SDFT_OK;
 }

@@ -166,6 +166,96 @@ __device__ __forceinline__ void epilogue2(const DevGeom &g, const EpiArgs &e, in
 
 // X is not __restrict__: with e.Xnext the CTA overwrites its own columns of
 // the same scratch (read into shared memory at the start) for the next step.
+// Filter-step epilogue for both orbitals of a pair at G index gi: every load
+// of both orbitals is issued before any store (OUT may alias PREV, so a load
+// placed after a store could not be moved above it), which doubles the loads
+// in flight per thread.  Same arithmetic as epilogue2 for CHEB1 / CHEBK /
+// NEWTON without dots; returns the written values (a: s1, b: s2).
+__device__ __forceinline__ void epilogue_pair_hot(const DevGeom &g, const EpiArgs &e, int s1, bool has2, int gi,
+                                                  bool g0, double f1r, double f1i, double f2r, double f2i,
+                                                  double &mx1, double &mx2, double &ar, double &ai, double &br,
+                                                  double &bi) {
+  const size_t n = g.ngp;
+  const size_t o1 = (size_t)s1 * 2 * n + gi, o2 = o1 + 2 * n;
+  const bool rec = e.mode == EPI_CHEBK;
+  const bool acc1 = e.ACC && e.nmu == 1 && !e.acoef0;
+  double c1r = e.C[o1], c1i = e.C[o1 + n], c2r = 0.0, c2i = 0.0;
+  double x1r = 0.0, x1i = 0.0, x2r = 0.0, x2i = 0.0;
+  double p1r = 0.0, p1i = 0.0, p2r = 0.0, p2i = 0.0;
+  double q1r = 0.0, q1i = 0.0, q2r = 0.0, q2i = 0.0;
+  if (has2) { c2r = e.C[o2]; c2i = e.C[o2 + n]; }
+  if (e.FNLf) {
+    x1r = e.FNLf[o1]; x1i = e.FNLf[o1 + n];
+    if (has2) { x2r = e.FNLf[o2]; x2i = e.FNLf[o2 + n]; }
+  } else if (e.FNL) {
+    x1r = e.FNL[o1]; x1i = e.FNL[o1 + n];
+    if (has2) { x2r = e.FNL[o2]; x2i = e.FNL[o2 + n]; }
+  }
+  if (rec) {
+    p1r = e.PREV[o1]; p1i = e.PREV[o1 + n];
+    if (has2) { p2r = e.PREV[o2]; p2i = e.PREV[o2 + n]; }
+  }
+  if (acc1) {
+    q1r = e.ACC[o1]; q1i = e.ACC[o1 + n];
+    if (has2) { q2r = e.ACC[o2]; q2i = e.ACC[o2 + n]; }
+  }
+  const double k2 = g0 ? 0.0 : 2.0 * g.ak2[gi];
+  f1r += x1r - k2 * c1r;
+  f2r += x2r - k2 * c2r;
+  f1i += x1i - k2 * c1i;
+  f2i += x2i - k2 * c2i;
+  const double sc = g0 ? e.s2 : e.s1;
+  ar = sc * f1r + e.pre * c1r;
+  br = sc * f2r + e.pre * c2r;
+  ai = g0 ? 0.0 : (e.s1 * f1i + e.pre * c1i);
+  bi = g0 ? 0.0 : (e.s1 * f2i + e.pre * c2i);
+  if (rec) {
+    ar -= p1r;
+    br -= p2r;
+    if (!g0) { ai -= p1i; bi -= p2i; }
+  }
+  e.OUT[o1] = ar;
+  e.OUT[o1 + n] = ai;
+  mx1 = fmax(mx1, fmax(absmax_key_d(ar), absmax_key_d(ai)));
+  if (has2) {
+    e.OUT[o2] = br;
+    e.OUT[o2 + n] = bi;
+    mx2 = fmax(mx2, fmax(absmax_key_d(br), absmax_key_d(bi)));
+  }
+  if (!e.ACC) return;
+  if (acc1) {
+    const double a = e.acoef[0];
+    const double ap = e.acoefp ? e.acoefp[0] : 0.0;
+    e.ACC[o1] = q1r + ap * c1r + a * ar;
+    e.ACC[o1 + n] = q1i + ap * c1i + a * ai;
+    if (has2) {
+      e.ACC[o2] = q2r + ap * c2r + a * br;
+      e.ACC[o2 + n] = q2i + ap * c2i + a * bi;
+    }
+    return;
+  }
+  for (int k = 0; k < (has2 ? 2 : 1); k++) {
+    const size_t o = k ? o2 : o1;
+    const double cr = k ? c2r : c1r, ci = k ? c2i : c1i, nr = k ? br : ar, ni = k ? bi : ai;
+    for (int imu = 0; imu < e.nmu; imu++) {
+      double *A = e.ACC + imu * e.acc_stride;
+      const double a = e.acoef[imu];
+      if (e.acoef0) {
+        const double a0 = e.acoef0[imu];
+        A[o] = a0 * cr + a * nr;
+        A[o + n] = a0 * ci + a * ni;
+      } else if (e.acoefp) {
+        const double ap = e.acoefp[imu];
+        A[o] += ap * cr + a * nr;
+        A[o + n] += ap * ci + a * ni;
+      } else {
+        A[o] += a * nr;
+        A[o + n] += a * ni;
+      }
+    }
+  }
+}
+
 template <typename T, int N3, bool HOT>
 __global__ void __launch_bounds__(kColThreads, 4)
 kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
@@ -231,8 +321,12 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
           f2i = -0.5 * (trc - tr);
         }
         double ar, ai, cr2 = 0.0, ci2 = 0.0;
-        epilogue2<HOT>(g, e, s1, gi, false, f1r, f1i, dt, mx1, ar, ai);
-        if (has2) epilogue2<HOT>(g, e, s2, gi, false, f2r, f2i, dt, mx2, cr2, ci2);
+        if constexpr (HOT) {
+          epilogue_pair_hot(g, e, s1, has2, gi, false, f1r, f1i, f2r, f2i, mx1, mx2, ar, ai, cr2, ci2);
+        } else {
+          epilogue2<HOT>(g, e, s1, gi, false, f1r, f1i, dt, mx1, ar, ai);
+          if (has2) epilogue2<HOT>(g, e, s2, gi, false, f2r, f2i, dt, mx2, cr2, ci2);
+        }
         if (pack) {  // stage A's packing of the pair (c1 + i c2) at +kc and -kc
           nbuf[lc * P3 + kd] = cmk<C2>(ar - ci2, ai + cr2);
           nbuf[lm * P3 + km] = cmk<C2>(ar + ci2, -ai + cr2);
@@ -243,8 +337,12 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
         const double tr = (double)F.x * invN, ti = (double)F.y * invN;
         const double m = noise ? -1.0 : -2.0;
         double ar, ai, cr2 = 0.0, ci2 = 0.0;
-        epilogue2<HOT>(g, e, s1, g0, true, m * tr, 0.0, dt, mx1, ar, ai);
-        if (has2) epilogue2<HOT>(g, e, s2, g0, true, m * ti, 0.0, dt, mx2, cr2, ci2);
+        if constexpr (HOT) {
+          epilogue_pair_hot(g, e, s1, has2, g0, true, m * tr, 0.0, m * ti, 0.0, mx1, mx2, ar, ai, cr2, ci2);
+        } else {
+          epilogue2<HOT>(g, e, s1, g0, true, m * tr, 0.0, dt, mx1, ar, ai);
+          if (has2) epilogue2<HOT>(g, e, s2, g0, true, m * ti, 0.0, dt, mx2, cr2, ci2);
+        }
         if (pack) nbuf[lc * P3] = cmk<C2>(ar, cr2);
       }
     }

@@ -748,7 +748,7 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="time the eager step only")
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
-    ap.add_argument("--workers", type=int, default=8, help="cfg5: host threads preparing requests")
+    ap.add_argument("--workers", type=int, default=16, help="cfg5: host threads preparing requests")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -228,6 +228,24 @@ void noise_rank_seeds(double seed, int np_states, double *out) {
 // which case the value is +0 (not negative).  The trig sign is evaluated
 // with the same libm calls as the Gaussian path, so the result matches it
 // exactly; only sqrt/log are skipped.  neg[i] = 1 if value < 0.
+// cos(2 pi phi) < 0 and sin(2 pi phi) < 0 for the uniform phi in (0, 1):
+// away from the zero crossings (phi = 1/4, 1/2, 3/4, 1) by more than 1e-9 the
+// sign is decided by comparing phi (the argument 2 pi phi is formed to
+// ~1e-16, so libm cannot disagree there); within the margin the same libm
+// call as the Gaussian path decides, so the result is identical to it.
+static inline bool cos_neg(double phi, double arg) {
+  const double d = 1e-9;
+  if (phi > 0.25 + d && phi < 0.75 - d) return true;
+  if (phi < 0.25 - d || (phi > 0.75 + d && phi < 1.0 - d)) return false;
+  return std::cos(arg) < 0.0;
+}
+static inline bool sin_neg(double phi, double arg) {
+  const double d = 1e-9;
+  if (phi > 0.5 + d && phi < 1.0 - d) return true;
+  if (phi > d && phi < 0.5 - d) return false;
+  return std::sin(arg) < 0.0;
+}
+
 void gauss_signs(long long nran, double *qseed, unsigned char *neg) {
   const double twopi = 2.0 * M_PI;
   long long loop = nran / 2;
@@ -238,8 +256,8 @@ void gauss_signs(long long nran, double *qseed, unsigned char *neg) {
     double phi = ran_uniform(qseed);
     double arg = twopi * phi;
     bool zero_al = (r == 1.0);
-    neg[2 * i] = (!zero_al && std::cos(arg) < 0.0) ? 1 : 0;
-    neg[2 * i + 1] = (!zero_al && std::sin(arg) < 0.0) ? 1 : 0;
+    neg[2 * i] = (!zero_al && cos_neg(phi, arg)) ? 1 : 0;
+    neg[2 * i + 1] = (!zero_al && sin_neg(phi, arg)) ? 1 : 0;
   }
   if (nran % 2 != 0) {
     double r = ran_uniform(qseed);
@@ -247,7 +265,7 @@ void gauss_signs(long long nran, double *qseed, unsigned char *neg) {
     r = std::min(r, 1.0);
     double phi = ran_uniform(qseed);
     double arg = twopi * phi;
-    neg[nran - 1] = (r != 1.0 && std::cos(arg) < 0.0) ? 1 : 0;
+    neg[nran - 1] = (r != 1.0 && cos_neg(phi, arg)) ? 1 : 0;
   }
 }
 }  // namespace sdft

@@ -31,21 +31,28 @@ def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None)
     """Context with resident noise orbitals and filter coefficients for one
     system (steps 2 of the request life cycle).  mu, if given, replaces the
     bisection result (the moments are still computed)."""
+    t = [time.perf_counter()]
     ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=precision, max_states=nsto,
                       device=device)
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
+    t.append(time.perf_counter())
     emin, emax = wl.lanczos_bounds(lambda r, i: ctx.calc_coef_force(r, i), s["ncoef"])
     ediff, emean = emax - emin, 0.5 * (emin + emax)
     scale = 2.0 / ediff
+    t.append(time.perf_counter())
     ctx.noise_dev(nsto, seed=seed)
+    t.append(time.perf_counter())
     mom = ctx.moments_dev(nsto, L, scale, emean)
+    t.append(time.perf_counter())
     mu_b, ne = pkg.calcChemPotCheby(L, ediff, emean, wl.BETA, wl.OCC, mom / nsto, s["num_elec"], 0.2, 0.05)
     mu = mu_b if mu is None else mu
     ec = pkg.calcChebyCoeff(L, ediff, emean, wl.BETA, mu, fun_flag=2)
     if tuner is not None:  # times short filters of the resident noise (accumulators only)
         tuner.tune(ctx, nsto, 4 * s["natm"], scale, emean)
-    return dict(ctx=ctx, ec=ec, scale=scale, emean=emean, mu=mu, num_elec=ne, occ_over=wl.OCC / nsto, nsto=nsto, L=L)
+    phases = dict(context_s=t[1] - t[0], lanczos_s=t[2] - t[1], noise_s=t[3] - t[2], moments_s=t[4] - t[3])
+    return dict(ctx=ctx, ec=ec, scale=scale, emean=emean, mu=mu, num_elec=ne, occ_over=wl.OCC / nsto, nsto=nsto, L=L,
+                phases=phases)
 
 
 def estimate_spec_bytes(spec, nsto, ecut=10.0, a0=10.26):
@@ -104,11 +111,15 @@ class Server:
         import torch
         torch.cuda.set_device(self.device)
         t_adm = time.perf_counter() - t0
+        tb = time.perf_counter()
         s = self.wl.build_spec(r["spec"])
+        build_s = time.perf_counter() - tb
         p = prepare(self.pkg, self.wl, s, r["nsto"], r["L"], self.precision, r["seed"], self.device, self.tuner,
                     mu=r.get("mu"))
         ctx = p["ctx"]
+        tc = time.perf_counter()
         b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
+        p["phases"].update(build_s=build_s, capture_s=time.perf_counter() - tc)
         st = torch.cuda.ExternalStream(b.stream_ptr)
         b.launch()
         ev = torch.cuda.Event(enable_timing=True)
@@ -174,7 +185,8 @@ class Server:
                         rec[i] = dict(arrival=r["arrival"], admitted=a["t_adm"], done=t_done,
                                       latency=t_done - r["arrival"], nsto=r["nsto"], L=r["L"], natm=a["natm"],
                                       mu=a["prep"]["mu"],
-                                      num_elec=float(rho.sum() / rho.size) if rho is not None else None, density=rho)
+                                      num_elec=float(rho.sum() / rho.size) if rho is not None else None, density=rho,
+                                      phases=a["prep"]["phases"])
                         a["batch"].close()
                         a["ctx"].close()
                         used -= a["mem"]
@@ -190,7 +202,8 @@ class Server:
                        orbitals_per_s=float(sum(r["nsto"] for r in rec) / span), span_s=float(span),
                        p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
                        mean_ms=float(lat.mean() * 1e3), peak_active=peak_active, peak_reserved_gb=peak_used / 1e9,
-                       workers=self.workers, slots=self.slots)
+                       workers=self.workers, slots=self.slots,
+                       prep_mean_s={k: float(np.mean([r["phases"][k] for r in rec])) for k in rec[0]["phases"]})
         return rec, summary
 
 

@@ -110,7 +110,11 @@ def algorithmic(kind, s, nsto, csz):
 
     stage A: read the orbitals (16 B/coef) + write the column scratch;
     stage B: read + write the column scratch + V_KS once;
-    stage C: read scratch + c, T_{k-2}, FNL, ACC; write T_k, ACC (all FP64);
+    stage C: read the scratch, c and T_{k-2}, write T_k (FP64 orbitals);
+    read FNL (FP32 in mixed precision, FP64 otherwise); the filter sum is
+    read and written every other step (one orbital block per step on
+    average); mixed precision also packs the next step's columns (write one
+    column scratch) in place of a stage A launch;
     GEMMs: 2*P*nsto*2*ncoef flops."""
     npairs = (nsto + 1) // 2
     n1, n2, n3 = s["grid"]
@@ -123,7 +127,9 @@ def algorithmic(kind, s, nsto, csz):
     if kind == "stage_b_plane_fft_vks":
         return "hbm", 2 * xb + n1 * n2 * n3 * (csz // 2)
     if kind == "stage_c_cfft_unpack_recur":
-        return "hbm", xb + 7 * vec
+        if csz == 8:
+            return "hbm", 2 * xb + 4.5 * vec
+        return "hbm", xb + 5 * vec
     if kind in ("kb_proj_gemm", "kb_back_gemm"):
         return "tensor", 2.0 * s["_P"] * nsto * 2 * ncoef
     if kind == "density_planes":
@@ -131,11 +137,13 @@ def algorithmic(kind, s, nsto, csz):
     return "hbm", None
 
 
-# DRAM bytes from ncu captures (profiles/): kf_stage_b<float,96,96> per
-# orbital pair (136.5 + 75.2 MB for 64 pairs, scaled by pairs); the KB GEMMs
+# DRAM bytes from ncu captures (profiles/): kf_stage_b<float,96,96> and
+# kf_stage_c<float,96,1> per orbital pair (136.5 + 75.2 MB and 294.2 +
+# 301.1 MB for 64 pairs, scaled by pairs); the KB GEMMs
 # per launch at 512 orbitals (full-size capture, mean of the projection
 # 1.14 GB + 63.8 MB and the back projection 865.8 + 398.0 MB)
-PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 75.2e6) / 64}
+PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 75.2e6) / 64,
+                    ("kf_stage_c", (96, 96, 96), True): (294.2e6 + 301.1e6) / 64}
 PROFILED_GEMM_TRAFFIC = {((96, 96, 96), True, 512): (1.14e9 + 63.8e6 + 865.8e6 + 398.0e6) / 2}
 
 KERNEL_OF = {"stage_a_pack_cfft": "kf_stage_a", "stage_b_plane_fft_vks": "kf_stage_b",

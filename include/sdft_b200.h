@@ -24,6 +24,7 @@
  *   sdft_density                      <- rhoCalcRealStoHybrid stodft/density.c:43 (+ sum_rho mathlib/fft_package.c:2502)
  *   sdft_noise_real                   <- genNoiseOrbitalReal stodft/gen-noise.c:162
  *   sdft_gaussran2                    <- gaussran2 / ran_essl / DURAND mathlib/mathlib.c:118,30; mathlib/blas_wrappers.f:39
+ *   sdft_gaussran2_signs_dev          <- the gaussran2 call of genNoiseOrbitalReal, stodft/gen-noise.c:256 (signs only)
  */
 #ifndef SDFT_B200_H
 #define SDFT_B200_H
@@ -246,6 +247,13 @@ int sdft_newton_coeff(int L, int num_chem_pot, const double *chem_pot, double be
                       double *expan_coeff);
 /* gaussran2 with the DURAND uniform generator; qseed updated in place. */
 int sdft_gaussran2(int nran, double *qseed, double *gauss);
+/* Signs of gaussran2(nran, *qseed) generated on the device: neg (device
+ * memory, nran bytes) gets 1 where the value is negative, 0 elsewhere --
+ * the sign pattern genNoiseOrbitalReal (stodft/gen-noise.c:256) turns into
+ * noise.  Byte-identical to the host generator; *qseed is left where
+ * gaussran2 leaves it.  Runs on `stream` (cudaStream_t, 0 = default) and
+ * synchronises it. */
+int sdft_gaussran2_signs_dev(long long nran, double *qseed, unsigned char *neg, void *stream);
 
 #ifdef __cplusplus
 }

@@ -135,6 +135,7 @@ _sig("sdft_chempot_cheby", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double
 _sig("sdft_newton_samp", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp])
 _sig("sdft_newton_coeff", C.c_int, [C.c_int, C.c_int, _dp, C.c_double, _dp, _dp, _dp])
 _sig("sdft_gaussran2", C.c_int, [C.c_int, _dp, _dp])
+_sig("sdft_gaussran2_signs_dev", C.c_int, [C.c_longlong, _dp, _vp, _vp])
 
 
 def _chk(rc):
@@ -228,6 +229,15 @@ def gaussran2(nran, seed):
     out = np.zeros(max(nran, 1))
     _chk(lib.sdft_gaussran2(nran, C.byref(q), _d(out)))
     return out[:nran], q.value
+
+
+def gaussran2_signs_dev(nran, seed, out_ptr, stream_ptr=0):
+    """Signs of gaussran2(nran, seed) (1 = negative) written as bytes to the
+    device buffer at out_ptr (nran bytes) on the device generator; returns the
+    generator state gaussran2 leaves."""
+    q = C.c_double(seed)
+    _chk(lib.sdft_gaussran2_signs_dev(int(nran), C.byref(q), C.c_void_p(out_ptr), C.c_void_p(stream_ptr)))
+    return q.value
 
 
 # ---------------------------------------------------------------------------

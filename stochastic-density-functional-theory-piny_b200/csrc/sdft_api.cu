@@ -14,6 +14,7 @@
 #include "sdft_kernels.cuh"
 #include "sdft_ctx.h"
 #include "sdft_kernels2.cuh"
+#include "sdft_noise.h"
 
 namespace sdft {
 
@@ -606,7 +607,8 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
   void *ptrs[] = {ctx->d_cp_gstart, ctx->d_cp_gcount, ctx->d_col_ab, ctx->d_gkc, ctx->d_ak2, ctx->d_tw,
                   ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
                   ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
-                  ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_enl,
+                  ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_noise_scratch,
+                  ctx->d_enl,
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
                   ctx->d_oz_part};
@@ -952,21 +954,26 @@ extern "C" int sdft_density_dev(sdft_ctx *ctx, int nstate, int imu, double scale
   return SDFT_OK;
 }
 
-// Noise: host signs of gaussran2 (sequential generator), device FFT to G.
+// Noise: signs of gaussran2 on the device (sdft_noise.cu: the DURAND
+// sequence jumped ahead per thread, identical to the host generator), then
+// the FFT to G.
 static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int myid) {
   if (np_states < 1 || myid < 0 || myid >= np_states) return set_error(SDFT_ERR_ARG, "noise: rank");
   std::vector<double> seeds(np_states);
   noise_rank_seeds(seed, np_states, seeds.data());
   double q = seeds[myid];
   const size_t n = (size_t)nstate * ctx->N;
-  std::vector<unsigned char> neg(n);
-  gauss_signs((long long)n, &q, neg.data());
   if (n > ctx->neg_cap) {
     if (ctx->d_neg) { cudaFree(ctx->d_neg); ctx->dev_bytes -= (long long)ctx->neg_cap; }
     DM(ctx->d_neg, n);
     ctx->neg_cap = n;
   }
-  CK(cudaMemcpyAsync(ctx->d_neg, neg.data(), n, cudaMemcpyHostToDevice, ctx->st));
+  if (!ctx->d_noise_scratch) DM(ctx->d_noise_scratch, noise_scratch_bytes());
+  {
+    int nk = 0, r0 = device_gauss_signs((long long)n, &q, ctx->d_neg, ctx->d_noise_scratch, ctx->st, &nk);
+    ctx->launches += nk;
+    if (r0) return r0;
+  }
   const int npairs = (nstate + 1) / 2;
   int r, chunk;
   if ((r = fp64_chunk(ctx, npairs, &chunk))) return r;

@@ -48,6 +48,7 @@ struct sdft_ctx {
   int rho_split = 0;
   unsigned char *d_neg = nullptr;
   size_t neg_cap = 0;
+  void *d_noise_scratch = nullptr;  // stop flag + phi margin list of the sign generator
   double *d_enl = nullptr;
   // state
   int resident = 0;          // orbitals in d_chi

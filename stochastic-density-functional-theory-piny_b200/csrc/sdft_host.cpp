@@ -246,27 +246,44 @@ static inline bool sin_neg(double phi, double arg) {
   return std::sin(arg) < 0.0;
 }
 
-void gauss_signs(long long nran, double *qseed, unsigned char *neg) {
+// One Box-Muller pair of gauss_signs: two draws from *qseed, the signs of
+// the cos and sin slots into b[0], b[1] (b[1] only when `both`).
+static inline void sign_pair(double *qseed, unsigned char *b, bool both) {
   const double twopi = 2.0 * M_PI;
-  long long loop = nran / 2;
-  for (long long i = 0; i < loop; i++) {
-    double r = ran_uniform(qseed);
-    r = std::max(r, 1e-30);
-    r = std::min(r, 1.0);
-    double phi = ran_uniform(qseed);
-    double arg = twopi * phi;
-    bool zero_al = (r == 1.0);
-    neg[2 * i] = (!zero_al && cos_neg(phi, arg)) ? 1 : 0;
-    neg[2 * i + 1] = (!zero_al && sin_neg(phi, arg)) ? 1 : 0;
+  double r = ran_uniform(qseed);
+  r = std::max(r, 1e-30);
+  r = std::min(r, 1.0);
+  double phi = ran_uniform(qseed);
+  double arg = twopi * phi;
+  bool zero_al = (r == 1.0);
+  b[0] = (!zero_al && cos_neg(phi, arg)) ? 1 : 0;
+  if (both) b[1] = (!zero_al && sin_neg(phi, arg)) ? 1 : 0;
+}
+
+void gauss_signs(long long nran, double *qseed, unsigned char *neg) {
+  const long long npairs = (nran + 1) / 2;
+  for (long long i = 0; i < npairs; i++) sign_pair(qseed, neg + 2 * i, 2 * i + 1 < nran);
+}
+
+bool durand_on_lattice(double q) {
+  const double s = q * 128.0;
+  return q >= 1.0 && q <= 2147483646.0 && s == std::floor(s);
+}
+
+long long gauss_signs_to_lattice(long long nran, long long p, long long pend, double *qseed, unsigned char *out) {
+  long long i = p;
+  while (i < pend) {
+    sign_pair(qseed, out + 2 * (i - p), 2 * i + 1 < nran);
+    ++i;
+    if (durand_on_lattice(*qseed)) break;
   }
-  if (nran % 2 != 0) {
-    double r = ran_uniform(qseed);
-    r = std::max(r, 1e-30);
-    r = std::min(r, 1.0);
-    double phi = ran_uniform(qseed);
-    double arg = twopi * phi;
-    neg[nran - 1] = (r != 1.0 && cos_neg(phi, arg)) ? 1 : 0;
-  }
+  return i;
+}
+
+void gauss_signs_from_phi(double phi, unsigned char *b) {
+  const double arg = 2.0 * M_PI * phi;
+  b[0] = cos_neg(phi, arg) ? 1 : 0;
+  b[1] = sin_neg(phi, arg) ? 1 : 0;
 }
 }  // namespace sdft
 

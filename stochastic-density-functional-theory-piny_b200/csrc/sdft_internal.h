@@ -15,6 +15,17 @@ double ran_uniform(double *qseed);
 void gaussran2(int nran, double *qseed, double *gauss);
 void noise_rank_seeds(double seed, int np_states, double *out);
 void gauss_signs(long long nran, double *qseed, unsigned char *neg);
+// DURAND state q on the lattice q = Q/128 (Q integer, 1 <= q <= 2147483646):
+// from there the FP64 generator follows Q <- 16807 Q mod 128 (2^31 - 1)
+// exactly until a draw finds q outside [1, 2147483646].
+bool durand_on_lattice(double q);
+// gauss_signs pairs p, p+1, ... (two draws each) from *qseed until the state
+// is on the lattice or pend is reached; bytes of pair i go to
+// out[2 (i - p)], out[2 (i - p) + 1] (the second only below nran).  Returns
+// the first pair not generated.
+long long gauss_signs_to_lattice(long long nran, long long p, long long pend, double *qseed, unsigned char *out);
+// Signs of one pair (r != 1) from its phi, as gauss_signs decides them.
+void gauss_signs_from_phi(double phi, unsigned char *b);
 int cheby_coeff(int L, int ngrid, double energy_diff, double energy_mean, double beta,
                 double chem_pot, int fun_flag, double *coeffs);
 

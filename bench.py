@@ -708,7 +708,8 @@ def run_serve(args):
     out_runs = {}
     recs = {}
     for name, prec in (("mixed", pkg.SDFT_PREC_MIXED), ("fp64", pkg.SDFT_PREC_FP64)):
-        srv = serve.Server(pkg, wl, prec, hbm_budget=150e9, slots=args.slots, workers=args.workers)
+        srv = serve.Server(pkg, wl, prec, hbm_budget=150e9, slots=args.slots, workers=args.workers,
+                           priorities=not args.no_priorities)
         srv.run([dict(r, arrival=0.0) for r in reqs[:2]])  # warm-up (module loads, first-use attributes)
         # FP64 serves the same stream with the mixed run's mu, so the density
         # difference is the precision alone (the moments are still computed)
@@ -719,6 +720,8 @@ def run_serve(args):
     errs = [float(np.linalg.norm(a["density"] - b["density"]) / np.linalg.norm(b["density"]))
             for a, b in zip(recs["mixed"], recs["fp64"])]
     m = out_runs["mixed"]
+    lat_small = [r["latency"] for r in recs["mixed"] if r["natm"] < 512]
+    lat_big = [r["latency"] for r in recs["mixed"] if r["natm"] >= 512]
     out = {
         "metric": "serving: filtered stochastic orbitals/s with p50/p99 request latency (Poisson 50 req/s)",
         "value": m["orbitals_per_s"], "unit": "orbitals/s", "n_gpus": 1, "steps": 1, "warmup": 1,
@@ -727,9 +730,13 @@ def run_serve(args):
         "data": "synthetic (seeded Poisson arrivals; Si supercells 8..216 atoms + 10 % 512-atom)",
         "config": {"workload": f"cfg5: {len(reqs)} requests at 50 req/s, slots {args.slots}, "
                                f"{args.workers} host workers, HBM budget 150 GB",
+                   "stream_priorities": "by request work (serve.request_priority)" if not args.no_priorities
+                   else "off",
                    "requests": len(reqs), "orbitals": m["orbitals"],
                    "atoms": [int(8 * np.prod(r["spec"]["nrep"])) for r in reqs]},
-        "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"], "mean": m["mean_ms"]},
+        "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"], "mean": m["mean_ms"],
+                       "p50_below_512_atoms": float(np.percentile(lat_small, 50) * 1e3) if lat_small else None,
+                       "max_512_atoms": float(max(lat_big) * 1e3) if lat_big else None},
         "mixed": m, "fp64": out_runs["fp64"],
         "mixed_speedup": m["orbitals_per_s"] / out_runs["fp64"]["orbitals_per_s"],
         "density_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
@@ -757,6 +764,7 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
     ap.add_argument("--workers", type=int, default=16, help="cfg5: host threads preparing requests")
+    ap.add_argument("--no-priorities", action="store_true", help="cfg5: all request streams at default priority")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -191,6 +191,11 @@ int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count);
  * Split-K of the nonlocal projection GEMM: 0 = built-in cost model,
  * 1..64 = fixed (chosen by the autotuner in tuner.py).                    */
 int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split);
+/* CUDA stream priority of the context's stream (lower = more urgent, 0 =
+ * default; clamped to the device's range).  Call while the context is idle:
+ * the stream is replaced.  A server gives cheap requests the urgent
+ * priorities so they are not queued behind large ones on a shared GPU. */
+int sdft_ctx_set_priority(sdft_ctx *ctx, int priority);
 /* One CUDA graph running, for every context i (orbitals resident, V and KB
  * set), the Chebyshev filter of nstate[i] orbitals with the L[i]
  * coefficients coeffs[i] (one chemical potential) followed by the density
@@ -207,6 +212,9 @@ int sdft_batch_create(int n, sdft_ctx *const *ctxs, const int *nstate, const int
 int sdft_batch_launch(sdft_batch *b);
 int sdft_batch_sync(sdft_batch *b);
 void *sdft_batch_stream(sdft_batch *b);
+/* Priority of the stream the batch's graph is launched into (its kernels
+ * run at that priority); as sdft_ctx_set_priority, while idle. */
+int sdft_batch_set_priority(sdft_batch *b, int priority);
 /* own kernels + memsets issued by one replay */
 long long sdft_batch_kernel_count(const sdft_batch *b);
 int sdft_batch_destroy(sdft_batch *b);

@@ -116,6 +116,8 @@ _sig("sdft_launch_count", C.c_longlong, [_vp])
 _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
+_sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
+_sig("sdft_batch_set_priority", C.c_int, [_vp, C.c_int])
 _sig("sdft_download_density", C.c_int, [_vp, _dp])
 _sig("sdft_batch_create", C.c_int, [C.c_int, C.POINTER(_vp), _ip, _ip, C.POINTER(_dp), _dp, _dp, _dp, C.POINTER(_vp)])
 _sig("sdft_batch_launch", C.c_int, [_vp])
@@ -428,6 +430,10 @@ class Context:
         """Split-K of the nonlocal projection GEMM (0 = cost model)."""
         _chk(lib.sdft_ctx_set_gemm_split(self._p, int(split)))
 
+    def set_priority(self, priority):
+        """CUDA priority of the context's stream (lower = more urgent); idle only."""
+        _chk(lib.sdft_ctx_set_priority(self._p, int(priority)))
+
     @property
     def stream_ptr(self):
         return int(lib.sdft_ctx_stream(self._p) or 0)
@@ -461,6 +467,10 @@ class Batch:
 
     def sync(self):
         _chk(lib.sdft_batch_sync(self._p))
+
+    def set_priority(self, priority):
+        """CUDA priority of the stream the graph is launched into; idle only."""
+        _chk(lib.sdft_batch_set_priority(self._p, int(priority)))
 
     @property
     def stream_ptr(self):

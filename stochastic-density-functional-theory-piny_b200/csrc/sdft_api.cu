@@ -51,14 +51,51 @@ using namespace sdft;
 
 
 namespace sdft {
-int dmalloc(sdft_ctx *c, void **p, size_t bytes) {
-  cudaError_t e = cudaMalloc(p, bytes);
+// Device memory comes from one stream-ordered pool per device: allocations
+// and releases are ordered on the owning context's stream and never
+// synchronise the whole device, so contexts created and destroyed while
+// other contexts' work runs (a server) do not wait for that work.  Released
+// blocks stay in the pool for reuse (release threshold unlimited).
+static cudaMemPool_t pool_of(int device) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = pool;
+  }
+  return pools[device];
+}
+
+int dev_alloc(int device, void *stream, void **p, size_t bytes) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaMemPool_t pool = pool_of(device);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaErrorMemoryAllocation;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // usable from any stream on return
   if (e != cudaSuccess) {
     *p = nullptr;
     char b[256];
-    snprintf(b, sizeof b, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    snprintf(b, sizeof b, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return set_error(SDFT_ERR_NOMEM, b);
   }
+  return SDFT_OK;
+}
+
+void dev_free(void *p, void *stream) {
+  if (p) cudaFreeAsync(p, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int dmalloc(sdft_ctx *c, void **p, size_t bytes) {
+  int r = dev_alloc(c->device, c->st, p, bytes);
+  if (r) return r;
   c->dev_bytes += (long long)bytes;
   return SDFT_OK;
 }
@@ -122,7 +159,7 @@ static int ensure_x(sdft_ctx *ctx, int npairs) {
   const size_t csz = ctx->fft64 ? sizeof(double2) : sizeof(float2);
   const size_t need = (size_t)npairs * ctx->n3 * ctx->cols.ncols_pad * csz;
   if (need <= ctx->x_bytes) return SDFT_OK;
-  if (ctx->d_x) { cudaFree(ctx->d_x); ctx->dev_bytes -= (long long)ctx->x_bytes; ctx->d_x = nullptr; }
+  if (ctx->d_x) { dev_free(ctx->d_x, ctx->st); ctx->dev_bytes -= (long long)ctx->x_bytes; ctx->d_x = nullptr; }
   DM(ctx->d_x, need);
   ctx->x_bytes = need;
   return SDFT_OK;
@@ -141,7 +178,7 @@ static int fp64_chunk(sdft_ctx *ctx, int npairs, int *chunk) {
 
 static int ensure_coef(sdft_ctx *ctx, size_t n) {
   if (n <= ctx->coef_cap) return SDFT_OK;
-  if (ctx->d_coef) { cudaFree(ctx->d_coef); ctx->dev_bytes -= (long long)(ctx->coef_cap * 8); }
+  if (ctx->d_coef) { dev_free(ctx->d_coef, ctx->st); ctx->dev_bytes -= (long long)(ctx->coef_cap * 8); }
   DM(ctx->d_coef, n * sizeof(double));
   ctx->coef_cap = n;
   return SDFT_OK;
@@ -149,7 +186,7 @@ static int ensure_coef(sdft_ctx *ctx, size_t n) {
 
 static int ensure_acc(sdft_ctx *ctx, int nmu) {
   if (nmu <= ctx->acc_nmu) return SDFT_OK;
-  if (ctx->d_acc) { cudaFree(ctx->d_acc); ctx->dev_bytes -= (long long)(ctx->acc_nmu * ctx->vec_elems * 8); }
+  if (ctx->d_acc) { dev_free(ctx->d_acc, ctx->st); ctx->dev_bytes -= (long long)(ctx->acc_nmu * ctx->vec_elems * 8); }
   DM(ctx->d_acc, (size_t)nmu * ctx->vec_elems * sizeof(double));
   CK(cudaMemsetAsync(ctx->d_acc, 0, (size_t)nmu * ctx->vec_elems * sizeof(double), ctx->st));
   ctx->acc_nmu = nmu;
@@ -158,7 +195,7 @@ static int ensure_acc(sdft_ctx *ctx, int nmu) {
 
 static int ensure_mom(sdft_ctx *ctx, size_t n) {
   if (n <= ctx->mom_cap) return SDFT_OK;
-  if (ctx->d_mom) { cudaFree(ctx->d_mom); ctx->dev_bytes -= (long long)(ctx->mom_cap * 8); }
+  if (ctx->d_mom) { dev_free(ctx->d_mom, ctx->st); ctx->dev_bytes -= (long long)(ctx->mom_cap * 8); }
   DM(ctx->d_mom, n * sizeof(double));
   ctx->mom_cap = n;
   return SDFT_OK;
@@ -563,13 +600,13 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   DMF(ctx->d_ak2, ncoef * sizeof(double));
   DMF(ctx->d_tw, tw.size() * sizeof(double2));
   DMF(ctx->d_twf, twf.size() * sizeof(float2));
-  CKF(cudaMemcpy(ctx->d_cp_gstart, cpg.data(), cpg.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_cp_gcount, cpc.data(), cpc.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_col_ab, colab.data(), colab.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_gkc, gkc.data(), ncoef * sizeof(int), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_ak2, ak2.data(), ncoef * sizeof(double), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(ctx->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpyAsync(ctx->d_cp_gstart, cpg.data(), cpg.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_cp_gcount, cpc.data(), cpc.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_col_ab, colab.data(), colab.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_gkc, gkc.data(), ncoef * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_ak2, ak2.data(), ncoef * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+  CKF(cudaMemcpyAsync(ctx->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
   DevGeom &g = ctx->g;
   g.n1 = n1; g.n2 = n2; g.n3 = n3; g.N = ctx->N;
   g.ncoef = ncoef; g.ngp = ctx->ngp;
@@ -584,13 +621,13 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   DMF(ctx->d_chi, vb);
   DMF(ctx->d_b1, vb);
   DMF(ctx->d_b2, vb);
-  CKF(cudaMemset(ctx->d_chi, 0, vb));
-  CKF(cudaMemset(ctx->d_b1, 0, vb));
-  CKF(cudaMemset(ctx->d_b2, 0, vb));
+  CKF(cudaMemsetAsync(ctx->d_chi, 0, vb, ctx->st));
+  CKF(cudaMemsetAsync(ctx->d_b1, 0, vb, ctx->st));
+  CKF(cudaMemsetAsync(ctx->d_b2, 0, vb, ctx->st));
   DMF(ctx->d_dots, (size_t)ctx->npairs_max * g.nbatch * 3 * sizeof(double));
   DMF(ctx->d_enl, sizeof(double));
   DMF(ctx->d_err, sizeof(int));
-  CKF(cudaMemset(ctx->d_err, 0, sizeof(int)));
+  CKF(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->st));
   const size_t vsz = is_fp64(ctx) ? sizeof(double) : sizeof(float);
   DMF(ctx->d_vp, (size_t)ctx->N * vsz);
   DMF(ctx->d_vks_tmp, (size_t)ctx->N * sizeof(double));
@@ -599,6 +636,8 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   *out = ctx;
   return SDFT_OK;
 }
+
+static void batch_detach(sdft_batch *b, sdft_ctx *c);
 
 extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
   if (!ctx) return SDFT_OK;
@@ -612,8 +651,11 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
                   ctx->d_oz_part};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  // a batch graph still holding the context: wait for its replays, drop the context from it
+  for (sdft_batch *b : ctx->batches) batch_detach(b, ctx);
+  ctx->batches.clear();
+  for (void *p : ptrs) dev_free(p, ctx->st);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
   for (auto &t : ctx->tev_pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
   for (auto e : ctx->tev_free) cudaEventDestroy(e);
   if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -627,7 +669,7 @@ extern "C" int sdft_ctx_set_kinetic_cap(sdft_ctx *ctx, double gcut) {
   std::vector<double> ak2(ctx->ncoef);
   sdft_ak2_kinetic(ctx->hmat, ctx->ncoef, ctx->ka.data(), ctx->kb.data(), ctx->kc.data(), gcut, ak2.data());
   cudaSetDevice(ctx->device);
-  CK(cudaMemcpy(ctx->d_ak2, ak2.data(), ctx->ncoef * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_ak2, ak2.data(), ctx->ncoef * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
   return SDFT_OK;
 }
 
@@ -688,7 +730,8 @@ extern "C" int sdft_sync(sdft_ctx *ctx) {
   CK(cudaStreamSynchronize(ctx->st));
   CK(cudaGetLastError());
   int e = 0;
-  CK(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   if (e) return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
   return SDFT_OK;
 }
@@ -902,7 +945,7 @@ static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double sca
   if ((r = fp64_chunk(ctx, npairs, &chunk))) return r;
   const int nsplit = npairs;  // one |psi|^2 plane set per pair, summed in pair order
   if (nsplit > ctx->rho_split) {
-    if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
+    if (ctx->d_rho_part) { dev_free(ctx->d_rho_part, ctx->st); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
     DM(ctx->d_rho_part, (size_t)nsplit * ctx->N * sizeof(double));
     ctx->rho_split = nsplit;
   }
@@ -964,7 +1007,7 @@ static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int
   double q = seeds[myid];
   const size_t n = (size_t)nstate * ctx->N;
   if (n > ctx->neg_cap) {
-    if (ctx->d_neg) { cudaFree(ctx->d_neg); ctx->dev_bytes -= (long long)ctx->neg_cap; }
+    if (ctx->d_neg) { dev_free(ctx->d_neg, ctx->st); ctx->dev_bytes -= (long long)ctx->neg_cap; }
     DM(ctx->d_neg, n);
     ctx->neg_cap = n;
   }
@@ -1031,6 +1074,28 @@ extern "C" int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split) {
   return SDFT_OK;
 }
 
+// Replace an idle stream by one of the given CUDA priority (lower = more
+// urgent), clamped to the device's range.
+static int replace_stream(cudaStream_t *st, int priority) {
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  priority = std::min(least, std::max(greatest, priority));
+  cudaStream_t ns = nullptr;
+  CK(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, priority));
+  if (*st) {
+    cudaStreamSynchronize(*st);
+    cudaStreamDestroy(*st);
+  }
+  *st = ns;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_set_priority(sdft_ctx *ctx, int priority) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  cudaSetDevice(ctx->device);
+  return replace_stream(&ctx->st, priority);
+}
+
 struct sdft_batch {
   int device = 0;
   cudaStream_t st = nullptr;
@@ -1052,7 +1117,7 @@ static int prepare_filter(sdft_ctx *ctx, int nstate, int L) {
   const int npairs = (nstate + 1) / 2;
   if ((r = ensure_x(ctx, std::max(npairs, 2)))) return r;  // as fp64_chunk needs it
   if (npairs > ctx->rho_split) {
-    if (ctx->d_rho_part) { cudaFree(ctx->d_rho_part); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
+    if (ctx->d_rho_part) { dev_free(ctx->d_rho_part, ctx->st); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
     ctx->d_rho_part = nullptr;
     if ((r = dmalloc(ctx, (void **)&ctx->d_rho_part, (size_t)npairs * ctx->N * sizeof(double)))) return r;
     ctx->rho_split = npairs;
@@ -1062,10 +1127,16 @@ static int prepare_filter(sdft_ctx *ctx, int nstate, int L) {
 }
 }  // namespace sdft
 
+static void batch_detach(sdft_batch *b, sdft_ctx *c) {
+  if (b->st) cudaStreamSynchronize(b->st);
+  b->ctxs.erase(std::remove(b->ctxs.begin(), b->ctxs.end(), c), b->ctxs.end());
+}
+
 extern "C" int sdft_batch_destroy(sdft_batch *b) {
   if (!b) return SDFT_OK;
   cudaSetDevice(b->device);
   if (b->st) cudaStreamSynchronize(b->st);
+  for (sdft_ctx *c : b->ctxs) c->batches.erase(std::remove(c->batches.begin(), c->batches.end(), b), c->batches.end());
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   for (cudaEvent_t e : b->evs) cudaEventDestroy(e);
@@ -1105,7 +1176,8 @@ extern "C" int sdft_batch_create(int n, sdft_ctx *const *ctxs, const int *nstate
   for (int i = 0; i < n; i++) {
     sdft_ctx *c = ctxs[i];
     if ((r = prepare_filter(c, nstate[i], L[i]))) return fail(r);
-    if ((r = ck(cudaMemcpy(c->d_coef, coeffs[i], (size_t)L[i] * sizeof(double), cudaMemcpyHostToDevice))))
+    if ((r = ck(cudaMemcpyAsync(c->d_coef, coeffs[i], (size_t)L[i] * sizeof(double), cudaMemcpyHostToDevice,
+                                c->st))))
       return fail(r);
     if ((r = ck(cudaStreamSynchronize(c->st)))) return fail(r);
     b->ctxs.push_back(c);
@@ -1136,6 +1208,7 @@ extern "C" int sdft_batch_create(int n, sdft_ctx *const *ctxs, const int *nstate
   long long l1 = 0;
   for (int i = 0; i < n; i++) { l1 += ctxs[i]->launches; ctxs[i]->filtered = nstate[i]; }
   b->launches_per_replay = l1 - l0;
+  for (sdft_ctx *c : b->ctxs) c->batches.push_back(b);
   *out = b;
   return SDFT_OK;
 }
@@ -1153,10 +1226,17 @@ extern "C" int sdft_batch_sync(sdft_batch *b) {
   CK(cudaStreamSynchronize(b->st));
   for (sdft_ctx *c : b->ctxs) {
     int e = 0;
-    CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     if (e) return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
   }
   return SDFT_OK;
+}
+
+extern "C" int sdft_batch_set_priority(sdft_batch *b, int priority) {
+  if (!b) return set_error(SDFT_ERR_ARG, "batch_set_priority: no batch");
+  cudaSetDevice(b->device);
+  return replace_stream(&b->st, priority);
 }
 
 extern "C" void *sdft_batch_stream(sdft_batch *b) { return b ? (void *)b->st : nullptr; }

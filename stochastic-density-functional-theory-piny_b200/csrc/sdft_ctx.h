@@ -6,6 +6,8 @@
 #include "sdft_kernels.cuh"
 #include "sdft_gemm_oz.cuh"
 
+struct sdft_batch;
+
 struct sdft_ctx {
   int device = 0;
   int prec = SDFT_PREC_FP64;
@@ -49,6 +51,7 @@ struct sdft_ctx {
   unsigned char *d_neg = nullptr;
   size_t neg_cap = 0;
   void *d_noise_scratch = nullptr;  // stop flag + phi margin list of the sign generator
+  std::vector<sdft_batch *> batches;  // graphs that replay this context's filter
   double *d_enl = nullptr;
   // state
   int resident = 0;          // orbitals in d_chi

@@ -8,6 +8,11 @@ namespace sdft {
 
 int set_error(int code, const char *msg);
 
+// Stream-ordered device memory from the library's per-device pool; complete
+// (usable from any stream) on return.  dev_free releases in stream order.
+int dev_alloc(int device, void *stream, void **p, size_t bytes);
+void dev_free(void *p, void *stream);
+
 // host helpers (sdft_host.cpp)
 void invert_cell(const double *h, double *hi);
 double cell_volume(const double *h);

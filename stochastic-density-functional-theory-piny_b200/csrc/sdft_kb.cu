@@ -145,6 +145,11 @@ static double spline_eval(const double *tab, int nsplin, double gmin, double dg,
 
 using namespace sdft;
 
+#define CKT(call)                                                           \
+  do {                                                                      \
+    int r__ = (call);                                                       \
+    if (r__) { rc = r__; goto done; }                                       \
+  } while (0)
 #define CKB(call)                                                           \
   do {                                                                      \
     cudaError_t e__ = (call);                                               \
@@ -155,11 +160,10 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   // release a previous projector set
   double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl};
   for (double **p : old)
-    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (*p) { dev_free(*p, ctx->st); *p = nullptr; }
   void *oldo[] = {ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig, ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc,
                   ctx->d_c_sc,   ctx->d_z_sc,   ctx->d_rowmax, ctx->d_oz_part};
-  for (void *p : oldo)
-    if (p) cudaFree(p);
+  for (void *p : oldo) dev_free(p, ctx->st);
   ctx->d_pj_dig = ctx->d_bk_dig = ctx->d_c_dig = ctx->d_z_dig = nullptr;
   ctx->d_pj_sc = ctx->d_bk_sc = ctx->d_c_sc = ctx->d_z_sc = nullptr;
   ctx->d_rowmax = nullptr;
@@ -249,27 +253,27 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     if ((r = dmalloc(ctx, (void **)&ctx->d_zwork, ctx->zwork_elems * sizeof(double)))) return r;
     if ((r = dmalloc(ctx, (void **)&ctx->d_fnl, ctx->vec_elems * sizeof(double)))) return r;
   }
-  CKB(cudaMemset(ctx->d_pj, 0, (size_t)Ppad * K1 * sizeof(double)));
-  CKB(cudaMemset(ctx->d_bk, 0, (size_t)Mpad2 * Ppad * sizeof(double)));
-  CKB(cudaMemset(ctx->d_z, 0, (size_t)ctx->s_pad * Ppad * sizeof(double)));
-  CKB(cudaMemset(ctx->d_fnl, 0, ctx->vec_elems * sizeof(double)));
-  CKB(cudaMemcpy(ctx->d_w, w.data(), Ppad * sizeof(double), cudaMemcpyHostToDevice));
-  CKB(cudaMalloc(&d_kv, kv.size() * sizeof(int)));
-  CKB(cudaMalloc(&d_rs, rstart.size() * sizeof(int)));
-  CKB(cudaMalloc(&d_rcnt, rcount.size() * sizeof(int)));
-  CKB(cudaMalloc(&d_frac, frac.size() * sizeof(double)));
-  CKB(cudaMalloc(&d_vtab, vtab.size() * sizeof(double)));
-  CKB(cudaMalloc(&d_ylm, ylm.size() * sizeof(double)));
-  CKB(cudaMalloc(&d_gz, kb->ntype * sizeof(double)));
-  CKB(cudaMalloc(&d_rows, rows.size() * sizeof(KbRow)));
-  CKB(cudaMemcpy(d_kv, kv.data(), kv.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_rs, rstart.data(), rstart.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_rcnt, rcount.data(), rcount.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_frac, frac.data(), frac.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_vtab, vtab.data(), vtab.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_ylm, ylm.data(), ylm.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_gz, kb->gzvps0, kb->ntype * sizeof(double), cudaMemcpyHostToDevice));
-  CKB(cudaMemcpy(d_rows, rows.data(), rows.size() * sizeof(KbRow), cudaMemcpyHostToDevice));
+  CKB(cudaMemsetAsync(ctx->d_pj, 0, (size_t)Ppad * K1 * sizeof(double), ctx->st));
+  CKB(cudaMemsetAsync(ctx->d_bk, 0, (size_t)Mpad2 * Ppad * sizeof(double), ctx->st));
+  CKB(cudaMemsetAsync(ctx->d_z, 0, (size_t)ctx->s_pad * Ppad * sizeof(double), ctx->st));
+  CKB(cudaMemsetAsync(ctx->d_fnl, 0, ctx->vec_elems * sizeof(double), ctx->st));
+  CKB(cudaMemcpyAsync(ctx->d_w, w.data(), Ppad * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_kv, kv.size() * sizeof(int)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_rs, rstart.size() * sizeof(int)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_rcnt, rcount.size() * sizeof(int)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_frac, frac.size() * sizeof(double)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_vtab, vtab.size() * sizeof(double)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_ylm, ylm.size() * sizeof(double)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_gz, kb->ntype * sizeof(double)));
+  CKT(dev_alloc(ctx->device, ctx->st, (void **)&d_rows, rows.size() * sizeof(KbRow)));
+  CKB(cudaMemcpyAsync(d_kv, kv.data(), kv.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_rs, rstart.data(), rstart.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_rcnt, rcount.data(), rcount.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_frac, frac.data(), frac.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_vtab, vtab.data(), vtab.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_ylm, ylm.data(), ylm.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_gz, kb->gzvps0, kb->ntype * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(d_rows, rows.data(), rows.size() * sizeof(KbRow), cudaMemcpyHostToDevice, ctx->st));
   {
     dim3 grid((ncoef + 127) / 128, kb->natm);
     k_build_proj<<<grid, 128, 0, ctx->st>>>(ncoef, ngp, Ppad, d_kv, d_frac, d_rs, d_rcnt, d_rows, d_vtab, lmax1,
@@ -303,10 +307,10 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
       rc = r;
       goto done;
     }
-    CKB(cudaMemset(ctx->d_c_dig, 0, cd));
-    CKB(cudaMemset(ctx->d_z_dig, 0, zd));
-    CKB(cudaMemset(ctx->d_c_sc, 0, S * sizeof(double)));
-    CKB(cudaMemset(ctx->d_z_sc, 0, S * sizeof(double)));
+    CKB(cudaMemsetAsync(ctx->d_c_dig, 0, cd, ctx->st));
+    CKB(cudaMemsetAsync(ctx->d_z_dig, 0, zd, ctx->st));
+    CKB(cudaMemsetAsync(ctx->d_c_sc, 0, S * sizeof(double), ctx->st));
+    CKB(cudaMemsetAsync(ctx->d_z_sc, 0, S * sizeof(double), ctx->st));
     launch_oz_slice_rows(ctx->d_pj, K1, Ppad, K1, ctx->d_rowmax, ctx->d_pj_dig, Kp, (size_t)Ppad * Kp, ctx->d_pj_sc,
                          ctx->st);
     launch_oz_slice_rows(ctx->d_bk, Ppad, Mpad2, Ppad, ctx->d_rowmax, ctx->d_bk_dig, Ppad, (size_t)Mpad2 * Ppad,
@@ -323,14 +327,16 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     g1.M = Ppad; g1.K = Kp; g1.ldo = Ppad; g1.Mst = P; g1.sa = ctx->d_pj_sc; g1.sb = ctx->d_c_sc;
     g2.M = Mpad2; g2.K = Ppad; g2.ldo = K1; g2.Mst = K1; g2.sa = ctx->d_bk_sc; g2.sb = ctx->d_z_sc;
     // the FP64 projector copies are not used by the mixed path
-    cudaFree(ctx->d_pj); ctx->d_pj = nullptr;
-    cudaFree(ctx->d_bk); ctx->d_bk = nullptr;
+    dev_free(ctx->d_pj, ctx->st); ctx->d_pj = nullptr;
+    dev_free(ctx->d_bk, ctx->st); ctx->d_bk = nullptr;
     ctx->dev_bytes -= (long long)((size_t)Ppad * K1 + (size_t)Mpad2 * Ppad) * 8;
     ctx->oz = true;
     ctx->rowmax_zero_n = 0;  // the projector slicing above left row maxima behind
   }
 done:
-  cudaFree(d_kv); cudaFree(d_rs); cudaFree(d_rcnt); cudaFree(d_frac);
-  cudaFree(d_vtab); cudaFree(d_ylm); cudaFree(d_gz); cudaFree(d_rows);
+  for (void *p : {(void *)d_kv, (void *)d_rs, (void *)d_rcnt, (void *)d_frac, (void *)d_vtab, (void *)d_ylm,
+                  (void *)d_gz, (void *)d_rows})
+    dev_free(p, ctx->st);
+  cudaStreamSynchronize(ctx->st);
   return rc;
 }

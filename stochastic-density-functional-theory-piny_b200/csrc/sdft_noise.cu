@@ -247,11 +247,13 @@ extern "C" int sdft_gaussran2_signs_dev(long long nran, double *qseed, unsigned 
   if (nran < 0 || !qseed || (nran > 0 && !neg)) return set_error(SDFT_ERR_ARG, "gaussran2_signs_dev: bad argument");
   if (nran == 0) return SDFT_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDFT_ERR_CUDA, "gaussran2_signs_dev: no device");
   void *scratch = nullptr;
-  cudaError_t e = cudaMalloc(&scratch, noise_scratch_bytes());
-  if (e != cudaSuccess) return set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
-  int r = device_gauss_signs(nran, qseed, neg, scratch, st, nullptr);
+  int r = dev_alloc(dev, stream, &scratch, noise_scratch_bytes());
+  if (r) return r;
+  r = device_gauss_signs(nran, qseed, neg, scratch, st, nullptr);
+  dev_free(scratch, stream);
   cudaStreamSynchronize(st);
-  cudaFree(scratch);
   return r;
 }

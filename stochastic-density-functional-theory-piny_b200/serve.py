@@ -12,7 +12,9 @@ every request the server
    the FP64 bisection (calcChemPotCheby) and the filter coefficients;
 3. captures its Chebyshev filter + density as a one-context CUDA graph
    (sdft_batch) and launches it on the request's own stream, so requests
-   admitted while others run overlap on the device;
+   admitted while others run overlap on the device; the request's streams
+   get a CUDA priority by its work (request_priority: cheaper = more urgent),
+   so short requests are not queued behind 512-atom ones;
 4. when the graph's completion event fires, downloads the density, frees the
    context and returns its memory to the budget.
 
@@ -27,13 +29,26 @@ from collections import deque
 import numpy as np
 
 
-def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None):
+def request_priority(grid, nsto, L, levels=6, ref_cost=1e11):
+    """CUDA stream priority of a request by its filter work nsto * L * grid
+    points: 0 (least urgent) at ref_cost and above, one level more urgent per
+    factor 4 less work, down to -(levels - 1) (clamped to the device range by
+    the library)."""
+    import math
+    cost = float(nsto) * L * grid[0] * grid[1] * grid[2]
+    return -min(levels - 1, max(0, int(math.log(ref_cost / cost, 4)))) if cost < ref_cost else 0
+
+
+def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None, priority=None):
     """Context with resident noise orbitals and filter coefficients for one
     system (steps 2 of the request life cycle).  mu, if given, replaces the
-    bisection result (the moments are still computed)."""
+    bisection result (the moments are still computed); priority, if given,
+    is the CUDA priority of the context's stream."""
     t = [time.perf_counter()]
     ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=precision, max_states=nsto,
                       device=device)
+    if priority is not None:
+        ctx.set_priority(priority)
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
     t.append(time.perf_counter())
@@ -52,7 +67,7 @@ def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None)
         tuner.tune(ctx, nsto, 4 * s["natm"], scale, emean)
     phases = dict(context_s=t[1] - t[0], lanczos_s=t[2] - t[1], noise_s=t[3] - t[2], moments_s=t[4] - t[3])
     return dict(ctx=ctx, ec=ec, scale=scale, emean=emean, mu=mu, num_elec=ne, occ_over=wl.OCC / nsto, nsto=nsto, L=L,
-                phases=phases)
+                phases=phases, priority=priority)
 
 
 def estimate_spec_bytes(spec, nsto, ecut=10.0, a0=10.26):
@@ -98,8 +113,10 @@ class Server:
     new requests overlaps the device work of running ones (the library's calls
     release the interpreter lock)."""
 
-    def __init__(self, pkg, wl, precision, hbm_budget=150e9, slots=16, device=0, tuner=None, workers=4):
+    def __init__(self, pkg, wl, precision, hbm_budget=150e9, slots=16, device=0, tuner=None, workers=4,
+                 priorities=True):
         self.pkg, self.wl = pkg, wl
+        self.priorities = bool(priorities)
         self.precision = precision
         self.budget = float(hbm_budget)
         self.slots = int(slots)
@@ -114,11 +131,14 @@ class Server:
         tb = time.perf_counter()
         s = self.wl.build_spec(r["spec"])
         build_s = time.perf_counter() - tb
+        prio = request_priority(s["grid"], r["nsto"], r["L"]) if self.priorities else None
         p = prepare(self.pkg, self.wl, s, r["nsto"], r["L"], self.precision, r["seed"], self.device, self.tuner,
-                    mu=r.get("mu"))
+                    mu=r.get("mu"), priority=prio)
         ctx = p["ctx"]
         tc = time.perf_counter()
         b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
+        if prio is not None:
+            b.set_priority(prio)
         p["phases"].update(build_s=build_s, capture_s=time.perf_counter() - tc)
         st = torch.cuda.ExternalStream(b.stream_ptr)
         b.launch()

@@ -25,6 +25,8 @@
  *   sdft_noise_real                   <- genNoiseOrbitalReal stodft/gen-noise.c:162
  *   sdft_gaussran2                    <- gaussran2 / ran_essl / DURAND mathlib/mathlib.c:118,30; mathlib/blas_wrappers.f:39
  *   sdft_gaussran2_signs_dev          <- the gaussran2 call of genNoiseOrbitalReal, stodft/gen-noise.c:256 (signs only)
+ *   sdft_lanczos_bounds               <- genEnergyMax/genEnergyMin stodft/calc-spectral-range.c:33,339 (Lanczos)
+ *   sdft_energy_chempot_dev           <- calcEnergyChemPot stodft/calc-energy.c:32
  */
 #ifndef SDFT_B200_H
 #define SDFT_B200_H
@@ -185,6 +187,27 @@ long long sdft_launch_count(const sdft_ctx *ctx);
 #define SDFT_NKIND 8
 int sdft_ctx_set_timing(sdft_ctx *ctx, int enable);
 int sdft_ctx_read_timing(sdft_ctx *ctx, double *ms, long long *count);
+
+/* ---- spectral bounds and energies --------------------------------------- */
+/* Spectral bounds of H from nstep Lanczos steps on one orbital, all vectors
+ * device resident (the role of genEnergyMax/genEnergyMin,
+ * stodft/calc-spectral-range.c:33,339, which run power iterations; 20
+ * Lanczos steps replace them here).  v0re/v0im (host, ncoef each): start
+ * vector, normalised on the device.  alpha/beta (nullable, nstep each) get
+ * the tridiagonal coefficients, *nsteps how many steps ran (fewer when
+ * beta < 1e-12).  *emin / *emax = extreme eigenvalues of the tridiagonal
+ * matrix -/+ margin (0.1 Ha in calc-spectral-range.c).  Uses orbital slot
+ * 0 of the context (resident orbitals are invalidated). */
+int sdft_lanczos_bounds(sdft_ctx *ctx, int nstep, const double *v0re, const double *v0im, double margin,
+                        double *alpha, double *beta, int *nsteps, double *emin, double *emax);
+/* calcEnergyChemPot (stodft/calc-energy.c:32-207) for chemical potential
+ * imu of the filtered orbitals resident on the device (first nstate):
+ * energy_ke = occ/2 sum_s sum_{G != 0} 2 ak2Kinetic |c_s(G)|^2 / nsto_total,
+ * energy_pnl = occ E_NL / nsto_total, E_NL the Kleinman-Bylander energy of
+ * the orbitals (stat_avg->cp_enl of calcNonLocalPseudoScf).  With several
+ * ranks, sum the per-rank values (each passing the global nsto_total). */
+int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total,
+                            double *energy_ke, double *energy_pnl);
 
 /* ---- tuning and batched systems ---------------------------------------- */
 /* No counterpart in the reference (it filters one system per run).

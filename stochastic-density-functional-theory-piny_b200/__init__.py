@@ -117,6 +117,8 @@ _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
+_sig("sdft_lanczos_bounds", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _ip, _dp, _dp])
+_sig("sdft_energy_chempot_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp])
 _sig("sdft_batch_set_priority", C.c_int, [_vp, C.c_int])
 _sig("sdft_download_density", C.c_int, [_vp, _dp])
 _sig("sdft_batch_create", C.c_int, [C.c_int, C.POINTER(_vp), _ip, _ip, C.POINTER(_dp), _dp, _dp, _dp, C.POINTER(_vp)])
@@ -433,6 +435,34 @@ class Context:
     def set_priority(self, priority):
         """CUDA priority of the context's stream (lower = more urgent); idle only."""
         _chk(lib.sdft_ctx_set_priority(self._p, int(priority)))
+
+    def lanczos_bounds(self, nstep=20, seed=15, margin=0.1, v0=None):
+        """Spectral bounds (Emin - margin, Emax + margin) from `nstep` Lanczos
+        steps on the device.  The start vector is the seeded standard normal
+        orbital of workload.lanczos_bounds (Im G0 = 0) unless v0 = (re, im)
+        is given.  Returns (emin, emax, alphas, betas)."""
+        if v0 is None:
+            rng = np.random.default_rng(seed)
+            cr = rng.standard_normal(self.ncoef)
+            ci = rng.standard_normal(self.ncoef)
+            ci[-1] = 0.0
+        else:
+            cr, ci = _f64(v0[0]), _f64(v0[1])
+        al = np.zeros(nstep)
+        be = np.zeros(nstep)
+        k = C.c_int(0)
+        lo, hi = C.c_double(0.0), C.c_double(0.0)
+        _chk(lib.sdft_lanczos_bounds(self._p, int(nstep), _d(cr), _d(ci), float(margin), _d(al), _d(be), C.byref(k),
+                                     C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value, al[:k.value], be[:k.value]
+
+    def energy_chempot_dev(self, nstate, imu=0, occ=2.0, nsto_total=None):
+        """(energy_ke, energy_pnl) of the filtered orbitals for chemical
+        potential imu, as calcEnergyChemPot stores them."""
+        ek, ep = C.c_double(0.0), C.c_double(0.0)
+        _chk(lib.sdft_energy_chempot_dev(self._p, int(nstate), int(imu), float(occ),
+                                         int(nsto_total or nstate), C.byref(ek), C.byref(ep)))
+        return ek.value, ep.value
 
     @property
     def stream_ptr(self):

@@ -15,6 +15,7 @@
 #include "sdft_ctx.h"
 #include "sdft_kernels2.cuh"
 #include "sdft_noise.h"
+#include "sdft_lanczos.h"
 
 namespace sdft {
 
@@ -223,7 +224,7 @@ static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 // orbitals held in `vec`, mixed precision: INT8 Ozaki GEMMs on the digit
 // form of the orbitals; Z = Pj C is split over K with FP64 partial sums, the
 // reduction also produces the digit form of Z for FNL = Bk Z.
-static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
+static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true) {
   const int K1 = 2 * ctx->ngp, S = ctx->s_oz, Ppad = ctx->Ppad;
   const int N = (nstate + 127) / 128 * 128;
   {
@@ -261,6 +262,7 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
     launch_enl(ctx->d_z, Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
     ctx->launches++;
   }
+  if (!back) return SDFT_OK;
   {
     TScope ts(ctx, 4);
     // FNL in FP32 (its rounding is below the FP32 transforms' error in the
@@ -271,9 +273,9 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   return r;
 }
 
-static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
+static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true) {
   if (ctx->P == 0) return SDFT_OK;
-  if (ctx->oz) return run_kb_oz(ctx, vec, nstate, want_enl);
+  if (ctx->oz) return run_kb_oz(ctx, vec, nstate, want_enl, back);
   const int spad = (int)rup(nstate, 64);
   const int K1 = 2 * ctx->ngp;
   // split K of the projection so that >= ~2 waves of CTAs exist
@@ -296,6 +298,7 @@ static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl) {
     launch_enl(ctx->d_z, ctx->Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
     ctx->launches++;
   }
+  if (!back) return SDFT_OK;
   {
     TScope ts(ctx, 4);
     launch_gemm_nt_f64(ctx->d_bk, ctx->Ppad, ctx->d_z, ctx->Ppad, ctx->d_fnl, K1, ctx->Mpad2, spad,
@@ -647,7 +650,7 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
                   ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
                   ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_noise_scratch,
-                  ctx->d_enl,
+                  ctx->d_enl, ctx->d_red,
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
                   ctx->d_oz_part};
@@ -1067,6 +1070,93 @@ extern "C" int sdft_noise_real(sdft_ctx *ctx, int nstate, double seed, int np_st
 // ============================================================================
 // Tuning knob and batched filters (one CUDA graph over several contexts)
 // ============================================================================
+// ---- spectral bounds and energies --------------------------------------------
+static int ensure_red(sdft_ctx *ctx) {
+  if (ctx->d_red) return SDFT_OK;
+  DM(ctx->d_red, (kRedBlocks + 8) * sizeof(double));
+  return SDFT_OK;
+}
+
+// Lanczos with device-resident vectors: c in row 0 of d_chi, H c in d_b1,
+// the previous vector in d_b2; alpha_k, beta_k read back per step.
+extern "C" int sdft_lanczos_bounds(sdft_ctx *ctx, int nstep, const double *v0re, const double *v0im, double margin,
+                                   double *alpha, double *beta, int *nsteps, double *emin, double *emax) {
+  int r = check_ready(ctx, 1);
+  if (r) return r;
+  if (nstep < 1 || !v0re || !v0im || !emin || !emax) return set_error(SDFT_ERR_ARG, "lanczos_bounds: bad argument");
+  cudaSetDevice(ctx->device);
+  if ((r = ensure_red(ctx))) return r;
+  const int nc = ctx->ncoef, ngp = ctx->ngp;
+  double *c = ctx->d_chi, *f = ctx->d_b1, *p = ctx->d_b2;
+  double *part = ctx->d_red, *sc = ctx->d_red + kRedBlocks;
+  ctx->resident = 0;
+  if ((r = upload_block(ctx, c, 1, v0re, v0im))) return r;
+  launch_half_dot(c, c, nc, ngp, part, sc, ctx->st);
+  launch_lz_div(c, sc, nc, ngp, ctx->st);
+  ctx->launches += 3;
+  std::vector<double> al, be;
+  double b = 0.0;
+  for (int k = 0; k < nstep; k++) {
+    EpiArgs e = base_epi(ctx);
+    e.mode = EPI_HPSI;
+    e.OUT = f;
+    if ((r = apply_h(ctx, c, 1, e, false))) return r;
+    launch_lz_hc(f, nc, ngp, ctx->st);
+    launch_half_dot(c, f, nc, ngp, part, sc, ctx->st);                 // alpha
+    launch_lz_w(f, c, k > 0 ? p : nullptr, sc, b, nc, ngp, ctx->st);  // w = H c - alpha c - beta p
+    launch_half_dot(f, f, nc, ngp, part, sc + 1, ctx->st);             // |w|^2
+    ctx->launches += 6;
+    double h2[2];
+    CK(cudaMemcpyAsync(h2, sc, sizeof h2, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    al.push_back(h2[0]);
+    b = std::sqrt(std::max(h2[1], 0.0));
+    be.push_back(b);
+    if (b < 1e-12) break;
+    launch_lz_next(f, c, p, b, nc, ngp, ctx->st);
+    ctx->launches++;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  const int k = (int)al.size();
+  for (int i = 0; i < k; i++) {
+    if (alpha) alpha[i] = al[i];
+    if (beta) beta[i] = be[i];
+  }
+  if (nsteps) *nsteps = k;
+  double lo = 0.0, hi = 0.0;
+  tridiag_extremes(al.data(), be.data(), k, &lo, &hi);
+  *emin = lo - margin;
+  *emax = hi + margin;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total,
+                                       double *energy_ke, double *energy_pnl) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->filtered || imu < 0 || imu >= ctx->acc_nmu)
+    return set_error(SDFT_ERR_STATE, "energy_chempot_dev: no filtered orbitals");
+  if (nsto_total < 1 || !energy_ke || !energy_pnl) return set_error(SDFT_ERR_ARG, "energy_chempot_dev: bad argument");
+  cudaSetDevice(ctx->device);
+  int r = ensure_red(ctx);
+  if (r) return r;
+  const double *v = ctx->d_acc + (size_t)imu * ctx->vec_elems;
+  double *sc = ctx->d_red + kRedBlocks;
+  launch_ekin(v, nstate, ctx->ncoef, ctx->ngp, ctx->d_ak2, ctx->d_red, sc + 2, ctx->st);
+  ctx->launches += 2;
+  double ek = 0.0, en = 0.0;
+  if (ctx->P) {
+    if ((r = run_kb(ctx, v, nstate, true, false))) return r;
+    CK(cudaMemcpyAsync(&en, ctx->d_enl, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  }
+  CK(cudaMemcpyAsync(&ek, sc + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  *energy_ke = occ * 0.5 * ek / nsto_total;
+  *energy_pnl = occ * en / nsto_total;
+  return SDFT_OK;
+}
+
 extern "C" int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split) {
   if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
   if (split < 0 || split > 64) return set_error(SDFT_ERR_ARG, "gemm_split: 0 (cost model) or 1..64");

@@ -53,6 +53,7 @@ struct sdft_ctx {
   void *d_noise_scratch = nullptr;  // stop flag + phi margin list of the sign generator
   std::vector<sdft_batch *> batches;  // graphs that replay this context's filter
   double *d_enl = nullptr;
+  double *d_red = nullptr;  // reduction partials + scalars (Lanczos, energies)
   // state
   int resident = 0;          // orbitals in d_chi
   int filtered = 0;          // orbitals with results in d_acc

@@ -8,7 +8,7 @@ every request the server
    (admission); memory is reserved from an estimate and corrected to the
    context's measured footprint once it exists;
 2. prepares it on its own context: V_KS, KB projectors, 20-step Lanczos
-   bounds, noise orbitals generated on the device, Chebyshev moments, mu by
+   bounds (device resident), noise orbitals generated on the device, Chebyshev moments, mu by
    the FP64 bisection (calcChemPotCheby) and the filter coefficients;
 3. captures its Chebyshev filter + density as a one-context CUDA graph
    (sdft_batch) and launches it on the request's own stream, so requests
@@ -52,7 +52,7 @@ def prepare(pkg, wl, s, nsto, L, precision, seed, device=0, tuner=None, mu=None,
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
     t.append(time.perf_counter())
-    emin, emax = wl.lanczos_bounds(lambda r, i: ctx.calc_coef_force(r, i), s["ncoef"])
+    emin, emax = ctx.lanczos_bounds(20, seed=15, margin=0.1)[:2]  # device Lanczos, same start vector as the host one
     ediff, emean = emax - emin, 0.5 * (emin + emax)
     scale = 2.0 / ediff
     t.append(time.perf_counter())

@@ -1,0 +1,76 @@
+"""Device Lanczos bounds (the role of genEnergyMax/genEnergyMin,
+stodft/calc-spectral-range.c:33,339, run as 20 Lanczos steps) and the
+energies of the filtered orbitals (calcEnergyChemPot, stodft/calc-energy.c:
+32-207) against the host Lanczos of the same H and against the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(pkg, s, prec, n):
+    c = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=n)
+    c.set_vks(s["vks"])
+    c.set_kb(s["kb_desc"])
+    return c
+
+
+@pytest.mark.parametrize("which,prec,tol", [("sys1", "fp64", 1e-9), ("sys2", "fp64", 1e-9), ("sys2", "mixed", 1e-6)])
+def test_lanczos_bounds_match_host_lanczos(pkg, wl, sys1, sys2, which, prec, tol):
+    s = sys1 if which == "sys1" else sys2
+    p = pkg.SDFT_PREC_FP64 if prec == "fp64" else pkg.SDFT_PREC_MIXED
+    host = _ctx(pkg, s, p, 1)
+    dev = _ctx(pkg, s, p, 1)
+    try:
+        lo_h, hi_h = wl.lanczos_bounds(lambda r, i: host.calc_coef_force(r, i), s["ncoef"])
+        lo_d, hi_d, al, be = dev.lanczos_bounds(20, seed=15, margin=0.1)
+    finally:
+        host.close()
+        dev.close()
+    assert len(al) == 20 and np.all(be > 0)
+    assert abs(lo_d - lo_h) <= tol and abs(hi_d - hi_h) <= tol
+    # the tridiagonal extremes by Sturm bisection agree with a dense solver
+    T = np.diag(al) + np.diag(be[:-1], 1) + np.diag(be[:-1], -1)
+    ev = np.linalg.eigvalsh(T)
+    assert abs(ev[0] - 0.1 - lo_d) < 1e-10 and abs(ev[-1] + 0.1 - hi_d) < 1e-10
+
+
+def _ak2(s):
+    L = np.diag(np.asarray(s["hmat"], float))
+    g = [2.0 * math.pi * np.asarray(s[k], float) / L[i] for i, k in enumerate(("ka", "kb", "kc"))]
+    return g[0] ** 2 + g[1] ** 2 + g[2] ** 2
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 2e-7)])
+def test_energy_chempot_matches_oracle(pkg, wl, sys1, prec, tol):
+    s = sys1
+    ns, L = 6, 32
+    rng = np.random.default_rng(21)
+    cr = rng.standard_normal(ns * s["ncoef"])
+    ci = rng.standard_normal(ns * s["ncoef"])
+    ci.reshape(ns, -1)[:, -1] = 0.0
+    o = O.OracleSys(s)
+    lo, hi = wl.lanczos_bounds(lambda r, i: o.hpsi(r, i), s["ncoef"])
+    ediff, emean = hi - lo, 0.5 * (hi + lo)
+    ec = pkg.calcChebyCoeff(L, ediff, emean, wl.BETA, 0.1, fun_flag=2)
+    p = pkg.SDFT_PREC_FP64 if prec == "fp64" else pkg.SDFT_PREC_MIXED
+    ctx = _ctx(pkg, s, p, ns)
+    try:
+        ctx.upload(cr, ci)
+        ctx.filter_cheby_dev(ns, ec, 1, 2.0 / ediff, emean)
+        ek, ep = ctx.energy_chempot_dev(ns, 0, occ=2.0, nsto_total=ns)
+        fr, fi = ctx.download_filtered(ns)
+    finally:
+        ctx.close()
+    # expectation from the FP64 oracle filter of the same orbitals
+    orr, oii = (a[0] for a in o.filter_cheby(cr, ci, ec, 1, 2.0 / ediff, emean))
+    ak2 = _ak2(s)[:-1]
+    R, I = orr.reshape(ns, -1)[:, :-1], oii.reshape(ns, -1)[:, :-1]
+    ek_ref = 2.0 * 0.5 * float(np.sum(2.0 * ak2 * (R * R + I * I))) / ns
+    ep_ref = 2.0 * o.hpsi(orr, oii, want_enl=True)[2] / ns
+    assert abs(ek - ek_ref) <= tol * abs(ek_ref)
+    assert abs(ep - ep_ref) <= tol * abs(ep_ref)

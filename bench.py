@@ -228,7 +228,7 @@ def run_ours(args):
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
     t0 = time.time()
-    emin, emax = wl.lanczos_bounds(lambda r, i: ctx.calc_coef_force(r, i), s["ncoef"])
+    emin, emax = ctx.lanczos_bounds(20, seed=15, margin=0.1)[:2]  # 20 device Lanczos steps
     ediff, emean = emax - emin, 0.5 * (emin + emax)
     scale = 2.0 / ediff
     # noise of this state rank (np_states = world): host copy kept for the e2e leg

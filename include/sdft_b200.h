@@ -27,6 +27,8 @@
  *   sdft_gaussran2_signs_dev          <- the gaussran2 call of genNoiseOrbitalReal, stodft/gen-noise.c:256 (signs only)
  *   sdft_lanczos_bounds               <- genEnergyMax/genEnergyMin stodft/calc-spectral-range.c:33,339 (Lanczos)
  *   sdft_energy_chempot_dev           <- calcEnergyChemPot stodft/calc-energy.c:32
+ *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
+ *                                        stodft/checkpointIO.c:32,218
  */
 #ifndef SDFT_B200_H
 #define SDFT_B200_H
@@ -208,6 +210,36 @@ int sdft_lanczos_bounds(sdft_ctx *ctx, int nstep, const double *v0re, const doub
  * ranks, sum the per-rank values (each passing the global nsto_total). */
 int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total,
                             double *energy_ke, double *energy_pnl);
+
+/* ---- density mixing and checkpoint files -------------------------------- */
+/* genDensityMix (stodft/diis.c:34-464) with the densities on the device,
+ * spin-unpolarised, one rank (with several ranks, each mixes its own slice
+ * of the grid; the DIIS dot products then need a sum over ranks, which this
+ * mixer does not do).  n grid values; num_diis <= 16 DIIS terms; the first
+ * num_step_mix steps after step 0 mix with mix_ratio_big, later ones run
+ * DIIS with the extra mixing alpha = mix_ratio_sm (steps <= 10) or
+ * mix_ratio_sm2. */
+typedef struct sdft_mixer sdft_mixer;
+int sdft_mixer_create(int device, long long n, int num_diis, int num_step_mix, double mix_ratio_big,
+                      double mix_ratio_sm, double mix_ratio_sm2, sdft_mixer **out);
+/* One SCF step iscf (0, 1, 2, ...): rho_correct = the new density
+ * (rhoUpCorrect), rho = the mixed density (rho_up), written for iscf >= 1
+ * and left untouched at iscf 0 as the reference does.  Host or device
+ * pointers (unified addressing). */
+int sdft_mixer_step(sdft_mixer *m, int iscf, const double *rho_correct, double *rho);
+/* Last step index, min(iscf, num_diis) and the DIIS coefficients of the
+ * last DIIS step (nullable outputs). */
+int sdft_mixer_state(const sdft_mixer *m, int *iscf, int *num_diis_now, double *coef);
+/* checkpointOutput (stodft/checkpointIO.c:32): text file "iscf numDiisNow",
+ * rho * vol, the banked densities and the errors, one "%.16lg" value per
+ * line -- byte-identical to the reference's density-checkpoint. */
+int sdft_mixer_write_checkpoint(sdft_mixer *m, const char *path, const double *rho, double vol);
+/* checkpointInput (stodft/checkpointIO.c:218): restores the step index,
+ * the banks and errors; rho and the mixer's rho_old receive the file's
+ * density values as stored (rho * vol, not divided back, as the reference
+ * does). */
+int sdft_mixer_read_checkpoint(sdft_mixer *m, const char *path, double *rho);
+int sdft_mixer_destroy(sdft_mixer *m);
 
 /* ---- tuning and batched systems ---------------------------------------- */
 /* No counterpart in the reference (it filters one system per run).

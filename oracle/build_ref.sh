@@ -16,7 +16,7 @@ SRCS="stodft/filter.c stodft/normh.c stodft/calc-chempot-chebyshev.c stodft/coef
       stodft/reduced-energy/cp-energy-ee-rho-stodft.c mathlib/fft_package.c mathlib/fft_create_package.c
       mathlib/mathlib.c energy/cp/cp_energy_eext_nonloc.c energy/cp/cp_energy_eext.c
       energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c
-      stodft/density.c stodft/gen-noise.c"
+      stodft/density.c stodft/gen-noise.c stodft/diis.c stodft/checkpointIO.c"
 OBJS=""
 for f in $SRCS; do
   o="$OUT/obj/$(echo "$f" | tr '/' '_').o"
@@ -24,6 +24,9 @@ for f in $SRCS; do
   # so the reference's own generator is compiled under another name
   EXTRA=""
   [ "$f" = "stodft/gen-noise.c" ] && EXTRA="-DgenNoiseOrbitalReal=ref_genNoiseOrbitalReal"
+  # checkpointIO.c uses the MPI datatype names without declaring them (a
+  # single-rank build never reaches the MPI calls)
+  [ "$f" = "stodft/checkpointIO.c" ] && EXTRA="-DMPI_DOUBLE=1 -DMPI_INT=2"
   if [ ! -f "$o" ] || [ "$REF/$f" -nt "$o" ]; then gcc -c $CFLAGS $EXTRA $INC "$REF/$f" -o "$o"; fi
   OBJS="$OBJS $o"
 done

@@ -36,6 +36,12 @@ def lib():
         L.ref_gaussran2.argtypes = [C.c_int, _dp, _dp]
         L.ref_noise.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
         L.ref_density.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
+        L.ref_mix_create.restype = C.c_void_p
+        L.ref_mix_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.ref_mix_step.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.ref_mix_set_rho.argtypes = [C.c_void_p, _dp]
+        L.ref_mix_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]
+        L.ref_mix_checkpoint.restype = C.c_int
         _lib = L
     return _lib
 
@@ -139,3 +145,28 @@ def gaussran2(n, seed):
 
 def round_fft(n):
     return lib().ref_round_fft(n)
+
+
+class RefMixer:
+    """genDensityMix (stodft/diis.c:34) and checkpointOutput
+    (stodft/checkpointIO.c:32) of the reference on one rank.  The handle is
+    not freed (test use)."""
+
+    def __init__(self, n, num_diis, num_step_mix, mix_ratio_big, mix_ratio_sm, mix_ratio_sm2):
+        self.n = int(n)
+        self._p = C.c_void_p(lib().ref_mix_create(self.n, num_diis, num_step_mix, mix_ratio_big, mix_ratio_sm,
+                                                  mix_ratio_sm2))
+
+    def set_rho(self, rho):
+        lib().ref_mix_set_rho(self._p, _d(f64(rho)))
+
+    def step(self, iscf, rho_correct):
+        out = np.zeros(self.n)
+        lib().ref_mix_step(self._p, int(iscf), _d(f64(rho_correct)), _d(out))
+        return out
+
+    def checkpoint(self, directory, cell):
+        rc = lib().ref_mix_checkpoint(self._p, str(directory).encode(), *[float(x) for x in cell])
+        if rc:
+            raise OSError("checkpointOutput harness failed")
+        return os.path.join(str(directory), "density-checkpoint")

@@ -23,6 +23,7 @@
 #include "../typ_defs/typedefs_bnd.h"
 #include "../typ_defs/typedefs_cp.h"
 #include <time.h>
+#include <unistd.h>
 
 /* reference prototypes used here */
 void create_para_fft_pkg3d(PARA_FFT_PKG3D *, int *, int *, int *, int);
@@ -160,14 +161,14 @@ static void sdft_ref_abort(const char *f) {
   void name(void) { sdft_ref_abort(#name); }
 ABORT_STUB(Allgather) ABORT_STUB(Allgatherv) ABORT_STUB(Allreduce) ABORT_STUB(Alltoall) ABORT_STUB(Alltoallv)
 ABORT_STUB(Finalize) ABORT_STUB(Gatherv) ABORT_STUB(Reduce) ABORT_STUB(Reduce_scatter) ABORT_STUB(Scatterv)
-ABORT_STUB(Bcast) ABORT_STUB(DGEMV) ABORT_STUB(DSYMV) ABORT_STUB(dsysv_) ABORT_STUB(rs_)
+ABORT_STUB(Bcast) ABORT_STUB(Send) ABORT_STUB(Recv) ABORT_STUB(DGEMV) ABORT_STUB(DSYMV) ABORT_STUB(dsysv_) ABORT_STUB(rs_)
 ABORT_STUB(calcChemPotInterp) ABORT_STUB(calcCoefForceWrap) ABORT_STUB(coef_force_calc_hybrid_threads_state)
 ABORT_STUB(coef_force_tau_fun_full_g) ABORT_STUB(coef_force_tau_fun_hybrid)
 ABORT_STUB(controlEnergyNlppRealThreads) ABORT_STUB(controlPotentialEnergyFilter) ABORT_STUB(control_contract_rho)
 ABORT_STUB(control_grad_rho) ABORT_STUB(control_nonloc_gh) ABORT_STUB(control_spread_rho)
 ABORT_STUB(cp_condiag_ksmat) ABORT_STUB(cp_rotate_vector) ABORT_STUB(dcfftb_generic_) ABORT_STUB(dcfftf_generic_)
 ABORT_STUB(dcffti_generic_) ABORT_STUB(excpot_pade_lda) ABORT_STUB(excpot_pade_lsda) ABORT_STUB(excpot_pw_lda)
-ABORT_STUB(excpot_pw_lsda) ABORT_STUB(excpot_pz_lda) ABORT_STUB(excpot_pz_lsda) ABORT_STUB(genDensityMix)
+ABORT_STUB(excpot_pw_lsda) ABORT_STUB(excpot_pz_lda) ABORT_STUB(excpot_pz_lsda)
 ABORT_STUB(getnl_fcoef_gh) ABORT_STUB(getnl_pot_pv_fatm_gh) ABORT_STUB(grad_corr_lda) ABORT_STUB(grad_corr_lsda)
 ABORT_STUB(cfopen)
 void Barrier(int c) { (void)c; }
@@ -532,4 +533,140 @@ int ref_density(RefSys *r, int ns, const double *re, const double *im, double *r
 void ref_gaussran2(int n, double *seed, double *out) {
   int is = 0;
   gaussran2(n, &is, &is, seed, out);
+}
+
+/* ====================================================================== */
+/* Density mixing (stodft/diis.c: genDensityMix) and checkpoint output     */
+/* (stodft/checkpointIO.c: checkpointOutput), single rank, spin-unpolarised */
+/* ====================================================================== */
+void genDensityMix(CP *, int);
+void checkpointOutput(CP *, GENERAL_DATA *);
+
+/* LAPACK dgesvd (A = U S V^T, column-major, square) by one-sided Jacobi
+ * (Hestenes) rotations; singular values in descending order.  Project-
+ * written stand-in for MKL: only diis.c's matrixInvSVD calls it. */
+void dgesvd_(char *jobu, char *jobvt, int *m, int *n, double *a, int *lda, double *s, double *u, int *ldu,
+             double *vt, int *ldvt, double *work, int *lwork, int *info) {
+  (void)jobu; (void)jobvt; (void)work; (void)lwork;
+  const int nn = *n, ld = *lda;
+  *info = 0;
+  if (*m != nn) { *info = -2; return; }
+  double *w = malloc(sizeof(double) * nn * nn), *v = calloc((size_t)nn * nn, sizeof(double));
+  for (int c = 0; c < nn; c++) {
+    for (int r = 0; r < nn; r++) w[r + c * nn] = a[r + c * ld];
+    v[c + c * nn] = 1.0;
+  }
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0;
+    for (int p = 0; p < nn - 1; p++)
+      for (int q = p + 1; q < nn; q++) {
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int r = 0; r < nn; r++) {
+          al += w[r + p * nn] * w[r + p * nn];
+          be += w[r + q * nn] * w[r + q * nn];
+          ga += w[r + p * nn] * w[r + q * nn];
+        }
+        if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
+        off = fmax(off, fabs(ga) / sqrt(al * be));
+        const double ze = (be - al) / (2.0 * ga);
+        const double tt = (ze >= 0.0 ? 1.0 : -1.0) / (fabs(ze) + sqrt(1.0 + ze * ze));
+        const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
+        for (int r = 0; r < nn; r++) {
+          const double x = w[r + p * nn], y = w[r + q * nn];
+          w[r + p * nn] = cs * x - sn * y;
+          w[r + q * nn] = sn * x + cs * y;
+          const double vx = v[r + p * nn], vy = v[r + q * nn];
+          v[r + p * nn] = cs * vx - sn * vy;
+          v[r + q * nn] = sn * vx + cs * vy;
+        }
+      }
+    if (off == 0.0) break;
+  }
+  int *ord = malloc(sizeof(int) * nn);
+  double *sv = malloc(sizeof(double) * nn);
+  for (int c = 0; c < nn; c++) {
+    double t2 = 0.0;
+    for (int r = 0; r < nn; r++) t2 += w[r + c * nn] * w[r + c * nn];
+    sv[c] = sqrt(t2);
+    ord[c] = c;
+  }
+  for (int i = 1; i < nn; i++)
+    for (int j = i; j > 0 && sv[ord[j]] > sv[ord[j - 1]]; j--) { int x = ord[j]; ord[j] = ord[j - 1]; ord[j - 1] = x; }
+  for (int k = 0; k < nn; k++) {
+    const int c = ord[k];
+    s[k] = sv[c];
+    for (int r = 0; r < nn; r++) {
+      u[r + k * *ldu] = sv[c] > 0.0 ? w[r + c * nn] / sv[c] : 0.0;
+      vt[k + r * *ldvt] = v[r + c * nn];
+    }
+  }
+  free(w); free(v); free(ord); free(sv);
+}
+
+/* BLAS dgemv: y = alpha op(A) x + beta y, column-major */
+void dgemv_(char *trans, int *m, int *n, double *alpha, double *a, int *lda, double *x, int *incx, double *beta,
+            double *y, int *incy) {
+  const int tr = (*trans == 't' || *trans == 'T');
+  const int ny = tr ? *n : *m, nx = tr ? *m : *n;
+  for (int i = 0; i < ny; i++) {
+    double acc = 0.0;
+    for (int j = 0; j < nx; j++) acc += (tr ? a[j + i * *lda] : a[i + j * *lda]) * x[j * *incx];
+    y[i * *incy] = *alpha * acc + *beta * y[i * *incy];
+  }
+}
+
+typedef struct {
+  CP cp;
+  GENERAL_DATA gd;
+  STODFTINFO si;
+  STODFTCOEFPOS sp;
+  double *rho1;  /* rho_up, 1-based */
+  double hmat[10];
+} RefMix;
+
+RefMix *ref_mix_create(int n, int num_diis, int num_step_mix, double r_big, double r_sm, double r_sm2) {
+  RefMix *m = calloc(1, sizeof(RefMix));
+  m->cp.stodftInfo = &m->si;
+  m->cp.stodftCoefPos = &m->sp;
+  m->cp.cpopts.cp_lsda = 0;
+  m->cp.communicate.myid_state = 0;
+  m->cp.communicate.np_states = 1;
+  m->si.rhoRealGridNum = n;
+  m->si.rhoRealGridTot = n;
+  m->si.numDiis = num_diis;
+  m->si.numStepMix = num_step_mix;
+  m->si.mixRatioBig = r_big;
+  m->si.mixRatioSM = r_sm;
+  m->si.mixRatioSM2 = r_sm2;
+  m->sp.rhoUpCorrect = malloc(sizeof(double) * n);
+  m->sp.rhoUpOld = malloc(sizeof(double) * n);
+  m->sp.rhoUpBank = calloc(num_diis + 1, sizeof(double *));
+  m->sp.rhoUpErr = calloc(num_diis + 1, sizeof(double *));
+  m->sp.diisCoeff = calloc(num_diis + 1, sizeof(double));
+  m->rho1 = calloc(n + 1, sizeof(double));
+  m->cp.cpscr.cpscr_rho.rho_up = m->rho1;
+  m->gd.cell.hmat_cp = m->hmat;
+  return m;
+}
+
+/* one SCF step of genDensityMix: rho_out = the mixed rho_up (unchanged from
+ * the previous step's value at iscf == 0, as in the reference) */
+void ref_mix_step(RefMix *m, int iscf, const double *rho_correct, double *rho_out) {
+  memcpy(m->sp.rhoUpCorrect, rho_correct, sizeof(double) * m->si.rhoRealGridNum);
+  m->si.iScf = iscf;
+  genDensityMix(&m->cp, iscf);
+  memcpy(rho_out, &m->rho1[1], sizeof(double) * m->si.rhoRealGridNum);
+}
+
+void ref_mix_set_rho(RefMix *m, const double *rho) { memcpy(&m->rho1[1], rho, sizeof(double) * m->si.rhoRealGridNum); }
+
+/* checkpointOutput into dir/density-checkpoint (the reference writes to the
+ * working directory); cell = diag(l1, l2, l3) for the volume factor */
+int ref_mix_checkpoint(RefMix *m, const char *dir, double l1, double l2, double l3) {
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof cwd) || chdir(dir) != 0) return 1;
+  memset(m->hmat, 0, sizeof m->hmat);
+  m->hmat[1] = l1; m->hmat[5] = l2; m->hmat[9] = l3;
+  checkpointOutput(&m->cp, &m->gd);
+  return chdir(cwd) != 0;
 }

@@ -117,6 +117,13 @@ _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
+_sig("sdft_mixer_create", C.c_int, [C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.POINTER(_vp)])
+_sig("sdft_mixer_step", C.c_int, [_vp, C.c_int, _vp, _vp])
+_sig("sdft_mixer_state", C.c_int, [_vp, _ip, _ip, _dp])
+_sig("sdft_mixer_write_checkpoint", C.c_int, [_vp, C.c_char_p, _vp, C.c_double])
+_sig("sdft_mixer_read_checkpoint", C.c_int, [_vp, C.c_char_p, _vp])
+_sig("sdft_mixer_destroy", C.c_int, [_vp])
 _sig("sdft_lanczos_bounds", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _ip, _dp, _dp])
 _sig("sdft_energy_chempot_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp])
 _sig("sdft_batch_set_priority", C.c_int, [_vp, C.c_int])
@@ -473,6 +480,61 @@ class Context:
         im = np.zeros(nstate * self.ncoef)
         _chk(lib.sdft_download_filtered(self._p, nstate, imu, _d(re), _d(im)))
         return re, im
+
+
+class DensityMixer:
+    """genDensityMix (stodft/diis.c:34) on the device (sdft_mixer_*), with
+    checkpointOutput / checkpointInput files (stodft/checkpointIO.c).
+    step() takes and returns numpy arrays, or device pointers (ints)."""
+
+    def __init__(self, n, num_diis, num_step_mix, mix_ratio_big, mix_ratio_sm, mix_ratio_sm2, device=0):
+        self.n = int(n)
+        p = _vp()
+        _chk(lib.sdft_mixer_create(int(device), self.n, int(num_diis), int(num_step_mix), float(mix_ratio_big),
+                                   float(mix_ratio_sm), float(mix_ratio_sm2), C.byref(p)))
+        self._p = p
+
+    @staticmethod
+    def _ptr(a):
+        return C.c_void_p(a) if isinstance(a, int) else a.ctypes.data_as(_vp)
+
+    def step(self, iscf, rho_correct, rho=None):
+        """One SCF step; returns rho (the mixed density; unchanged at iscf 0)."""
+        if isinstance(rho_correct, int):
+            if not isinstance(rho, int):
+                raise TypeError("device rho_correct needs a device rho pointer")
+            _chk(lib.sdft_mixer_step(self._p, int(iscf), C.c_void_p(rho_correct), C.c_void_p(rho)))
+            return rho
+        rc = _f64(rho_correct)
+        out = np.zeros(self.n) if rho is None else rho
+        _chk(lib.sdft_mixer_step(self._p, int(iscf), self._ptr(rc), self._ptr(out)))
+        return out
+
+    def state(self):
+        it, nd = C.c_int(0), C.c_int(0)
+        coef = np.zeros(16)
+        _chk(lib.sdft_mixer_state(self._p, C.byref(it), C.byref(nd), _d(coef)))
+        return it.value, nd.value, coef[:nd.value]
+
+    def write_checkpoint(self, path, rho, vol):
+        r = rho if isinstance(rho, int) else _f64(rho)
+        _chk(lib.sdft_mixer_write_checkpoint(self._p, str(path).encode(), self._ptr(r), float(vol)))
+
+    def read_checkpoint(self, path):
+        rho = np.zeros(self.n)
+        _chk(lib.sdft_mixer_read_checkpoint(self._p, str(path).encode(), self._ptr(rho)))
+        return rho
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib.sdft_mixer_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

@@ -709,7 +709,7 @@ def run_serve(args):
     recs = {}
     for name, prec in (("mixed", pkg.SDFT_PREC_MIXED), ("fp64", pkg.SDFT_PREC_FP64)):
         srv = serve.Server(pkg, wl, prec, hbm_budget=150e9, slots=args.slots, workers=args.workers,
-                           priorities=not args.no_priorities)
+                           priorities=not args.no_priorities, graph=not args.serve_eager)
         srv.run([dict(r, arrival=0.0) for r in reqs[:2]])  # warm-up (module loads, first-use attributes)
         # FP64 serves the same stream with the mixed run's mu, so the density
         # difference is the precision alone (the moments are still computed)
@@ -732,6 +732,7 @@ def run_serve(args):
                                f"{args.workers} host workers, HBM budget 150 GB",
                    "stream_priorities": "by request work (serve.request_priority)" if not args.no_priorities
                    else "off",
+                   "request_launch": "kernels on the request stream" if args.serve_eager else "captured CUDA graph",
                    "requests": len(reqs), "orbitals": m["orbitals"],
                    "atoms": [int(8 * np.prod(r["spec"]["nrep"])) for r in reqs]},
         "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"], "mean": m["mean_ms"],
@@ -765,6 +766,8 @@ def main():
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
     ap.add_argument("--workers", type=int, default=16, help="cfg5: host threads preparing requests")
     ap.add_argument("--no-priorities", action="store_true", help="cfg5: all request streams at default priority")
+    ap.add_argument("--serve-eager", action="store_true",
+                    help="cfg5: issue each request's kernels directly instead of as a captured CUDA graph")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -10,11 +10,13 @@ every request the server
 2. prepares it on its own context: V_KS, KB projectors, 20-step Lanczos
    bounds (device resident), noise orbitals generated on the device, Chebyshev moments, mu by
    the FP64 bisection (calcChemPotCheby) and the filter coefficients;
-3. captures its Chebyshev filter + density as a one-context CUDA graph
-   (sdft_batch) and launches it on the request's own stream, so requests
-   admitted while others run overlap on the device; the request's streams
-   get a CUDA priority by its work (request_priority: cheaper = more urgent),
-   so short requests are not queued behind 512-atom ones;
+3. issues its Chebyshev filter + density on the request's own stream as a
+   captured one-context CUDA graph (sdft_batch; graph=False issues the
+   kernels directly, which measured slower: thousands of launches from
+   concurrent host threads), so requests admitted while others run overlap
+   on the device; the request's streams get a CUDA priority by its work
+   (request_priority: cheaper = more urgent), so short requests are not
+   queued behind 512-atom ones;
 4. when the graph's completion event fires, downloads the density, frees the
    context and returns its memory to the budget.
 
@@ -114,9 +116,10 @@ class Server:
     release the interpreter lock)."""
 
     def __init__(self, pkg, wl, precision, hbm_budget=150e9, slots=16, device=0, tuner=None, workers=4,
-                 priorities=True):
+                 priorities=True, graph=True):
         self.pkg, self.wl = pkg, wl
         self.priorities = bool(priorities)
+        self.graph = bool(graph)
         self.precision = precision
         self.budget = float(hbm_budget)
         self.slots = int(slots)
@@ -136,12 +139,18 @@ class Server:
                     mu=r.get("mu"), priority=prio)
         ctx = p["ctx"]
         tc = time.perf_counter()
-        b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
-        if prio is not None:
-            b.set_priority(prio)
-        p["phases"].update(build_s=build_s, capture_s=time.perf_counter() - tc)
-        st = torch.cuda.ExternalStream(b.stream_ptr)
-        b.launch()
+        if self.graph:  # one captured graph per request, replayed once
+            b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
+            if prio is not None:
+                b.set_priority(prio)
+            st = torch.cuda.ExternalStream(b.stream_ptr)
+            b.launch()
+        else:  # the same kernels issued directly on the context's stream (no capture / instantiation)
+            b = None
+            st = torch.cuda.ExternalStream(ctx.stream_ptr)
+            ctx.filter_cheby_dev(r["nsto"], p["ec"], 1, p["scale"], p["emean"])
+            ctx.density_dev(r["nsto"], 0, p["occ_over"], want=False)
+        p["phases"].update(build_s=build_s, launch_s=time.perf_counter() - tc)
         ev = torch.cuda.Event(enable_timing=True)
         ev.record(st)
         return dict(i=i, ctx=ctx, batch=b, ev=ev, mem=ctx.device_bytes, t_adm=t_adm, prep=p, natm=s["natm"])
@@ -197,7 +206,10 @@ class Server:
                 still = []
                 for a in active:
                     if a["ev"].query():
-                        a["batch"].sync()
+                        if a["batch"] is not None:
+                            a["batch"].sync()
+                        else:
+                            a["ctx"].sync()
                         i = a["i"]
                         rho = a["ctx"].download_density() if keep_density else None
                         t_done = t0_ev.elapsed_time(a["ev"]) / 1e3
@@ -207,7 +219,8 @@ class Server:
                                       mu=a["prep"]["mu"],
                                       num_elec=float(rho.sum() / rho.size) if rho is not None else None, density=rho,
                                       phases=a["prep"]["phases"])
-                        a["batch"].close()
+                        if a["batch"] is not None:
+                            a["batch"].close()
                         a["ctx"].close()
                         used -= a["mem"]
                     else:

@@ -44,11 +44,12 @@ def test_batch_graph_matches_eager(pkg, wl, prec):
         p["ctx"].close()
 
 
-def test_serving_same_result_alone_and_in_mix(pkg, wl):
+@pytest.mark.parametrize("graph", [False, True])
+def test_serving_same_result_alone_and_in_mix(pkg, wl, graph):
     serve = _serve_mod(pkg)
     reqs = [dict(arrival=0.0 + 0.001 * i, spec=sp, nsto=sp["nsto"], L=sp["L"], seed=30.0 + i)
             for i, sp in enumerate(SPECS)]
-    srv = serve.Server(pkg, wl, pkg.SDFT_PREC_MIXED, hbm_budget=150e9, slots=8)
+    srv = serve.Server(pkg, wl, pkg.SDFT_PREC_MIXED, hbm_budget=150e9, slots=8, graph=graph)
     mix, summ = srv.run(reqs)
     assert summ["requests"] == 3 and summ["p99_ms"] >= summ["p50_ms"] > 0
     for i, r in enumerate(reqs):

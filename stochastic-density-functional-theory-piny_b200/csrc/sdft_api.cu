@@ -564,6 +564,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   if (cudaSetDevice(device) != cudaSuccess) return fail(set_error(SDFT_ERR_CUDA, "cudaSetDevice failed"));
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess)
     return fail(set_error(SDFT_ERR_CUDA, "stream create failed"));
+  if (init_const_twiddles()) return fail(set_error(SDFT_ERR_CUDA, "constant twiddle tables"));
   std::vector<int> cpg, cpc, colab;
   int r = build_columns(ctx, cpg, cpc, colab);
   if (r) return fail(r);

@@ -146,9 +146,14 @@ struct UnitIter {
   }
 };
 
-// natural -> permuted.  twN: exp(-2 pi i t/N) in shared memory.
-template <int N, int ES, int DIR, typename C, typename LM>
-__device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
+// Twiddle source of dif/dit: exp(-2 pi i t/N) from a shared-memory table
+// (pointer) or from an accessor object with operator()(t).
+template <typename C, typename P> __device__ __forceinline__ C tw_at(P *tw, int t) { return lds_tw(tw + t); }
+template <typename C, typename TW> __device__ __forceinline__ C tw_at(const TW &tw, int t) { return tw(t); }
+
+// natural -> permuted.  twN: exp(-2 pi i t/N) (shared-memory table or accessor).
+template <int N, int ES, int DIR, typename C, typename LM, typename TW>
+__device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
   if (nl > 0) {
 #pragma unroll 1
@@ -163,7 +168,7 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, 
       p[j2 * ES] = v[0];
 #pragma unroll
       for (int k1 = 1; k1 < R1; k1++) {
-        C w = lds_tw(twN + j2 * k1);
+        C w = tw_at<C>(twN, j2 * k1);
         if (DIR > 0) w.y = -w.y;
         p[(j2 + R2 * k1) * ES] = cmul(v[k1], w);
       }
@@ -188,8 +193,8 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const C *twN, 
 }
 
 // permuted -> natural
-template <int N, int ES, int DIR, typename C, typename LM>
-__device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, int tid, int nthr) {
+template <int N, int ES, int DIR, typename C, typename LM, typename TW>
+__device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
   if (nl > 0) {
 #pragma unroll 1
@@ -204,7 +209,7 @@ __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const C *twN, 
       p[0] = v[0];
 #pragma unroll
       for (int j2 = 1; j2 < R2; j2++) {
-        C w = lds_tw(twN + j2 * k1);
+        C w = tw_at<C>(twN, j2 * k1);
         if (DIR > 0) w.y = -w.y;
         p[j2 * ES] = cmul(v[j2], w);
       }

@@ -11,12 +11,61 @@
 //   stage C transforms X rows r back to natural kc (permuted -> natural).
 // So no data movement is ever spent on undoing an FFT permutation.
 #include <cuda_runtime.h>
+#include <cmath>
 #include "sdft_fft2.cuh"
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
 #include "sdft_kernels2.cuh"
 
 namespace sdft {
+
+// exp(-2 pi i t/N) of every compile-time FFT edge in constant memory (the
+// warps of the plane passes read one twiddle index at a time, which the
+// constant cache broadcasts without a shared-memory wavefront); offsets of
+// the edges 12, 16, 24, 32, 36, 48, 64, 72, 96, 128
+constexpr int kTwEdges[] = {12, 16, 24, 32, 36, 48, 64, 72, 96, 128};
+constexpr int kTwTotal = 528;
+constexpr int tw_off(int n) {
+  int o = 0;
+  for (int e : kTwEdges) {
+    if (e == n) return o;
+    o += e;
+  }
+  return -1;
+}
+template <int N> struct TwOff {
+  static constexpr int value = tw_off(N);
+  static_assert(value >= 0, "edge without a constant twiddle table");
+};
+__constant__ float2 c_twf[kTwTotal];
+__constant__ double2 c_twd[kTwTotal];
+
+template <int N, typename C> struct TwC;
+template <int N> struct TwC<N, float2> {
+  __device__ __forceinline__ float2 operator()(int t) const { return c_twf[TwOff<N>::value + t]; }
+};
+template <int N> struct TwC<N, double2> {
+  __device__ __forceinline__ double2 operator()(int t) const { return c_twd[TwOff<N>::value + t]; }
+};
+
+int init_const_twiddles() {
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  if (done[dev]) return 0;
+  float2 hf[kTwTotal];
+  double2 hd[kTwTotal];
+  for (int e : kTwEdges)
+    for (int t = 0; t < e; t++) {  // the same values as the context's twiddle tables
+      const double a = 2.0 * M_PI * (double)t / (double)e;
+      hd[tw_off(e) + t] = make_double2(std::cos(a), -std::sin(a));
+      hf[tw_off(e) + t] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+  if (cudaMemcpyToSymbol(c_twf, hf, sizeof hf) != cudaSuccess) return 1;
+  if (cudaMemcpyToSymbol(c_twd, hd, sizeof hd) != cudaSuccess) return 1;
+  done[dev] = true;
+  return 0;
+}
 
 template <typename T> __device__ __forceinline__ const typename CT<T>::type *twp(const DevGeom &g, int d);
 template <> __device__ __forceinline__ const double2 *twp<double>(const DevGeom &g, int d) {
@@ -403,9 +452,9 @@ template <int N1> struct RowsPerm {  // rows given in permuted-a order
 // DFT -> x V -> inverse DFT without a round trip through shared memory.
 // Rows with kamax < ka < N1 - kamax are zero on input (outside the sphere)
 // and not needed on output: they are neither read nor written.
-template <int N1, typename C2, typename T>
+template <int N1, typename C2, typename T, typename TW>
 __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, const T *__restrict__ Vpl, int kamax,
-                                             const C2 *tw1, int tid, int nthr) {
+                                             const TW &tw1, int tid, int nthr) {
   constexpr int R1 = Plan<N1>::R1, R2 = Plan<N1>::R2;
   auto active = [&](int ka) { return ka <= kamax || ka >= N1 - kamax; };
 #pragma unroll 1
@@ -422,7 +471,7 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
     p[j2 * P2] = v[0];
 #pragma unroll
     for (int k1 = 1; k1 < R1; k1++) {
-      C2 w = lds_tw(tw1 + j2 * k1);
+      C2 w = tw_at<C2>(tw1, j2 * k1);
       w.y = -w.y;
       p[(j2 + R2 * k1) * P2] = cmul(v[k1], w);
     }
@@ -442,7 +491,7 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
     dftr<R2, -1>(v);
     p[0] = v[0];
 #pragma unroll
-    for (int j2 = 1; j2 < R2; j2++) p[j2 * P2] = cmul(v[j2], lds_tw(tw1 + j2 * k1));
+    for (int j2 = 1; j2 < R2; j2++) p[j2 * P2] = cmul(v[j2], tw_at<C2>(tw1, j2 * k1));
   }
   __syncthreads();
 #pragma unroll 1
@@ -495,9 +544,9 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
   // b-transforms over the sphere rows, each row group padded to 16 lanes
   const int g1 = (ka + 1 + 15) & ~15, g2 = (ka + 15) & ~15;
   const Lines2P rowsp{ka + 1, g1, ka, P2, (N1 - ka) * P2};
-  dif<N2, 1, +1>(pl, rowsp, g1 + g2, tw2, tid, NT);
-  plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, tw1, tid, NT);
-  dit<N2, 1, -1>(pl, rowsp, g1 + g2, tw2, tid, NT);
+  dif<N2, 1, +1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+  plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
+  dit<N2, 1, -1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
   for (int col = tid; col < g.ncols; col += NT) {
     const int ab = g.col_ab[col];
     Xrow[col] = pl[(ab >> 16) * P2 + (ab & 0xffff)];

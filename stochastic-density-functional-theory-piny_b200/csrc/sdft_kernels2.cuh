@@ -7,6 +7,9 @@
 
 namespace sdft {
 bool fast_supported(int n1, int n2, int n3);
+// twiddle tables of the compile-time FFT edges in constant memory, once per
+// device (call with the device current); nonzero on failure
+int init_const_twiddles();
 template <typename T>
 bool fast_stage_a(const DevGeom &g, const double *C, int nstate, int pair0, int npairs, void *X, cudaStream_t st);
 template <typename T>

@@ -83,7 +83,6 @@ __global__ void __launch_bounds__(kColThreads)
 kf_stage_a(DevGeom g, const double *__restrict__ C, int nstate, int pair0, typename CT<T>::type *__restrict__ X) {
   using C2 = typename CT<T>::type;
   constexpr int P3 = N3 + 1;
-  __shared__ __align__(16) C2 tw[N3];
   __shared__ __align__(16) C2 buf[2 * kCPB * P3];
   const int tid = threadIdx.x;
   const int cp0 = blockIdx.x * kCPB;
@@ -93,8 +92,6 @@ kf_stage_a(DevGeom g, const double *__restrict__ C, int nstate, int pair0, typen
   const int p = pair0 + blockIdx.y;
   const int s1 = 2 * p, s2 = 2 * p + 1;
   const bool has2 = s2 < nstate;
-  const C2 *twg = twp<T>(g, 3);
-  for (int t = tid; t < N3; t += kColThreads) tw[t] = twg[t];
   for (int i = tid; i < ncl * P3; i += kColThreads) buf[i] = cmk<C2>(0.0, 0.0);
   __syncthreads();
   const size_t o1 = (size_t)s1 * 2 * g.ngp, o2 = (size_t)s2 * 2 * g.ngp;
@@ -120,7 +117,7 @@ kf_stage_a(DevGeom g, const double *__restrict__ C, int nstate, int pair0, typen
     }
   }
   __syncthreads();
-  dif<N3, 1, +1>(buf, Lines1{P3}, ncl, tw, tid, kColThreads);
+  dif<N3, 1, +1>(buf, Lines1{P3}, ncl, TwC<N3, C2>{}, tid, kColThreads);
   C2 *Xp = X + (size_t)blockIdx.y * N3 * g.ncols_pad;
   for (int i = tid; i < N3 * ncl; i += kColThreads) {
     const int r = i / ncl, cl = i - r * ncl;
@@ -310,7 +307,6 @@ __global__ void __launch_bounds__(kColThreads, 4)
 kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   using C2 = typename CT<T>::type;
   constexpr int P3 = N3 + 1;
-  __shared__ __align__(16) C2 tw[N3];
   __shared__ __align__(16) C2 buf[2 * kCPB * P3];
   // packed OUT columns for the next step (e.Xnext; FP32 columns only: the
   // FP64 instance has no room for a second buffer in static shared memory)
@@ -325,8 +321,6 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   const int p = e.pair0 + blockIdx.y;
   const int s1 = 2 * p, s2 = 2 * p + 1;
   const bool has2 = s2 < e.nstate;
-  const C2 *twg = twp<T>(g, 3);
-  for (int t = tid; t < N3; t += kColThreads) tw[t] = twg[t];
   const C2 *Xp = X + (size_t)blockIdx.y * N3 * g.ncols_pad;
   for (int i = tid; i < N3 * ncl; i += kColThreads) {
     const int r = i / ncl, cl = i - r * ncl;
@@ -336,7 +330,7 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   if (pack)
     for (int i = tid; i < ncl * P3; i += kColThreads) nbuf[i] = cmk<C2>(0.0, 0.0);
   __syncthreads();
-  dit<N3, 1, -1>(buf, Lines1{P3}, ncl, tw, tid, kColThreads);
+  dit<N3, 1, -1>(buf, Lines1{P3}, ncl, TwC<N3, C2>{}, tid, kColThreads);
   Dots2 dt{0.0, 0.0, 0.0};
   double mx1 = 0.0, mx2 = 0.0;
   const int warp = tid >> 5, lane = tid & 31;
@@ -418,7 +412,7 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   }
   if (pack) {  // the next application's stage A: forward c-transform, store columns
     __syncthreads();
-    dif<N3, 1, +1>(nbuf, Lines1{P3}, ncl, tw, tid, kColThreads);
+    dif<N3, 1, +1>(nbuf, Lines1{P3}, ncl, TwC<N3, C2>{}, tid, kColThreads);
     C2 *Xn = reinterpret_cast<C2 *>(e.Xnext) + (size_t)blockIdx.y * N3 * g.ncols_pad;
     for (int i = tid; i < N3 * ncl; i += kColThreads) {
       const int r = i / ncl, cl = i - r * ncl;

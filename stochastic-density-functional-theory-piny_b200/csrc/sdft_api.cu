@@ -620,6 +620,25 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   g.gkc = ctx->d_gkc; g.ak2 = ctx->d_ak2;
   g.tw1 = ctx->d_tw; g.tw2 = ctx->d_tw + n1; g.tw3 = ctx->d_tw + n1 + n2;
   g.tw1f = ctx->d_twf; g.tw2f = ctx->d_twf + n1; g.tw3f = ctx->d_twf + n1 + n2;
+  // signed kb range of the sphere columns on each plane row a (a = ka mod n1),
+  // and whether every row's columns fill their range
+  {
+    std::vector<int2> rng(n1, make_int2(1, 0));
+    std::vector<int> cnt(n1, 0);
+    for (int ab : colab) {
+      const int a = ab >> 16, b = ab & 0xffff;
+      const int kb = b <= n2 / 2 ? b : b - n2;
+      if (cnt[a]++ == 0) rng[a] = make_int2(kb, kb);
+      else rng[a] = make_int2(std::min(rng[a].x, kb), std::max(rng[a].y, kb));
+    }
+    g.kb_contig = 1;
+    for (int a = 0; a < n1; a++)
+      if (cnt[a] && cnt[a] != rng[a].y - rng[a].x + 1) g.kb_contig = 0;
+    DMF(ctx->d_kb_rng, n1 * sizeof(int2));
+    CKF(cudaMemcpyAsync(ctx->d_kb_rng, rng.data(), n1 * sizeof(int2), cudaMemcpyHostToDevice, ctx->st));
+    CKF(cudaStreamSynchronize(ctx->st));  // (rng is a local)
+    g.kb_rng = ctx->d_kb_rng;
+  }
   // orbital blocks (zero padded)
   const size_t vb = ctx->vec_elems * sizeof(double);
   DMF(ctx->d_chi, vb);
@@ -651,7 +670,7 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_twf, ctx->d_vp, ctx->d_vks_tmp, ctx->d_pj, ctx->d_bk, ctx->d_w, ctx->d_z,
                   ctx->d_zwork, ctx->d_chi, ctx->d_b1, ctx->d_b2, ctx->d_fnl, ctx->d_acc, ctx->d_coef,
                   ctx->d_x, ctx->d_dots, ctx->d_mom, ctx->d_rho_part, ctx->d_rho, ctx->d_neg, ctx->d_noise_scratch,
-                  ctx->d_enl, ctx->d_red,
+                  ctx->d_enl, ctx->d_red, ctx->d_kb_rng,
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
                   ctx->d_oz_part};

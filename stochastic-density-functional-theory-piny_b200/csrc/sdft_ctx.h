@@ -54,6 +54,7 @@ struct sdft_ctx {
   std::vector<sdft_batch *> batches;  // graphs that replay this context's filter
   double *d_enl = nullptr;
   double *d_red = nullptr;  // reduction partials + scalars (Lanczos, energies)
+  int2 *d_kb_rng = nullptr;  // per plane row: signed kb range of its sphere columns
   // state
   int resident = 0;          // orbitals in d_chi
   int filtered = 0;          // orbitals with results in d_acc

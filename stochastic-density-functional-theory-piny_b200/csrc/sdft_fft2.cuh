@@ -151,9 +151,20 @@ struct UnitIter {
 template <typename C, typename P> __device__ __forceinline__ C tw_at(P *tw, int t) { return lds_tw(tw + t); }
 template <typename C, typename TW> __device__ __forceinline__ C tw_at(const TW &tw, int t) { return tw(t); }
 
+// Elements of a line that hold data (mask.line(l)(k) for natural index k of
+// line l): dif reads only those on input (the others count as zero and need
+// not be stored), dit writes only those on output.  AllElems: every element.
+struct AllK {
+  __device__ __forceinline__ bool operator()(int) const { return true; }
+};
+struct AllElems {
+  __device__ __forceinline__ AllK line(int) const { return AllK{}; }
+};
+
 // natural -> permuted.  twN: exp(-2 pi i t/N) (shared-memory table or accessor).
-template <int N, int ES, int DIR, typename C, typename LM, typename TW>
-__device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr) {
+template <int N, int ES, int DIR, typename C, typename LM, typename TW, typename MK = AllElems>
+__device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr,
+                                    const MK &mask = MK{}) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
   if (nl > 0) {
 #pragma unroll 1
@@ -162,8 +173,12 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN,
       if (!lm.valid(l)) continue;
       C *p = buf + lm.base(l);
       C v[R1];
+      const auto in = mask.line(l);
 #pragma unroll
-      for (int j1 = 0; j1 < R1; j1++) v[j1] = p[(j2 + R2 * j1) * ES];
+      for (int j1 = 0; j1 < R1; j1++) {
+        const int k = j2 + R2 * j1;
+        v[j1] = in(k) ? p[k * ES] : cmk<C>(0.0, 0.0);
+      }
       dftr<R1, DIR>(v);
       p[j2 * ES] = v[0];
 #pragma unroll
@@ -193,8 +208,9 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN,
 }
 
 // permuted -> natural
-template <int N, int ES, int DIR, typename C, typename LM, typename TW>
-__device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr) {
+template <int N, int ES, int DIR, typename C, typename LM, typename TW, typename MK = AllElems>
+__device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr,
+                                    const MK &mask = MK{}) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
   if (nl > 0) {
 #pragma unroll 1
@@ -226,8 +242,12 @@ __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN,
 #pragma unroll
       for (int k1 = 0; k1 < R1; k1++) v[k1] = p[(R2 * k1 + j2) * ES];
       dftr<R1, DIR>(v);
+      const auto out = mask.line(l);
 #pragma unroll
-      for (int j1 = 0; j1 < R1; j1++) p[(j2 + R2 * j1) * ES] = v[j1];
+      for (int j1 = 0; j1 < R1; j1++) {
+        const int k = j2 + R2 * j1;
+        if (out(k)) p[k * ES] = v[j1];
+      }
     }
   }
   __syncthreads();

@@ -18,6 +18,8 @@ struct DevGeom {
   int ngp;              // pitch of one re (or im) block of an orbital
   int ncols, ncols_pad, ncp, kamax;
   int nbatch;           // ceil(ncp / kCPB)
+  const int2 *kb_rng;   // [n1] per plane row a: signed kb range [x, y] of its sphere columns
+  int kb_contig;        // every row's columns fill its kb range (else kb_rng is not used)
   const int *cp_gstart; // [ncp] first G index of the pair's direct column
   const int *cp_gcount; // [ncp]
   const int *col_ab;    // [ncols] (ka mod n1) << 16 | (kb mod n2)

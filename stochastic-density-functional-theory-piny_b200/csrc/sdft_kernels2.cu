@@ -505,28 +505,48 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
   __syncthreads();
 }
 
+// Sphere rows of a plane as b-lines (Lines2P order): line l < g1 is row l,
+// line l >= g1 is row base2 + l - g1; element k of a line holds data when
+// its signed kb lies in the row's column range.
+template <int N2> struct RowKb {
+  const int2 *rng;
+  int g1, base2;
+  struct In {
+    int lo, hi;
+    __device__ __forceinline__ bool operator()(int k) const {
+      const int kb = k <= N2 / 2 ? k : k - N2;
+      return kb >= lo && kb <= hi;
+    }
+  };
+  __device__ __forceinline__ In line(int l) const {
+    const int2 r = rng[l < g1 ? l : base2 + (l - g1)];
+    return In{r.x, r.y};
+  }
+};
+
 template <typename T, int N1, int N2>
 __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
 kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict__ Vp) {
   using C2 = typename CT<T>::type;
   constexpr int NT = PlaneCfg<T>::NT, P2 = N2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2 *tw1 = reinterpret_cast<C2 *>(smem_raw);
-  C2 *tw2 = tw1 + N1;
-  C2 *pl = tw2 + N2;
+  // (the first N1 + N2 complex slots held twiddles before they moved to
+  // constant memory; the row kb ranges use the first N1 of them)
+  int2 *rng = reinterpret_cast<int2 *>(smem_raw);
+  C2 *pl = reinterpret_cast<C2 *>(smem_raw) + N1 + N2;
   const int tid = threadIdx.x;
   const int r = blockIdx.x;
-  {
-    const C2 *t1 = twp<T>(g, 1), *t2 = twp<T>(g, 2);
-    for (int t = tid; t < N1; t += NT) tw1[t] = t1[t];
-    for (int t = tid; t < N2; t += NT) tw2[t] = t2[t];
-  }
   const int ka = g.kamax;
-  const Lines2 rows{ka + 1, P2, (N1 - ka) * P2};
-  // zero only the 2 kamax + 1 rows inside the sphere's a-range
-  for (int i = tid; i < (2 * ka + 1) * N2; i += NT) {
-    const int l = i / N2, b = i - l * N2;
-    pl[rows.base(l) + b] = cmk<C2>(0.0, 0.0);
+  const bool contig = g.kb_contig != 0;
+  if (contig) {
+    for (int t = tid; t < N1; t += NT) rng[t] = g.kb_rng[t];
+  } else {
+    // zero the 2 kamax + 1 rows inside the sphere's a-range
+    const Lines2 rows{ka + 1, P2, (N1 - ka) * P2};
+    for (int i = tid; i < (2 * ka + 1) * N2; i += NT) {
+      const int l = i / N2, b = i - l * N2;
+      pl[rows.base(l) + b] = cmk<C2>(0.0, 0.0);
+    }
   }
   __syncthreads();
   C2 *Xrow = X + ((size_t)blockIdx.y * g.n3 + r) * g.ncols_pad;
@@ -538,9 +558,16 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
   // b-transforms over the sphere rows, each row group padded to 16 lanes
   const int g1 = (ka + 1 + 15) & ~15, g2 = (ka + 15) & ~15;
   const Lines2P rowsp{ka + 1, g1, ka, P2, (N1 - ka) * P2};
-  dif<N2, 1, +1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
-  plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
-  dit<N2, 1, -1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+  if (contig) {  // only the sphere's elements are read before and written after the b-transforms
+    const RowKb<N2> m{rng, g1, N1 - ka};
+    dif<N2, 1, +1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
+    plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
+    dit<N2, 1, -1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
+  } else {
+    dif<N2, 1, +1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+    plane_a_vmul<N1>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
+    dit<N2, 1, -1>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+  }
   for (int col = tid; col < g.ncols; col += NT) {
     const int ab = g.col_ab[col];
     Xrow[col] = pl[(ab >> 16) * P2 + (ab & 0xffff)];

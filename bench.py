@@ -138,11 +138,11 @@ def algorithmic(kind, s, nsto, csz):
 
 
 # DRAM bytes from ncu captures (profiles/): kf_stage_b<float,96,96> and
-# kf_stage_c<float,96,1> per orbital pair (136.5 + 75.2 MB and 294.2 +
+# kf_stage_c<float,96,1> per orbital pair (136.5 + 73.2 MB and 294.2 +
 # 301.1 MB for 64 pairs, scaled by pairs); the KB GEMMs
 # per launch at 512 orbitals (full-size capture, mean of the projection
 # 1.14 GB + 63.8 MB and the back projection 865.8 + 398.0 MB)
-PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 75.2e6) / 64,
+PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 73.2e6) / 64,
                     ("kf_stage_c", (96, 96, 96), True): (294.2e6 + 301.1e6) / 64}
 PROFILED_GEMM_TRAFFIC = {((96, 96, 96), True, 512): (1.14e9 + 63.8e6 + 865.8e6 + 398.0e6) / 2}
 

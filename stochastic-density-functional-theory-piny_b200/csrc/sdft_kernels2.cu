@@ -302,8 +302,10 @@ __device__ __forceinline__ void epilogue_pair_hot(const DevGeom &g, const EpiArg
   }
 }
 
+// 6 CTAs/SM (40 registers, some spilled): latency-bound, the extra resident
+// CTAs measured 4 % faster than 4 CTAs/SM at equal clocks
 template <typename T, int N3, bool HOT>
-__global__ void __launch_bounds__(kColThreads, 4)
+__global__ void __launch_bounds__(kColThreads, 6)
 kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   using C2 = typename CT<T>::type;
   constexpr int P3 = N3 + 1;

@@ -151,14 +151,15 @@ KERNEL_OF = {"stage_a_pack_cfft": "kf_stage_a", "stage_b_plane_fft_vks": "kf_sta
              "density_planes": "kf_stage_b_density"}
 
 
-def rooflines(timing, s, nsto, mixed):
+def rooflines(timing, s, nsto, mixed, back_products=10):
     """Roofline of every kernel function with an algorithmic model, largest
     total time first.  Tensor: the KB GEMMs (projection and back projection,
     one kernel) -- mixed: int8 tcgen05 ops (10 digit products per FP64-
     equivalent multiply-add) against 2 x the measured bf16 burst peak (B200's
     dense int8 rate is twice its bf16 rate); FP64: DMMA flops against the
     nominal 40 TFLOP/s FP64 tensor rate.  HBM: algorithmic bytes (algorithmic())
-    against the measured copy bandwidth."""
+    against the measured copy bandwidth.  back_products: int8 digit products
+    of the back projection (10, or 6 with the 24-bit digits of mixed_fast)."""
     pk, src = peaks()
     csz = 8 if mixed else 16
     agg = {}
@@ -167,12 +168,14 @@ def rooflines(timing, s, nsto, mixed):
         if kern is None or n == 0:
             continue
         bound, work = algorithmic(kind, s, nsto, csz)
-        a = agg.setdefault(kern, [bound, 0.0, 0, 0.0])
+        a = agg.setdefault(kern, [bound, 0.0, 0, 0.0, 0.0])
         a[1] += ms
         a[2] += n
         a[3] += work * n
+        if bound == "tensor":  # int8 products executed
+            a[4] += work * n * (back_products if kind == "kb_back_gemm" else 10)
     out = []
-    for kern, (bound, ms, n, work) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+    for kern, (bound, ms, n, work, ops8) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
         t = ms / 1e3
         if bound == "hbm":
             ach = work / t / 1e9
@@ -183,7 +186,7 @@ def rooflines(timing, s, nsto, mixed):
                         "peak_source": src, "ms_total": ms, "launches": n})
         else:
             if mixed:
-                ach = 10.0 * work / t / 1e12
+                ach = ops8 / t / 1e12
                 peak = 2.0 * pk["bf16_tflops"]
                 psrc = f"int8 dense = 2 x {src} bf16 burst ({pk['bf16_tflops']})"
                 name = "kb_gemm (k_gemm_oz8, int8 tcgen05)"
@@ -223,7 +226,7 @@ def run_ours(args):
     s["_P"] = 4 * s["natm"]
     nsto = cfg["nsto"] if args.nsto is None else args.nsto
     L = cfg["L"] if args.L is None else args.L
-    prec = pkg.SDFT_PREC_MIXED if args.prec == "mixed" else pkg.SDFT_PREC_FP64
+    prec = {"mixed": pkg.SDFT_PREC_MIXED, "mixed_fast": pkg.SDFT_PREC_MIXED_FAST, "fp64": pkg.SDFT_PREC_FP64}[args.prec]
     ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=nsto, device=local)
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
@@ -364,7 +367,7 @@ def run_ours(args):
 
     # ---- FP64 arm and accuracy of the mixed arm (rank 0 data)
     fp64 = None
-    if prec == pkg.SDFT_PREC_MIXED and not args.no_fp64:
+    if prec != pkg.SDFT_PREC_FP64 and not args.no_fp64:
         c64 = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=pkg.SDFT_PREC_FP64,
                           max_states=nsto, device=local)
         c64.set_vks(s["vks"])
@@ -426,7 +429,8 @@ def run_ours(args):
         c64.close()
 
     # ---- roofline: per kernel function, the dominant one first
-    roof_all = rooflines(timing, s, nsto, prec == pkg.SDFT_PREC_MIXED)
+    roof_all = rooflines(timing, s, nsto, prec != pkg.SDFT_PREC_FP64,
+                         back_products=6 if prec == pkg.SDFT_PREC_MIXED_FAST else 10)
     roof = roof_all[0] if roof_all else None
     kernel_table = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / max(1e-9, sum(x[0] for x in
                     timing.values()))} for k, v in timing.items() if v[1]}
@@ -439,7 +443,9 @@ def run_ours(args):
         "metric": "filtered stochastic orbitals/s (512-atom Si, mixed vs FP64 GPU); p50/p99 latency",
         "value": value, "unit": "orbitals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "mixed(fp32 fft, int8-ozaki kb gemm, fp64 recurrence)" if prec == pkg.SDFT_PREC_MIXED else "f64",
+        "dtype": ("mixed(fp32 fft, int8-ozaki kb gemm, fp64 recurrence)" if prec == pkg.SDFT_PREC_MIXED else
+                  "mixed_fast(fp32 fft, int8-ozaki kb gemm with 24-bit back projection, fp64 recurrence)"
+                  if prec == pkg.SDFT_PREC_MIXED_FAST else "f64"),
         "data": "synthetic (seeded Si supercell, Gaussian V_loc, Gaussian s+p KB, +-1 noise)",
         "config": {"workload": f"{args.config}: {s['natm']}-atom Si, grid {s['grid'][0]}x{s['grid'][1]}x{s['grid'][2]}, "
                                f"{nsto} orbitals/GPU, Chebyshev L={L}, ncoef={s['ncoef']}, P={s['_P']}",
@@ -600,7 +606,7 @@ def run_batch(args):
     pkg = g.load_package()
     wl = g.load_workload()
     serve, tuner_mod = _modules(pkg)
-    prec = pkg.SDFT_PREC_MIXED if args.prec == "mixed" else pkg.SDFT_PREC_FP64
+    prec = {"mixed": pkg.SDFT_PREC_MIXED, "mixed_fast": pkg.SDFT_PREC_MIXED_FAST, "fp64": pkg.SDFT_PREC_FP64}[args.prec]
     specs = wl.batch_specs()
     t0 = time.time()
     tuner = tuner_mod.Tuner(pkg)
@@ -754,7 +760,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg3")
-    ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--prec", default="mixed", choices=["mixed", "mixed_fast", "fp64"])
     ap.add_argument("--nsto", type=int, default=None)
     ap.add_argument("--L", type=int, default=None)
     ap.add_argument("--cpu-steps", type=int, default=2)

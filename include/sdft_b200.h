@@ -54,6 +54,11 @@ extern "C" {
                                   (about 28-bit operands, exact products and
                                   sums), FP64 recurrence / accumulators /
                                   reductions */
+#define SDFT_PREC_MIXED_FAST 2 /* as MIXED, but the back projection (whose
+                                  result is stored in FP32) multiplies
+                                  24-bit digits (3 x 8 bits, 6 products
+                                  instead of 10): about 8 % faster at 512
+                                  atoms, force error ~2e-7 instead of ~2e-8 */
 
 typedef struct sdft_ctx sdft_ctx;
 

@@ -40,6 +40,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libsdft_b200.so")
 
 SDFT_PREC_FP64 = 0
 SDFT_PREC_MIXED = 1
+SDFT_PREC_MIXED_FAST = 2
 
 _ERRNAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "UNSUPPORTED", 6: "NODEVICE", 7: "TIMEOUT"}
 

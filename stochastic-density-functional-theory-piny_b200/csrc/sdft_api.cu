@@ -253,7 +253,7 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
     // also zeroes d_rowmax[0, nstate) for the next stage C (the slice above
     // has consumed it)
     launch_oz_reduce_slice(ctx->d_oz_part, split, stride, Ppad, ctx->P, nstate, ctx->d_z, ctx->d_z_dig,
-                           (size_t)S * Ppad, ctx->d_z_sc, ctx->d_rowmax, ctx->st);
+                           (size_t)S * Ppad, ctx->d_z_sc, ctx->d_rowmax, ctx->st, ctx->om2.fmt);
     ctx->launches += 2;
     ctx->rowmax_zero_n = nstate;
     ctx->omax_vec = nullptr;
@@ -538,7 +538,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   if (!edge_ok(n1) || !edge_ok(n2) || !edge_ok(n3))
     return set_error(SDFT_ERR_UNSUPPORTED, "FFT edges must be 2^a 3^b in [2,128]");
   if (ncoef < 2 || max_states < 1) return set_error(SDFT_ERR_ARG, "ctx_create: ncoef/max_states");
-  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED)
+  if (precision != SDFT_PREC_FP64 && precision != SDFT_PREC_MIXED && precision != SDFT_PREC_MIXED_FAST)
     return set_error(SDFT_ERR_ARG, "ctx_create: precision");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(SDFT_ERR_NODEVICE, "no CUDA device");

@@ -16,7 +16,10 @@
 //             acc3, one conversion to FP64 (exact: |value| < 2^53 for K
 //             ranges below 2^20), scaling by 2^(Ea+Eb-33), coalesced store.
 // int32 accumulation cannot overflow while (K range) * 4 * 64^2 < 2^31,
-// i.e. K ranges up to 131072 (checked on the host).
+// i.e. K ranges up to 131072 (checked on the host).  The OZ_8x3 instance
+// (3 slices, 6 products, the unsigned lower digits multiplied as u8) has
+// three accumulators, four pipeline stages of 48 KB, and K ranges up to
+// 16384.
 // All mbarrier waits are bounded (sdft_tc_common.cuh).  No TMA multicast.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -28,18 +31,28 @@
 
 namespace sdft {
 
-constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 64, OZ_STAGES = 3;
-constexpr int OZ_MAX_KRANGE = 131072;
+constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 64;
 
-struct OzSmem {
+// per digit format: slices, digit bits, pipeline stages, K range limit and
+// the power of two that turns the combined accumulators into the product
+template <int FMT> struct OzF;
+template <> struct OzF<OZ_7x4> {
+  static constexpr int NS = 4, BITS = 7, STAGES = 3, MAX_KRANGE = 131072, SCALE_EXP = -33;
+};
+template <> struct OzF<OZ_8x3> {
+  static constexpr int NS = 3, BITS = 8, STAGES = 4, MAX_KRANGE = 16384, SCALE_EXP = -30;
+};
+
+template <int FMT> struct OzSmem {
+  static constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES;
   static constexpr int A_SLICE = OZ_BM * OZ_BK;          // 8 KB
   static constexpr int B_SLICE = OZ_BN * OZ_BK;          // 8 KB
-  static constexpr int A_BYTES = kOzSlices * A_SLICE;    // 32 KB
-  static constexpr int B_BYTES = kOzSlices * B_SLICE;    // 32 KB
-  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 64 KB
+  static constexpr int A_BYTES = NS * A_SLICE;
+  static constexpr int B_BYTES = NS * B_SLICE;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 64 KB (7x4) or 48 KB (8x3)
   static constexpr int BAR_OFF = OZ_STAGES * STAGE_BYTES;
   static constexpr int TOTAL = BAR_OFF + 8 * (2 * OZ_STAGES + 1) + 16 + 1024;  // + alignment slack
-  static constexpr int TMEM_COLS = 4 * OZ_BN;                                   // 512
+  static constexpr int TMEM_COLS = 512;                                         // NS accumulators of OZ_BN
 };
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
@@ -52,12 +65,13 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, 
 constexpr int OZ_EPI_WARPS = 8;                 // two per TMEM lane quadrant
 constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
 
-template <typename OutT>
+template <typename OutT, int FMT>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int ktiles_total,
            int ktiles_per_split, const double *__restrict__ sa, const double *__restrict__ sb,
            OutT *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
-  using S = OzSmem;
+  using S = OzSmem<FMT>;
+  constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES, BITS = OzF<FMT>::BITS;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_u32(smem);
@@ -104,9 +118,9 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      // D = S32, A = B = signed 8-bit, K-major, N = 128, M = 128
-      constexpr uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
-                                 ((uint32_t)(OZ_BM >> 4) << 24);
+      // D = S32, A / B = signed (1) or unsigned (0) 8-bit, K-major, N = 128, M = 128;
+      // OZ_8x3: digit 0 signed, digits 1 and 2 unsigned
+      constexpr uint32_t idesc0 = (2u << 4) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
       uint32_t started = 0;  // bit q: accumulator q holds data
       for (int it = 0; it < nkt; it++) {
         const int s = it % OZ_STAGES;
@@ -116,10 +130,12 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
 #pragma unroll
         for (int ks = 0; ks < OZ_BK / 32; ks++) {
 #pragma unroll
-          for (int sa_ = 0; sa_ < kOzSlices; sa_++) {
+          for (int sa_ = 0; sa_ < NS; sa_++) {
 #pragma unroll
-            for (int tb = 0; tb + sa_ < kOzSlices; tb++) {
+            for (int tb = 0; tb + sa_ < NS; tb++) {
               const int q = sa_ + tb;
+              const bool as = FMT == OZ_7x4 || sa_ == 0, bs = FMT == OZ_7x4 || tb == 0;
+              const uint32_t idesc = idesc0 | (as ? 1u << 7 : 0u) | (bs ? 1u << 10 : 0u);
               const uint64_t ad = smem_desc<64>(st + sa_ * S::A_SLICE + ks * 32);
               const uint64_t bd = smem_desc<64>(st + S::A_BYTES + tb * S::B_SLICE + ks * 32);
               mma_i8(tmem + (uint32_t)(q * OZ_BN), ad, bd, idesc, (started >> q) & 1u);
@@ -138,7 +154,7 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int m = m0 + 32 * qd + lane;
     const bool row_ok = ok && m < Mst && nkt > 0;
-    const double fa = row_ok ? sa[m] * 0x1p-33 : 0.0;
+    const double fa = row_ok ? ldexp(sa[m], OzF<FMT>::SCALE_EXP) : 0.0;
     const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
     constexpr int CH = OZ_BN / 16 / 2;  // 16-column chunks per epilogue warp
 #pragma unroll 1
@@ -147,15 +163,19 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
       tmem_ld16(tl + 0 * OZ_BN + c * 16, r0);
       tmem_ld16(tl + 1 * OZ_BN + c * 16, r1);
       tmem_ld16(tl + 2 * OZ_BN + c * 16, r2);
-      tmem_ld16(tl + 3 * OZ_BN + c * 16, r3);
+      if constexpr (NS == 4) tmem_ld16(tl + 3 * OZ_BN + c * 16, r3);
       tmem_ld_wait();
       if (!(ok && m < Mst)) continue;
 #pragma unroll
       for (int j = 0; j < 16; j++) {
         const int n = n0 + c * 16 + j;
         if (n < Nst) {
-          const long long v = ((long long)(int)r0[j] << 21) + ((long long)(int)r1[j] << 14) +
-                              ((long long)(int)r2[j] << 7) + (long long)(int)r3[j];
+          long long v;
+          if constexpr (NS == 4)
+            v = ((long long)(int)r0[j] << (3 * BITS)) + ((long long)(int)r1[j] << (2 * BITS)) +
+                ((long long)(int)r2[j] << BITS) + (long long)(int)r3[j];
+          else
+            v = ((long long)(int)r0[j] << (2 * BITS)) + ((long long)(int)r1[j] << BITS) + (long long)(int)r2[j];
           out[(size_t)blockIdx.z * split_stride + (size_t)n * ldo + m] = (OutT)(row_ok ? (double)v * fa * sb[n] : 0.0);
         }
       }
@@ -199,16 +219,19 @@ __device__ __forceinline__ int row_exponent(unsigned long long maxbits) {
   return max(-1000, max(field, 1) - 1022);
 }
 
-// four digits of x * 2^(6-E) (|.| < 64), each a round-to-nearest integer
-// of the running remainder times 2^7; all steps exact in FP64.
-__device__ __forceinline__ void digits4(double r, int *d) {
+// Digits of one value, all steps exact in FP64.  OZ_7x4: four round-to-
+// nearest digits of x 2^(6-E) (|.| < 64), the remainder times 2^7 each
+// step.  OZ_8x3: floor(x 2^(7-E)) in [-128, 127], then two floors of the
+// remainder (in [0, 1)) times 2^8, in [0, 255].
+template <int FMT> __device__ __forceinline__ void digits_of(double r, int *d) {
 #pragma unroll
-  for (int s = 0; s < kOzSlices; s++) {
-    const double q = rint(r);
+  for (int s = 0; s < OzF<FMT>::NS; s++) {
+    const double q = FMT == OZ_7x4 ? rint(r) : floor(r);
     d[s] = (int)q;
-    r = (r - q) * 128.0;
+    r = (r - q) * (FMT == OZ_7x4 ? 128.0 : 256.0);
   }
 }
+template <int FMT> constexpr int kTopShift = FMT == OZ_7x4 ? 6 : 7;  // x 2^(shift - E) is the top digit's value
 
 __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
   return (uint32_t)(a & 0xff) | ((uint32_t)(b & 0xff) << 8) | ((uint32_t)(c & 0xff) << 16) |
@@ -217,9 +240,11 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 
 // digits of rows x cols doubles; 4 consecutive columns per thread, zero
 // digits for cols <= k < ld.
+template <int FMT>
 __global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, int cols,
                              const unsigned long long *__restrict__ rowmax, int8_t *__restrict__ dig, int ld,
                              size_t sstride, double *__restrict__ scale) {
+  constexpr int NS = OzF<FMT>::NS;
   const int g4 = ld >> 2;
   const size_t tot = (size_t)rows * g4;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
@@ -227,16 +252,16 @@ __global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, in
     const unsigned long long mb = rowmax[row];
     const bool bad = mb >= 0x7ff0000000000000ull;
     const int E = bad ? 0 : row_exponent(mb);
-    const double p = ldexp(1.0, 6 - E);
-    int d[4][kOzSlices];
+    const double p = ldexp(1.0, kTopShift<FMT> - E);
+    int d[4][NS];
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const int c = c4 + e;
       const double v = (c < cols && !bad) ? x[(size_t)row * ldx + c] : 0.0;
-      digits4(v * p, d[e]);
+      digits_of<FMT>(v * p, d[e]);
     }
 #pragma unroll
-    for (int s = 0; s < kOzSlices; s++)
+    for (int s = 0; s < NS; s++)
       *(uint32_t *)(dig + s * sstride + (size_t)row * ld + c4) = pack4(d[0][s], d[1][s], d[2][s], d[3][s]);
     if (c4 == 0) scale[row] = bad ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, E);
   }
@@ -244,9 +269,11 @@ __global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, in
 
 // Sum of split-K partials for one row per CTA, then the digit form of the
 // row (second sweep over the just-written row, which is L2 resident).
+template <int FMT>
 __global__ void k_reduce_slice(const double *__restrict__ part, int split, size_t stride, int ldo, int Mst,
                                double *__restrict__ out, int8_t *__restrict__ dig, size_t dig_stride,
                                double *__restrict__ scale, unsigned long long *__restrict__ zero_rowmax) {
+  constexpr int NS = OzF<FMT>::NS;
   const int n = blockIdx.x;
   if (zero_rowmax && threadIdx.x == 0) zero_rowmax[n] = 0ull;
   double mx = 0.0;
@@ -269,13 +296,13 @@ __global__ void k_reduce_slice(const double *__restrict__ part, int split, size_
   __syncthreads();
   const bool bad = mbits >= 0x7ff0000000000000ull;
   const int E = bad ? 0 : row_exponent(mbits);
-  const double p = ldexp(1.0, 6 - E);
+  const double p = ldexp(1.0, kTopShift<FMT> - E);
   for (int m4 = threadIdx.x * 4; m4 < ldo; m4 += blockDim.x * 4) {
-    int d[4][kOzSlices];
+    int d[4][NS];
 #pragma unroll
-    for (int e = 0; e < 4; e++) digits4(bad ? 0.0 : out[(size_t)n * ldo + m4 + e] * p, d[e]);
+    for (int e = 0; e < 4; e++) digits_of<FMT>(bad ? 0.0 : out[(size_t)n * ldo + m4 + e] * p, d[e]);
 #pragma unroll
-    for (int s = 0; s < kOzSlices; s++)
+    for (int s = 0; s < NS; s++)
       *(uint32_t *)(dig + s * dig_stride + (size_t)n * ldo + m4) = pack4(d[0][s], d[1][s], d[2][s], d[3][s]);
   }
   if (threadIdx.x == 0) scale[n] = bad ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, E);
@@ -305,13 +332,14 @@ static PFN_encodeTiledOz get_encode_oz() {
 
 bool gemm_oz_available() { return get_encode_oz() != nullptr; }
 
-int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld) {
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt) {
   PFN_encodeTiledOz enc = get_encode_oz();
   if (!enc) return set_error(SDFT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   if (((uintptr_t)dig & 15) || ld % OZ_BK || rows % 128) return set_error(SDFT_ERR_ARG, "oz tensor map alignment");
-  cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)kOzSlices};
+  const int ns = oz_slices(fmt);
+  cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)ns};
   cuuint64_t strides[2] = {(cuuint64_t)ld, (cuuint64_t)ld * rows};
-  cuuint32_t box[3] = {(cuuint32_t)OZ_BK, 128u, (cuuint32_t)kOzSlices};
+  cuuint32_t box[3] = {(cuuint32_t)OZ_BK, 128u, (cuuint32_t)ns};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void *)dig, dims, strides, box, es,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -330,7 +358,7 @@ int oz_choose_split(int tiles, int ktiles, int max_split) {
   const int lim = max_split < 1 ? 1 : max_split;
   for (int s = 1; s <= lim && s <= ktiles; s++) {
     const int kps = (ktiles + s - 1) / s;
-    if (kps * OZ_BK > OZ_MAX_KRANGE) continue;
+    if (kps * OZ_BK > OzF<OZ_7x4>::MAX_KRANGE) continue;
     const int se = (ktiles + kps - 1) / kps;
     const int waves = (tiles * se + nsm - 1) / nsm;
     const double cost = (double)waves * kps + (se > 1 ? 8.0 * se * tiles / nsm : 0.0);
@@ -339,29 +367,35 @@ int oz_choose_split(int tiles, int ktiles, int max_split) {
   return best;
 }
 
-template <typename OutT>
+template <typename OutT, int FMT>
 static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_stride, int *err, cudaStream_t st) {
+  using S = OzSmem<FMT>;
   const int ktiles = (g.K + OZ_BK - 1) / OZ_BK;
   if (g.M % OZ_BM || g.N % OZ_BN || ktiles < 1) return set_error(SDFT_ERR_ARG, "oz gemm: shape");
   if (split < 1) split = 1;
   if (split > ktiles) split = ktiles;
-  const int kps = (ktiles + split - 1) / split;
-  if (kps * OZ_BK > OZ_MAX_KRANGE) return set_error(SDFT_ERR_ARG, "oz gemm: K range per CTA too long");
+  int kps = (ktiles + split - 1) / split;
+  if (kps * OZ_BK > OzF<FMT>::MAX_KRANGE) {
+    if (split_stride == 0) return set_error(SDFT_ERR_ARG, "oz gemm: K range per CTA too long");
+    kps = OzF<FMT>::MAX_KRANGE / OZ_BK;
+  }
   split = (ktiles + kps - 1) / kps;
   static const bool attr_once =
-      (cudaFuncSetAttribute(k_gemm_oz8<OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, OzSmem::TOTAL), true);
+      (cudaFuncSetAttribute(k_gemm_oz8<OutT, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL), true);
   (void)attr_once;
   dim3 grid(g.N / OZ_BN, g.M / OZ_BM, split);
-  k_gemm_oz8<OutT><<<grid, OZ_THREADS, OzSmem::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride, g.ldo,
-                                                       g.Mst, g.Nst, err);
+  k_gemm_oz8<OutT, FMT><<<grid, OZ_THREADS, S::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride,
+                                                            g.ldo, g.Mst, g.Nst, err);
   return SDFT_OK;
 }
 
 int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st) {
-  return run_gemm_oz_t<double>(g, split, out, split_stride, err, st);
+  return g.fmt == OZ_8x3 ? run_gemm_oz_t<double, OZ_8x3>(g, split, out, split_stride, err, st)
+                         : run_gemm_oz_t<double, OZ_7x4>(g, split, out, split_stride, err, st);
 }
 int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st) {
-  return run_gemm_oz_t<float>(g, split, out, split_stride, err, st);
+  return g.fmt == OZ_8x3 ? run_gemm_oz_t<float, OZ_8x3>(g, split, out, split_stride, err, st)
+                         : run_gemm_oz_t<float, OZ_7x4>(g, split, out, split_stride, err, st);
 }
 
 void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {
@@ -373,23 +407,31 @@ void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned lon
 }
 
 void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
-                     int ld, size_t slice_stride, double *scale, cudaStream_t st) {
+                     int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt) {
   const size_t tot = (size_t)rows * (ld / 4);
   int blocks = (int)((tot + 255) / 256);
   if (blocks > 148 * 32) blocks = 148 * 32;
-  k_slice_rows<<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
+  if (fmt == OZ_8x3)
+    k_slice_rows<OZ_8x3><<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
+  else
+    k_slice_rows<OZ_7x4><<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
 }
 
 void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
-                          int ld, size_t slice_stride, double *scale, cudaStream_t st) {
+                          int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt) {
   launch_oz_rowmax(x, ldx, rows, cols, rowmax, st);
-  launch_oz_slice(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale, st);
+  launch_oz_slice(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale, st, fmt);
 }
 
 void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
                             int8_t *dig, size_t dig_stride, double *scale, unsigned long long *zero_rowmax,
-                            cudaStream_t st) {
-  k_reduce_slice<<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale, zero_rowmax);
+                            cudaStream_t st, int fmt) {
+  if (fmt == OZ_8x3)
+    k_reduce_slice<OZ_8x3><<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale,
+                                                 zero_rowmax);
+  else
+    k_reduce_slice<OZ_7x4><<<Nst, 256, 0, st>>>(part, split, stride, ldo, Mst, out, dig, dig_stride, scale,
+                                                 zero_rowmax);
 }
 
 }  // namespace sdft

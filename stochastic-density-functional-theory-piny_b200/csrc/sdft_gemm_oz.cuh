@@ -18,23 +18,34 @@ namespace sdft {
 // dig[s*rows*ld + row*ld + k], ld a multiple of 64, zero for k >= K.
 constexpr int kOzSlices = 4;
 
-// out[n*ldo + m] = sum_k A[m][k] B[n][k] over the digit products with
-// s + t <= 3 (10 of the 16; the rest lie below 2^-28 of the leading term).
-// Every product is an exact int8 x int8 -> int32 tensor-core MMA; the four
-// digit orders are accumulated exactly in four TMEM accumulators and
-// combined exactly in 64-bit integers, so a K range contributes
-// an exactly representable FP64 value and the only rounding is the
-// FP64 sum of split-K partials.  A: M x K (M multiple of 128), B: N x K
+// Digit formats.  OZ_7x4 (above): 4 signed 7-bit digits, 28 bits.  OZ_8x3:
+// 3 digits of 8 bits, the first signed (floor of x 2^(7-E), in [-128, 127])
+// and two unsigned (floor of the remainder times 2^8, in [0, 255]),
+//     x ~= 2^E * 2^-23 * (d0 2^16 + d1 2^8 + d2),
+// truncation below 2^-23 of the row's scale; products with s + t <= 2
+// (6 of 9), int32 accumulation exact for K ranges up to 16384.  Used where
+// the result is stored in FP32 (the back projection).
+enum OzFmt : int { OZ_7x4 = 0, OZ_8x3 = 1 };
+__host__ __device__ constexpr int oz_slices(int fmt) { return fmt == OZ_8x3 ? 3 : 4; }
+
+// out[n*ldo + m] = sum_k A[m][k] B[n][k] over the digit products of the
+// format (OZ_7x4: s + t <= 3, 10 of the 16; the rest lie below 2^-28 of
+// the leading term).  Every product is an exact int8 x int8 -> int32
+// tensor-core MMA; the digit orders are accumulated exactly in TMEM
+// accumulators and combined exactly in 64-bit integers, so a K range
+// contributes an exactly representable FP64 value and the only rounding is
+// the FP64 sum of split-K partials.  A: M x K (M multiple of 128), B: N x K
 // (N multiple of 128); only m < Mst, n < Nst are stored.
 struct OzGemm {
   CUtensorMap tA, tB;
   int M, N, K, ldo, Mst, Nst;
   const double *sa, *sb;  // row scales 2^E of A (M) and B (N)
+  int fmt = OZ_7x4;       // digit format of both operands
 };
 
 bool gemm_oz_available();
-// tensor map of a digit array [kOzSlices][rows][ld] (int8, K-major)
-int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld);
+// tensor map of a digit array [oz_slices(fmt)][rows][ld] (int8, K-major)
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt = OZ_7x4);
 // split == 1: out = result; split > 1: FP64 partial z at out + z*split_stride.
 int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st);
 // the same with FP32 output (rounded once from the exact FP64 tile value)
@@ -46,15 +57,15 @@ void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned lon
 // digits (row pitch ld, slice pitch slice_stride bytes) + scales of rows x
 // cols doubles under the row maxima in rowmax
 void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
-                     int ld, size_t slice_stride, double *scale, cudaStream_t st);
+                     int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt = OZ_7x4);
 // both of the above
 void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,
-                          int ld, size_t slice_stride, double *scale, cudaStream_t st);
+                          int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt = OZ_7x4);
 // out[n*ldo+m] = sum_z part[z*stride + n*ldo + m] (m < Mst, else 0) for
 // n < Nst, plus the digit form of each row n (ld = ldo, slice pitch
 // dig_stride bytes).  zero_rowmax (nullable): words [0, Nst) set to 0.
 void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ldo, int Mst, int Nst, double *out,
                             int8_t *dig, size_t dig_stride, double *scale, unsigned long long *zero_rowmax,
-                            cudaStream_t st);
+                            cudaStream_t st, int fmt = OZ_7x4);
 
 }  // namespace sdft

@@ -285,15 +285,19 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->P = P;
   ctx->Ppad = Ppad;
   ctx->Mpad2 = Mpad2;
-  if (ctx->prec == SDFT_PREC_MIXED && gemm_oz_available()) {
+  if ((ctx->prec == SDFT_PREC_MIXED || ctx->prec == SDFT_PREC_MIXED_FAST) && gemm_oz_available()) {
     // digit form of the projector matrices for the INT8 tensor-core GEMMs
     const int S = (ctx->max_states + 127) / 128 * 128;
     const int Kp = (K1 + 63) / 64 * 64;
     ctx->s_oz = S;
     ctx->kp_oz = Kp;
     int r;
-    const size_t pjd = (size_t)kOzSlices * Ppad * Kp, bkd = (size_t)kOzSlices * Mpad2 * Ppad;
-    const size_t cd = (size_t)kOzSlices * S * Kp, zd = (size_t)kOzSlices * S * Ppad;
+    // the projection (FP64 partials, FP64 Z) uses the 28-bit digits; the back
+    // projection (FP32 result) the 24-bit ones in SDFT_PREC_MIXED_FAST (K =
+    // Ppad; that format accumulates K ranges up to 16384 exactly)
+    const int f2 = (ctx->prec == SDFT_PREC_MIXED_FAST && Ppad <= 16384) ? OZ_8x3 : OZ_7x4;
+    const size_t pjd = (size_t)kOzSlices * Ppad * Kp, bkd = (size_t)oz_slices(f2) * Mpad2 * Ppad;
+    const size_t cd = (size_t)kOzSlices * S * Kp, zd = (size_t)oz_slices(f2) * S * Ppad;
     const int maxrows = std::max(std::max(Ppad, Mpad2), S);
     ctx->oz_part_elems = (size_t)32 * S * Ppad;
     if ((r = dmalloc(ctx, (void **)&ctx->d_pj_dig, pjd)) || (r = dmalloc(ctx, (void **)&ctx->d_bk_dig, bkd)) ||
@@ -314,18 +318,21 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     launch_oz_slice_rows(ctx->d_pj, K1, Ppad, K1, ctx->d_rowmax, ctx->d_pj_dig, Kp, (size_t)Ppad * Kp, ctx->d_pj_sc,
                          ctx->st);
     launch_oz_slice_rows(ctx->d_bk, Ppad, Mpad2, Ppad, ctx->d_rowmax, ctx->d_bk_dig, Ppad, (size_t)Mpad2 * Ppad,
-                         ctx->d_bk_sc, ctx->st);
+                         ctx->d_bk_sc, ctx->st, f2);
     ctx->launches += 4;
     CKB(cudaGetLastError());
     CKB(cudaStreamSynchronize(ctx->st));
     OzGemm &g1 = ctx->om1, &g2 = ctx->om2;
     if ((r = make_tmap_oz(&g1.tA, ctx->d_pj_dig, Ppad, Kp)) || (r = make_tmap_oz(&g1.tB, ctx->d_c_dig, S, Kp)) ||
-        (r = make_tmap_oz(&g2.tA, ctx->d_bk_dig, Mpad2, Ppad)) || (r = make_tmap_oz(&g2.tB, ctx->d_z_dig, S, Ppad))) {
+        (r = make_tmap_oz(&g2.tA, ctx->d_bk_dig, Mpad2, Ppad, f2)) ||
+        (r = make_tmap_oz(&g2.tB, ctx->d_z_dig, S, Ppad, f2))) {
       rc = r;
       goto done;
     }
     g1.M = Ppad; g1.K = Kp; g1.ldo = Ppad; g1.Mst = P; g1.sa = ctx->d_pj_sc; g1.sb = ctx->d_c_sc;
     g2.M = Mpad2; g2.K = Ppad; g2.ldo = K1; g2.Mst = K1; g2.sa = ctx->d_bk_sc; g2.sb = ctx->d_z_sc;
+    g1.fmt = OZ_7x4;
+    g2.fmt = f2;
     // the FP64 projector copies are not used by the mixed path
     dev_free(ctx->d_pj, ctx->st); ctx->d_pj = nullptr;
     dev_free(ctx->d_bk, ctx->st); ctx->d_bk = nullptr;

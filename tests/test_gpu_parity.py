@@ -241,6 +241,23 @@ def test_mixed_hpsi_tensor_core(pkg, which, ns, request):
     c.close()
 
 
+@pytest.mark.parametrize("which,ns", [("sys1", 5), ("sys2", 130)])
+def test_mixed_fast_hpsi(pkg, which, ns, request):
+    """SDFT_PREC_MIXED_FAST: the back projection on 24-bit digits (3 x 8 bits,
+    6 products) -- the force error grows to a few 1e-7, the nonlocal energy
+    (from the 28-bit projection) is unchanged."""
+    s = request.getfixturevalue(which)
+    c = _ctx(pkg, s, ns, prec=pkg.SDFT_PREC_MIXED_FAST)
+    o = O.OracleSys(s)
+    cr, ci = _rand(s["ncoef"], ns, 17)
+    fr, fi, e = c.calc_coef_force(cr, ci, want_enl=True)
+    orr, oi, oe = o.hpsi(cr, ci, want_enl=True)
+    assert rel_l2(np.concatenate([fr, fi]), np.concatenate([orr, oi])) < 6e-7
+    assert abs(e - oe) < 1e-6 * abs(oe)
+    c.sync()
+    c.close()
+
+
 def test_mixed_newton_and_moments_close_to_fp64(pkg, sys1):
     """Mixed-precision Newton filter (in-place recurrence, paired accumulation,
     fused packing of the next step) and Chebyshev moments against FP64."""

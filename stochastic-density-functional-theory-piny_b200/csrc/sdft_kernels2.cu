@@ -331,6 +331,16 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   const bool pack = kCanPack && e.Xnext != nullptr;
   if (pack)
     for (int i = tid; i < ncl * P3; i += kColThreads) nbuf[i] = cmk<C2>(0.0, 0.0);
+  // hot instance: first item (point) of each column pair in the CTA's item list
+  __shared__ int pref[kCPB + 1];
+  if (HOT && tid == 0) {
+    int s = 0;
+    for (int k = 0; k < cp1 - cp0; k++) {
+      pref[k] = s;
+      s += g.cp_gcount[cp0 + k] + (cp0 + k == g.ncp - 1 ? 1 : 0);
+    }
+    pref[cp1 - cp0] = s;
+  }
   __syncthreads();
   dit<N3, 1, -1>(buf, Lines1{P3}, ncl, TwC<N3, C2>{}, tid, kColThreads);
   Dots2 dt{0.0, 0.0, 0.0};
@@ -338,13 +348,13 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   const int warp = tid >> 5, lane = tid & 31;
   const double invN = e.invN;
   const bool noise = !HOT && (e.mode == EPI_NOISE);
-  for (int cp = cp0 + warp; cp < cp1; cp += kColThreads / 32) {
+  // one point en of column pair cp
+  auto item = [&](int cp, int en) {
     const int lc = 2 * (cp - cp0);
     const bool zc = (cp == g.ncp - 1);
     const int lm = zc ? lc : lc + 1;
     const int gs = g.cp_gstart[cp], gc = g.cp_gcount[cp];
-    const int ntot = gc + (zc ? 1 : 0);
-    for (int en = lane; en < ntot; en += 32) {
+    {
       if (en < gc) {
         const int gi = gs + en;
         const int kc = g.gkc[gi];
@@ -390,6 +400,19 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
         }
         if (pack) nbuf[lc * P3] = cmk<C2>(ar, cr2);
       }
+    }
+  };
+  if constexpr (HOT) {  // the CTA's points dealt out over all threads
+    const int tot = pref[cp1 - cp0];
+    for (int it = tid; it < tot; it += kColThreads) {
+      int k = 0;
+      while (k + 1 < cp1 - cp0 && it >= pref[k + 1]) k++;
+      item(cp0 + k, it - pref[k]);
+    }
+  } else {  // a warp per column pair, lanes over its points
+    for (int cp = cp0 + warp; cp < cp1; cp += kColThreads / 32) {
+      const int ntot = g.cp_gcount[cp] + (cp == g.ncp - 1 ? 1 : 0);
+      for (int en = lane; en < ntot; en += 32) item(cp, en);
     }
   }
   if (e.omax) {

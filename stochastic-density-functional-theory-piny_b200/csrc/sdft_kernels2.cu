@@ -333,9 +333,9 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
   const bool pack = kCanPack && e.Xnext != nullptr;
   if (pack)
     for (int i = tid; i < ncl * P3; i += kCThreads) nbuf[i] = cmk<C2>(0.0, 0.0);
-  // hot instance: first item (point) of each column pair in the CTA's item list
+  // first item (point) of each column pair in the CTA's item list
   __shared__ int pref[kCPB + 1];
-  if (HOT && tid == 0) {
+  if (tid == 0) {
     int s = 0;
     for (int k = 0; k < cp1 - cp0; k++) {
       pref[k] = s;
@@ -404,17 +404,12 @@ kf_stage_c(DevGeom g, const typename CT<T>::type *X, EpiArgs e) {
       }
     }
   };
-  if constexpr (HOT) {  // the CTA's points dealt out over all threads
+  {  // the CTA's points dealt out over all threads
     const int tot = pref[cp1 - cp0];
     for (int it = tid; it < tot; it += kCThreads) {
       int k = 0;
       while (k + 1 < cp1 - cp0 && it >= pref[k + 1]) k++;
       item(cp0 + k, it - pref[k]);
-    }
-  } else {  // a warp per column pair, lanes over its points
-    for (int cp = cp0 + warp; cp < cp1; cp += kCThreads / 32) {
-      const int ntot = g.cp_gcount[cp] + (cp == g.ncp - 1 ? 1 : 0);
-      for (int en = lane; en < ntot; en += 32) item(cp, en);
     }
   }
   if (e.omax) {

@@ -171,6 +171,13 @@ std::vector<double> pinv_solve(int n, const std::vector<double> &a, const std::v
 
 int alloc_vec(sdft_mixer *m, double **p) { return dev_alloc(m->device, m->st, (void **)p, (size_t)m->n * 8); }
 
+// n doubles between host and device (or device and device) in the mixer's
+// stream order, complete on return
+bool copy_sync(sdft_mixer *m, void *dst, const void *src, cudaMemcpyKind kind) {
+  return cudaMemcpyAsync(dst, src, (size_t)m->n * 8, kind, m->st) == cudaSuccess &&
+         cudaStreamSynchronize(m->st) == cudaSuccess;
+}
+
 // bank <- rho (newest first); the oldest buffer is reused
 int bank_push(sdft_mixer *m, const double *rho) {
   double *buf = m->bank.back();
@@ -354,13 +361,13 @@ extern "C" int sdft_mixer_write_checkpoint(sdft_mixer *m, const char *path, cons
   std::vector<char> iobuf(1 << 22);
   setvbuf(f, iobuf.data(), _IOFBF, iobuf.size());
   int r = fprintf(f, "%i %i\n", m->iscf, nd) < 0 ? set_error(SDFT_ERR_ARG, "write_checkpoint: write failed") : 0;
-  if (!r && cudaMemcpy(h.data(), rho, (size_t)m->n * 8, cudaMemcpyDefault) != cudaSuccess)
+  if (!r && !copy_sync(m, h.data(), rho, cudaMemcpyDefault))
     r = set_error(SDFT_ERR_CUDA, "write_checkpoint: copy");
   if (!r) r = write_vec(f, h.data(), m->n, vol, true);
   for (int k = 0; !r && k < nout + nd; k++) {
     const double *src = k < nout ? m->bank[k] : m->err[k - nout];
     if (!src) { r = set_error(SDFT_ERR_STATE, "write_checkpoint: bank entry missing"); break; }
-    if (cudaMemcpy(h.data(), src, (size_t)m->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (!copy_sync(m, h.data(), src, cudaMemcpyDeviceToHost))
       r = set_error(SDFT_ERR_CUDA, "write_checkpoint: copy");
     else
       r = write_vec(f, h.data(), m->n, 1.0, false);
@@ -381,16 +388,16 @@ extern "C" int sdft_mixer_read_checkpoint(sdft_mixer *m, const char *path, doubl
     r = set_error(SDFT_ERR_ARG, "read_checkpoint: bad header");
   std::vector<double> h((size_t)m->n);
   if (!r) r = read_vec(f, h.data(), m->n);
-  if (!r && cudaMemcpy(rho, h.data(), (size_t)m->n * 8, cudaMemcpyDefault) != cudaSuccess)
+  if (!r && !copy_sync(m, rho, h.data(), cudaMemcpyDefault))
     r = set_error(SDFT_ERR_CUDA, "read_checkpoint: copy");
-  if (!r && cudaMemcpy(m->old, h.data(), (size_t)m->n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+  if (!r && !copy_sync(m, m->old, h.data(), cudaMemcpyHostToDevice))
     r = set_error(SDFT_ERR_CUDA, "read_checkpoint: copy");
   const int nout = nd < m->num_diis ? nd + 1 : nd;
   for (int k = 0; !r && k < nout + nd; k++) {
     double **slot = k < nout ? &m->bank[k] : &m->err[k - nout];
     if (!*slot && (r = alloc_vec(m, slot))) break;
     if ((r = read_vec(f, h.data(), m->n))) break;
-    if (cudaMemcpy(*slot, h.data(), (size_t)m->n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!copy_sync(m, *slot, h.data(), cudaMemcpyHostToDevice))
       r = set_error(SDFT_ERR_CUDA, "read_checkpoint: copy");
   }
   fclose(f);

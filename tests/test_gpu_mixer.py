@@ -17,10 +17,11 @@ def _densities(n, steps, seed=3):
     return [base + (0.6 ** k) * 1e-3 * rng.standard_normal(n) for k in range(steps)]
 
 
-@pytest.mark.parametrize("n", [1000, 96 ** 3])
-def test_device_mixer_matches_oracle(pkg, n):
-    dev = pkg.DensityMixer(n, **PARAMS)
-    orc = OM.DensityMixer(n, **PARAMS)
+@pytest.mark.parametrize("n,params", [(1000, PARAMS), (96 ** 3, PARAMS), (5000, dict(PARAMS, num_diis=1, num_step_mix=0)),
+                                      (5000, dict(PARAMS, num_diis=7, num_step_mix=1))])
+def test_device_mixer_matches_oracle(pkg, n, params):
+    dev = pkg.DensityMixer(n, **params)
+    orc = OM.DensityMixer(n, **params)
     rho = np.zeros(n)
     try:
         for k, rc in enumerate(_densities(n, 14)):
@@ -28,7 +29,7 @@ def test_device_mixer_matches_oracle(pkg, n):
             b = orc.step(k, rc)
             if k == 0:
                 assert not a.any()  # rho_up untouched at step 0
-            elif k <= PARAMS["num_step_mix"]:
+            elif k <= params["num_step_mix"]:
                 assert np.array_equal(a, b), k
             else:
                 assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b)), k

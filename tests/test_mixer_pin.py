@@ -20,14 +20,16 @@ def _densities(n, steps, seed=3):
     return [base + (0.6 ** k) * 1e-3 * rng.standard_normal(n) for k in range(steps)]
 
 
-def test_mixing_matches_reference():
+@pytest.mark.parametrize("params", [PARAMS, dict(PARAMS, num_diis=1, num_step_mix=0),
+                                    dict(PARAMS, num_diis=7, num_step_mix=1)])
+def test_mixing_matches_reference(params):
     n, steps = 4096, 14
-    ref = R.RefMixer(n, **PARAMS)
-    orc = OM.DensityMixer(n, **PARAMS)
+    ref = R.RefMixer(n, **params)
+    orc = OM.DensityMixer(n, **params)
     for k, rho in enumerate(_densities(n, steps)):
         a = ref.step(k, rho)
         b = orc.step(k, rho)
-        if k <= PARAMS["num_step_mix"]:
+        if k <= params["num_step_mix"]:
             assert np.array_equal(a, b), k  # bank / simple mix: same operations
         else:
             assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a)), k

@@ -146,6 +146,13 @@ PROFILED_TRAFFIC = {("kf_stage_b", (96, 96, 96), True): (136.5e6 + 73.2e6) / 64,
                     ("kf_stage_c", (96, 96, 96), True): (294.2e6 + 301.1e6) / 64}
 PROFILED_GEMM_TRAFFIC = {((96, 96, 96), True, 512): (1.14e9 + 63.8e6 + 865.8e6 + 398.0e6) / 2}
 
+# What bounds the HBM-class kernels that sit well below the copy bandwidth,
+# from their ncu captures (profiles/)
+PROFILED_LIMITER = {
+    "kf_stage_b": "shared-memory pipe (l1tex 70.7 % of peak, issue 68 %; ten plane-sized shared passes per plane)",
+    "kf_stage_c": "latency (long-scoreboard and barrier stalls lead; DRAM 35 % on a 64-pair capture)",
+}
+
 KERNEL_OF = {"stage_a_pack_cfft": "kf_stage_a", "stage_b_plane_fft_vks": "kf_stage_b",
              "stage_c_cfft_unpack_recur": "kf_stage_c", "kb_proj_gemm": "kb_gemm", "kb_back_gemm": "kb_gemm",
              "density_planes": "kf_stage_b_density"}
@@ -184,6 +191,8 @@ def rooflines(timing, s, nsto, mixed, back_products=10):
             out.append({"kernel": kern, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                         "frac": ach / peak, "traffic": tr * ((nsto + 1) // 2) if tr else None,
                         "peak_source": src, "ms_total": ms, "launches": n})
+            if kern in PROFILED_LIMITER:
+                out[-1]["limiter"] = PROFILED_LIMITER[kern]
         else:
             if mixed:
                 ach = ops8 / t / 1e12

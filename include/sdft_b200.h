@@ -27,6 +27,7 @@
  *   sdft_gaussran2_signs_dev          <- the gaussran2 call of genNoiseOrbitalReal, stodft/gen-noise.c:256 (signs only)
  *   sdft_lanczos_bounds               <- genEnergyMax/genEnergyMin stodft/calc-spectral-range.c:33,339 (Lanczos)
  *   sdft_energy_chempot_dev           <- calcEnergyChemPot stodft/calc-energy.c:32
+ *   sdft_xc_lda_dev                   <- excpot_pz_lda / excpot_pw_lda energy/cp/xc_functionals.c:268,378
  *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
  *                                        stodft/checkpointIO.c:32,218
  */
@@ -215,6 +216,17 @@ int sdft_lanczos_bounds(sdft_ctx *ctx, int nstep, const double *v0re, const doub
  * ranks, sum the per-rank values (each passing the global nsto_total). */
 int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total,
                             double *energy_ke, double *energy_pnl);
+
+/* ---- exchange-correlation ----------------------------------------------- */
+#define SDFT_XC_PZ_LDA 1  /* Perdew-Zunger 1981 (excpot_pz_lda)            */
+#define SDFT_XC_PW_LDA 2  /* Perdew-Wang 1992 (excpot_pw_lda)              */
+/* The LDA step of cpGetVksStodft (stodft/reduced-energy/
+ * cp-energy-ee-rho-stodft.c:838-870; energy/cp/xc_functionals.c:268,378),
+ * spin-unpolarised: over the n real-space points, vks += V_xc(rho) and
+ * *exc / *muxc (nullable) = E_xc and sum V_xc rho, both times vol / n.
+ * rho and vks are device pointers; runs on `stream` and synchronises it. */
+int sdft_xc_lda_dev(int kind, long long n, const double *rho, double *vks, double vol, double *exc,
+                    double *muxc, void *stream);
 
 /* ---- density mixing and checkpoint files -------------------------------- */
 /* genDensityMix (stodft/diis.c:34-464) with the densities on the device,

@@ -42,6 +42,7 @@ def lib():
         L.ref_mix_set_rho.argtypes = [C.c_void_p, _dp]
         L.ref_mix_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]
         L.ref_mix_checkpoint.restype = C.c_int
+        L.ref_xc_lda.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, _dp, _dp]
         _lib = L
     return _lib
 
@@ -170,3 +171,13 @@ class RefMixer:
         if rc:
             raise OSError("checkpointOutput harness failed")
         return os.path.join(str(directory), "density-checkpoint")
+
+
+def xc_lda(kind, rho, vks, vol):
+    """excpot_pz_lda (kind 1) / excpot_pw_lda (kind 2) of the reference:
+    returns (vks + V_xc, E_xc, mu_xc)."""
+    rho = f64(rho).copy()
+    v = f64(vks).copy()
+    exc, muxc = C.c_double(0.0), C.c_double(0.0)
+    lib().ref_xc_lda(int(kind), rho.size, _d(rho), _d(v), float(vol), C.byref(exc), C.byref(muxc))
+    return v, exc.value, muxc.value

@@ -167,8 +167,8 @@ ABORT_STUB(coef_force_tau_fun_full_g) ABORT_STUB(coef_force_tau_fun_hybrid)
 ABORT_STUB(controlEnergyNlppRealThreads) ABORT_STUB(controlPotentialEnergyFilter) ABORT_STUB(control_contract_rho)
 ABORT_STUB(control_grad_rho) ABORT_STUB(control_nonloc_gh) ABORT_STUB(control_spread_rho)
 ABORT_STUB(cp_condiag_ksmat) ABORT_STUB(cp_rotate_vector) ABORT_STUB(dcfftb_generic_) ABORT_STUB(dcfftf_generic_)
-ABORT_STUB(dcffti_generic_) ABORT_STUB(excpot_pade_lda) ABORT_STUB(excpot_pade_lsda) ABORT_STUB(excpot_pw_lda)
-ABORT_STUB(excpot_pw_lsda) ABORT_STUB(excpot_pz_lda) ABORT_STUB(excpot_pz_lsda)
+ABORT_STUB(dcffti_generic_) 
+
 ABORT_STUB(getnl_fcoef_gh) ABORT_STUB(getnl_pot_pv_fatm_gh) ABORT_STUB(grad_corr_lda) ABORT_STUB(grad_corr_lsda)
 ABORT_STUB(cfopen)
 void Barrier(int c) { (void)c; }
@@ -669,4 +669,19 @@ int ref_mix_checkpoint(RefMix *m, const char *dir, double l1, double l2, double 
   m->hmat[1] = l1; m->hmat[5] = l2; m->hmat[9] = l3;
   checkpointOutput(&m->cp, &m->gd);
   return chdir(cwd) != 0;
+}
+
+/* ====================================================================== */
+/* LDA exchange-correlation (energy/cp/xc_functionals.c): kind 1 = PZ81,  */
+/* 2 = PW92; rho and vks 0-based (vks += V_xc)                            */
+/* ====================================================================== */
+void excpot_pz_lda(double *, double *, double *, double *, int, int, double, int, int, double *, int);
+void excpot_pw_lda(double *, double *, double *, double *, int, int, double, int, int, double *, int);
+
+void ref_xc_lda(int kind, int n, double *rho, double *vks, double vol, double *exc, double *muxc) {
+  double pvten[10] = {0};
+  *exc = 0.0;
+  *muxc = 0.0;
+  if (kind == 1) excpot_pz_lda(vks - 1, rho - 1, exc, muxc, 2 * n, 2 * n, vol, 0, 0, pvten, 0);
+  else excpot_pw_lda(vks - 1, rho - 1, exc, muxc, 2 * n, 2 * n, vol, 0, 0, pvten, 0);
 }

@@ -118,6 +118,7 @@ _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
+_sig("sdft_xc_lda_dev", C.c_int, [C.c_int, C.c_longlong, _vp, _vp, C.c_double, _dp, _dp, _vp])
 _sig("sdft_mixer_create", C.c_int, [C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.POINTER(_vp)])
 _sig("sdft_mixer_step", C.c_int, [_vp, C.c_int, _vp, _vp])
@@ -241,6 +242,19 @@ def gaussran2(nran, seed):
     out = np.zeros(max(nran, 1))
     _chk(lib.sdft_gaussran2(nran, C.byref(q), _d(out)))
     return out[:nran], q.value
+
+
+SDFT_XC_PZ_LDA = 1
+SDFT_XC_PW_LDA = 2
+
+
+def xc_lda_dev(kind, n, rho_ptr, vks_ptr, vol, stream_ptr=0):
+    """vks += V_xc(rho) on the device (pointers of n doubles); returns
+    (E_xc, sum V_xc rho) times vol / n (the LDA step of cpGetVksStodft)."""
+    exc, muxc = C.c_double(0.0), C.c_double(0.0)
+    _chk(lib.sdft_xc_lda_dev(int(kind), int(n), C.c_void_p(rho_ptr), C.c_void_p(vks_ptr), float(vol), C.byref(exc),
+                             C.byref(muxc), C.c_void_p(stream_ptr)))
+    return exc.value, muxc.value
 
 
 def gaussran2_signs_dev(nran, seed, out_ptr, stream_ptr=0):

@@ -27,6 +27,8 @@
  *   sdft_gaussran2_signs_dev          <- the gaussran2 call of genNoiseOrbitalReal, stodft/gen-noise.c:256 (signs only)
  *   sdft_lanczos_bounds               <- genEnergyMax/genEnergyMin stodft/calc-spectral-range.c:33,339 (Lanczos)
  *   sdft_energy_chempot_dev           <- calcEnergyChemPot stodft/calc-energy.c:32
+ *   sdft_nl_force_dev                 <- calcEnergyForce stodft/calc-nuclei-force.c:33 (nonlocal part:
+ *                                        calcNlPseudoPostScf stodft/reduced-energy/energy-wrapper-post-scf.c:224)
  *   sdft_xc_lda_dev                   <- excpot_pz_lda / excpot_pw_lda energy/cp/xc_functionals.c:268,378
  *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
  *                                        stodft/checkpointIO.c:32,218
@@ -216,6 +218,16 @@ int sdft_lanczos_bounds(sdft_ctx *ctx, int nstep, const double *v0re, const doub
  * ranks, sum the per-rank values (each passing the global nsto_total). */
 int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total,
                             double *energy_ke, double *energy_pnl);
+/* The nonlocal (Kleinman-Bylander) atomic forces of calcEnergyForce
+ * (stodft/calc-nuclei-force.c:33-480: calcNlPseudoPostScf, then occNumber /
+ * numStateStoUp) for chemical potential imu of the filtered orbitals
+ * resident on the device (first nstate):
+ * fatm[3 a + d] = -2 occ / nsto_total sum_{s, l, m} vnorm_l / vol
+ *                 (Re Z dRe Z/dR_ad + Im Z dIm Z/dR_ad),
+ * atoms in the order of sdft_kb_desc.pos.  energy_pnl (nullable) as in
+ * sdft_energy_chempot_dev.  With several ranks, sum the per-rank forces. */
+int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total, double *fatm,
+                      double *energy_pnl);
 
 /* ---- exchange-correlation ----------------------------------------------- */
 #define SDFT_XC_PZ_LDA 1  /* Perdew-Zunger 1981 (excpot_pz_lda)            */

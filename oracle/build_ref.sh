@@ -16,7 +16,8 @@ SRCS="stodft/filter.c stodft/normh.c stodft/calc-chempot-chebyshev.c stodft/coef
       stodft/reduced-energy/cp-energy-ee-rho-stodft.c mathlib/fft_package.c mathlib/fft_create_package.c
       mathlib/mathlib.c energy/cp/cp_energy_eext_nonloc.c energy/cp/cp_energy_eext.c
       energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c
-      stodft/density.c stodft/gen-noise.c stodft/diis.c stodft/checkpointIO.c energy/cp/xc_functionals.c"
+      stodft/density.c stodft/gen-noise.c stodft/diis.c stodft/checkpointIO.c energy/cp/xc_functionals.c
+      stodft/reduced-energy/energy-wrapper-post-scf.c"
 OBJS=""
 for f in $SRCS; do
   o="$OUT/obj/$(echo "$f" | tr '/' '_').o"

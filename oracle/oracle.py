@@ -37,6 +37,7 @@ def lib():
         L.oracle_set_kb.argtypes = [C.c_void_p, C.c_int, _dp, _ip, C.c_int, C.c_int, _ip, C.c_int, C.c_double,
                                     C.c_double, _dp, _dp, _dp]
         L.oracle_hpsi.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.oracle_nl_force.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
         L.oracle_normh_cheby.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _dp, _dp,
                                          _dp, _dp, _dp, _dp]
         L.oracle_normh_newton.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp,
@@ -116,6 +117,16 @@ class OracleSys:
         e = C.c_double()
         lib().oracle_hpsi(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e))
         return (fr, fi, e.value) if want_enl else (fr, fi)
+
+    def nl_force(self, cre, cim):
+        """KB nonlocal atomic forces [natm, 3] and energy of the given orbitals
+        (raw sums over them, before occ / numStateStoUp)."""
+        cre, cim = f64(cre), f64(cim)
+        n = self._keep[0].size // 3 if hasattr(self, "_keep") else 0
+        f = np.zeros(3 * max(n, 1))
+        e = C.c_double()
+        lib().oracle_nl_force(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(f), C.byref(e))
+        return f[:3 * n].reshape(n, 3), e.value
 
     def filter_cheby(self, cre, cim, ec, nmu, scale, emean, store_moments=False):
         cre, cim, ec = f64(cre), f64(cim), f64(ec)

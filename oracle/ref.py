@@ -26,6 +26,7 @@ def lib():
         L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int, _dp,
                                  C.c_int, C.c_double, C.c_double, _dp, _dp, C.c_double, C.c_int]
         L.ref_hpsi.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.ref_nl_force.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
         L.ref_filter.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_int, _dp, _dp, C.c_double,
                                  C.c_double, _dp, _dp, _dp]
         L.ref_moments.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, _dp]
@@ -70,6 +71,7 @@ class RefSys:
         kb = s["kb_desc"]
         self.ncoef = len(s["ka"])
         self.N = int(np.prod(s["grid"]))
+        self.natm = int(kb["natm"])
         self.keep = [i32(s["ka"]), i32(s["kb"]), i32(s["kc"]), i32(s["ib1"]), i32(s["ib2"]),
                      f64(np.asarray(s["hmat"], float).T.reshape(9)), f64(s["vks"]), f64(kb["pos"]), f64(kb["vps"]),
                      f64(kb["vpsnorm"])]
@@ -84,6 +86,15 @@ class RefSys:
         e = C.c_double()
         lib().ref_hpsi(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e))
         return fr, fi, e.value
+
+    def nl_force(self, cre, cim):
+        """calcNlPseudoPostScf on the given orbitals: KB atomic forces [natm, 3]
+        and energy, before calcEnergyForce's occ / numStateStoUp."""
+        cre, cim = f64(cre), f64(cim)
+        f = np.zeros(3 * self.natm)
+        e = C.c_double()
+        lib().ref_nl_force(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(f), C.byref(e))
+        return f.reshape(self.natm, 3), e.value
 
     def filter(self, cheby, cre, cim, ec, nmu, scale, emean, samp=None, moments=False):
         cre, cim, ec = f64(cre), f64(cim), f64(ec)

@@ -162,7 +162,7 @@ static void sdft_ref_abort(const char *f) {
 ABORT_STUB(Allgather) ABORT_STUB(Allgatherv) ABORT_STUB(Allreduce) ABORT_STUB(Alltoall) ABORT_STUB(Alltoallv)
 ABORT_STUB(Finalize) ABORT_STUB(Gatherv) ABORT_STUB(Reduce) ABORT_STUB(Reduce_scatter) ABORT_STUB(Scatterv)
 ABORT_STUB(Bcast) ABORT_STUB(Send) ABORT_STUB(Recv) ABORT_STUB(DGEMV) ABORT_STUB(DSYMV) ABORT_STUB(dsysv_) ABORT_STUB(rs_)
-ABORT_STUB(calcChemPotInterp) ABORT_STUB(calcCoefForceWrap) ABORT_STUB(coef_force_calc_hybrid_threads_state)
+ABORT_STUB(calcChemPotInterp) ABORT_STUB(coef_force_calc_hybrid_threads_state)
 ABORT_STUB(coef_force_tau_fun_full_g) ABORT_STUB(coef_force_tau_fun_hybrid)
 ABORT_STUB(controlEnergyNlppRealThreads) ABORT_STUB(controlPotentialEnergyFilter) ABORT_STUB(control_contract_rho)
 ABORT_STUB(control_grad_rho) ABORT_STUB(control_nonloc_gh) ABORT_STUB(control_spread_rho)
@@ -324,8 +324,12 @@ RefSys *ref_create(int n1, int n2, int n3, int ncoef, const int *ka, const int *
   ps->np_nl = i1(4); ps->np_nl_gh = i1(4);
   ps->np_nl[1] = natm; ps->np_nl[2] = natm;
   ps->np_nonloc_cp_box_kb = natm; ps->np_nonloc_cp_box_gh = 0;
-  ps->ip_nl = i1(natm); ps->ip_nl_rev = i1(2 * natm + 2);
-  for (int i = 1; i <= natm; i++) { ps->ip_nl[i] = i; ps->ip_nl_rev[i] = i; ps->ip_nl_rev[i + natm] = i; }
+  /* ip_nl / ip_nl_rev are indexed (ipart + l*natm) for each open l channel */
+  ps->ip_nl = i1(2 * natm + 2); ps->ip_nl_rev = i1(2 * natm + 2);
+  for (int i = 1; i <= natm; i++) {
+    ps->ip_nl[i] = ps->ip_nl[i + natm] = i;
+    ps->ip_nl_rev[i] = ps->ip_nl_rev[i + natm] = i;
+  }
   ps->nrad_max_l = i1(4); ps->nrad_max_l[1] = 1; ps->nrad_max_l[2] = 1;
   ps->np_nl_rad_str = (int **)calloc(4, sizeof(int *));
   for (int l = 1; l <= 3; l++) { ps->np_nl_rad_str[l] = i1(2); ps->np_nl_rad_str[l][1] = 1; }
@@ -382,6 +386,27 @@ int ref_hpsi(RefSys *r, int ns, const double *re, const double *im, double *fre,
   calcCoefForceWrapSCF(&r->cls, &r->gd, &r->cp, &r->cpos, &r->apos);
   memcpy(fre, &r->cpos.fcre_up[1], sizeof(double) * ns * r->ncoef);
   memcpy(fim, &r->cpos.fcim_up[1], sizeof(double) * ns * r->ncoef);
+  if (enl) *enl = r->gd.stat_avg.cp_enl;
+  return 0;
+}
+
+/* KB nonlocal atomic forces and energy of the loaded states through the
+ * reference's calcNlPseudoPostScf (stodft/reduced-energy/energy-wrapper-post-scf.c:224):
+ * control_ewd_non_loc / get_nlmat (Z and dZ/dR) then getnl_pot_pv_fatm.
+ * f[3a+d]: the raw per-atom sums, before calcEnergyForce's occ / numStateStoUp. */
+void calcNlPseudoPostScf(CLASS *, GENERAL_DATA *, CP *, CPCOEFFS_POS *, CLATOMS_POS *);
+int ref_nl_force(RefSys *r, int ns, const double *re, const double *im, double *f, double *enl) {
+  load_states(r, ns, re, im);
+  memset(&r->cpos.fcre_up[1], 0, sizeof(double) * ns * r->ncoef);
+  memset(&r->cpos.fcim_up[1], 0, sizeof(double) * ns * r->ncoef);
+  for (int a = 1; a <= r->natm; a++) r->apos.fx[a] = r->apos.fy[a] = r->apos.fz[a] = 0.0;
+  r->gd.stat_avg.cp_enl = 0.0;
+  calcNlPseudoPostScf(&r->cls, &r->gd, &r->cp, &r->cpos, &r->apos);
+  for (int a = 0; a < r->natm; a++) {
+    f[3 * a] = r->apos.fx[a + 1];
+    f[3 * a + 1] = r->apos.fy[a + 1];
+    f[3 * a + 2] = r->apos.fz[a + 1];
+  }
   if (enl) *enl = r->gd.stat_avg.cp_enl;
   return 0;
 }

@@ -265,15 +265,19 @@ static void ylm(double xk, double yk, double zk, double g, double *yr, double *y
  *   back proj.   getnl_fcoef energy/cp/cp_energy_eext_nonloc.c:1669-1935, control_nlfcoef,
  *                get_nlfor :2136-2173, get_nlfor0 :2229-2265                             */
 /* ------------------------------------------------------------------------ */
-static void kb_force(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *fcre,
-                     double *fcim, double *enl_out) {
-  if (s->natm == 0) { if (enl_out) *enl_out = 0.0; return; }
+/* Z[atom][state][lm] re/im of the KB projection and, when dzr is given, its
+ * derivatives by the atom positions dZ/dR_d (d = x, y, z; [d][atom][state][lm]),
+ * as get_nlmat accumulates them next to Z (energy/cp/cp_energy_eext_nonloc.c:
+ * 648-748): d(c e^{iG.R})/dR_d = i G_d c e^{iG.R}, so for even l
+ * dZr_d += -cbyhel_i 2Yr G_d, dZi_d += -cbyhel_i 2Yi G_d and for odd l
+ * dZr_d += -cbyhel_r 2Yi G_d, dZi_d += cbyhel_r 2Yr G_d.  The G = 0 term has
+ * no position dependence.  Caller zeroes zr, zi (and dzr, dzi). */
+static void kb_project(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *zr, double *zi,
+                       double *dzr, double *dzi) {
   const int ncoef = s->ncoef, nk = ncoef - 1, natm = s->natm;
   const int nlm = (s->lmax + 1) * (s->lmax + 1);
+  const size_t zn = (size_t)natm * nstate * nlm;
   const double tpi = 2.0 * M_PI, *hi = s->hmati;
-  /* Z[atom][state][lm] re/im */
-  double *zr = calloc((size_t)natm * nstate * nlm, sizeof(double));
-  double *zi = calloc((size_t)natm * nstate * nlm, sizeof(double));
   double *sx = malloc(sizeof(double) * natm * 3), *cossc = malloc(sizeof(double) * natm),
          *sinsc = malloc(sizeof(double) * natm), *helr = malloc(sizeof(double) * natm),
          *heli = malloc(sizeof(double) * natm);
@@ -287,12 +291,11 @@ static void kb_force(const oracle_sys *s, int nstate, const double *cre, const d
     sinsc[a] = sin(sx[3 * a + 2] * tpi);
   }
   double yr[10], yi[10];
-  /* projection */
   for (int ic = 0; ic < nk; ic++) {
     double aka = s->ka[ic], akb = s->kb[ic], akc = s->kc[ic];
     double xk = (aka * hi[0] + akb * hi[1] + akc * hi[2]) * tpi, yk = (aka * hi[3] + akb * hi[4] + akc * hi[5]) * tpi,
            zk = (aka * hi[6] + akb * hi[7] + akc * hi[8]) * tpi;
-    double g = sqrt(xk * xk + yk * yk + zk * zk);
+    double g = sqrt(xk * xk + yk * yk + zk * zk), gk[3] = {xk, yk, zk};
     if (s->ib1[ic])
       for (int a = 0; a < natm; a++) {
         double arg = (aka * sx[3 * a] + akb * sx[3 * a + 1] + akc * sx[3 * a + 2]) * tpi;
@@ -310,8 +313,14 @@ static void kb_force(const oracle_sys *s, int nstate, const double *cre, const d
           for (int st = 0; st < nstate; st++) {
             double c_r = cre[(size_t)st * ncoef + ic], c_i = cim[(size_t)st * ncoef + ic];
             double bhr = c_r * hr - c_i * hm, bhi = c_r * hm + c_i * hr;
-            if (l % 2 == 1) { zr[ZI(a, st, lm - 1)] += -bhi * tyi; zi[ZI(a, st, lm - 1)] += bhi * tyr; }
-            else { zr[ZI(a, st, lm - 1)] += bhr * tyr; zi[ZI(a, st, lm - 1)] += bhr * tyi; }
+            size_t z = ZI(a, st, lm - 1);
+            if (l % 2 == 1) { zr[z] += -bhi * tyi; zi[z] += bhi * tyr; }
+            else { zr[z] += bhr * tyr; zi[z] += bhr * tyi; }
+            if (dzr)
+              for (int d = 0; d < 3; d++) {
+                if (l % 2 == 1) { dzr[d * zn + z] += -bhr * tyi * gk[d]; dzi[d * zn + z] += bhr * tyr * gk[d]; }
+                else { dzr[d * zn + z] += -bhi * tyr * gk[d]; dzi[d * zn + z] += -bhi * tyi * gk[d]; }
+              }
           }
         }
       }
@@ -333,6 +342,31 @@ static void kb_force(const oracle_sys *s, int nstate, const double *cre, const d
       for (int st = 0; st < nstate; st++) zr[ZI(a, st, 0)] += cre[(size_t)st * ncoef + nk] * vt;
     }
   }
+#undef ZI
+  free(sx); free(cossc); free(sinsc); free(helr); free(heli);
+}
+
+static void kb_force(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *fcre,
+                     double *fcim, double *enl_out) {
+  if (s->natm == 0) { if (enl_out) *enl_out = 0.0; return; }
+  const int ncoef = s->ncoef, nk = ncoef - 1, natm = s->natm;
+  const int nlm = (s->lmax + 1) * (s->lmax + 1);
+  const double tpi = 2.0 * M_PI, *hi = s->hmati;
+  /* Z[atom][state][lm] re/im */
+  double *zr = calloc((size_t)natm * nstate * nlm, sizeof(double));
+  double *zi = calloc((size_t)natm * nstate * nlm, sizeof(double));
+  double *sx = malloc(sizeof(double) * natm * 3), *cossc = malloc(sizeof(double) * natm),
+         *sinsc = malloc(sizeof(double) * natm), *helr = malloc(sizeof(double) * natm),
+         *heli = malloc(sizeof(double) * natm);
+#define ZI(a, st, lm) (((size_t)(a) * nstate + (st)) * nlm + (lm))
+  for (int a = 0; a < natm; a++) {
+    double dx = s->pos[3 * a], dy = s->pos[3 * a + 1], dz = s->pos[3 * a + 2];
+    double as[3] = {dx * hi[0] + dy * hi[3] + dz * hi[6], dx * hi[1] + dy * hi[4] + dz * hi[7],
+                    dx * hi[2] + dy * hi[5] + dz * hi[8]};
+    for (int d = 0; d < 3; d++) sx[3 * a + d] = as[d] - nearbyint(as[d]);
+  }
+  double yr[10], yi[10];
+  kb_project(s, nstate, cre, cim, zr, zi, NULL, NULL);
   /* energy */
   double enl = 0.0;
   for (int a = 0; a < natm; a++) {
@@ -399,6 +433,41 @@ static void kb_force(const oracle_sys *s, int nstate, const double *cre, const d
   }
 #undef ZI
   free(zr); free(zi); free(sx); free(cossc); free(sinsc); free(helr); free(heli);
+}
+
+/* KB nonlocal atomic forces and energy of nstate orbitals, the sum that
+ * calcNlPseudoPostScf (stodft/reduced-energy/energy-wrapper-post-scf.c:224-615)
+ * forms through control_ewd_non_loc / get_nlmat and getnl_pot_pv_fatm ->
+ * sumnl_pot_pv_fatm_hess (energy/cp/cp_energy_eext_nonloc.c:1122-1530), one
+ * radial channel:  F_a,d = -2 sum_{state, l, m} (dZr_d Zr + dZi_d Zi) vnorm_l / vol,
+ * E_NL = sum |Z|^2 vnorm_l / vol.  Raw sums over the given states, before the
+ * occNumber / numStateStoUp of calcEnergyForce (stodft/calc-nuclei-force.c:
+ * 462-480).  f: natm * 3 (x, y, z per atom). */
+void oracle_nl_force(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *f, double *enl) {
+  const int natm = s->natm;
+  for (int i = 0; i < 3 * natm; i++) f[i] = 0.0;
+  if (enl) *enl = 0.0;
+  if (natm == 0 || nstate < 1) return;
+  const int nlm = (s->lmax + 1) * (s->lmax + 1);
+  const size_t zn = (size_t)natm * nstate * nlm;
+  double *zr = calloc(zn, sizeof(double)), *zi = calloc(zn, sizeof(double));
+  double *dzr = calloc(3 * zn, sizeof(double)), *dzi = calloc(3 * zn, sizeof(double));
+  kb_project(s, nstate, cre, cim, zr, zi, dzr, dzi);
+  double e = 0.0;
+  for (int a = 0; a < natm; a++) {
+    int t = s->type[a];
+    for (int l = 0; l <= s->lmax_type[t]; l++) {
+      double vn = s->vpsnorm[t * (s->lmax + 1) + l] / s->vol;
+      for (int m = 1; m <= 2 * l + 1; m++)
+        for (int st = 0; st < nstate; st++) {
+          size_t z = ((size_t)a * nstate + st) * nlm + (m + l * l - 1);
+          e += (zr[z] * zr[z] + zi[z] * zi[z]) * vn;
+          for (int d = 0; d < 3; d++) f[3 * a + d] += -2.0 * (dzr[d * zn + z] * zr[z] + dzi[d * zn + z] * zi[z]) * vn;
+        }
+    }
+  }
+  if (enl) *enl = e;
+  free(zr); free(zi); free(dzr); free(dzi);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -14,6 +14,8 @@ void oracle_set_kinetic_cap(oracle_sys *s, double gcut);
 void oracle_set_kb(oracle_sys *s, int natm, const double *pos, const int *type, int ntype, int lmax,
                    const int *lmax_type, int nsplin, double gmin, double dg, const double *vps,
                    const double *vpsnorm, const double *gzvps0);
+/* KB nonlocal atomic forces f[natm*3] and energy of nstate orbitals (raw sums) */
+void oracle_nl_force(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *f, double *enl);
 void oracle_hpsi(const oracle_sys *s, int nstate, const double *cre, const double *cim, double *fcre, double *fcim,
                  double *enl);
 void oracle_normh_cheby(const oracle_sys *s, int nstate, int ipoly, int cpy, double scale, double emean, double *cre,

@@ -128,6 +128,7 @@ _sig("sdft_mixer_read_checkpoint", C.c_int, [_vp, C.c_char_p, _vp])
 _sig("sdft_mixer_destroy", C.c_int, [_vp])
 _sig("sdft_lanczos_bounds", C.c_int, [_vp, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _ip, _dp, _dp])
 _sig("sdft_energy_chempot_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp])
+_sig("sdft_nl_force_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp])
 _sig("sdft_batch_set_priority", C.c_int, [_vp, C.c_int])
 _sig("sdft_download_density", C.c_int, [_vp, _dp])
 _sig("sdft_batch_create", C.c_int, [C.c_int, C.POINTER(_vp), _ip, _ip, C.POINTER(_dp), _dp, _dp, _dp, C.POINTER(_vp)])
@@ -309,6 +310,7 @@ class Context:
         """kb: dict with natm,pos,type,ntype,lmax,lmax_type,nsplin_g,gmin_spl,dg_spl,vps,vpsnorm,gzvps0"""
         if kb is None or kb["natm"] == 0:
             _chk(lib.sdft_ctx_set_kb(self._p, None))
+            self._kb_keep = None
             return
         self._kb_keep = {k: (_f64(v) if k in ("pos", "vps", "vpsnorm", "gzvps0") else
                              (_i32(v) if k in ("type", "lmax_type") else v)) for k, v in kb.items()}
@@ -485,6 +487,18 @@ class Context:
         _chk(lib.sdft_energy_chempot_dev(self._p, int(nstate), int(imu), float(occ),
                                          int(nsto_total or nstate), C.byref(ek), C.byref(ep)))
         return ek.value, ep.value
+
+    def nl_force_dev(self, nstate, imu=0, occ=2.0, nsto_total=None):
+        """(forces [natm, 3], energy_pnl): the nonlocal atomic forces of the
+        filtered orbitals for chemical potential imu, as calcEnergyForce forms
+        them (occ / nsto_total times the calcNlPseudoPostScf sums)."""
+        kb = getattr(self, "_kb_keep", None)
+        natm = int(kb["natm"]) if kb else 0
+        f = np.zeros(3 * max(natm, 1))
+        ep = C.c_double(0.0)
+        _chk(lib.sdft_nl_force_dev(self._p, int(nstate), int(imu), float(occ), int(nsto_total or nstate), _d(f),
+                                   C.byref(ep)))
+        return f[:3 * natm].reshape(natm, 3), ep.value
 
     @property
     def stream_ptr(self):

@@ -231,6 +231,8 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
     TScope ts(ctx, 7);
     // row maxima: from the stage C that wrote `vec`, else one pass over it
     if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
+      // the pass takes the max into d_rowmax: clear maxima a stage C left there
+      if (ctx->rowmax_zero_n < nstate) CK(cudaMemsetAsync(ctx->d_rowmax, 0, (size_t)nstate * 8, ctx->st));
       launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);
       ctx->launches++;
     }
@@ -673,7 +675,7 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_enl, ctx->d_red, ctx->d_kb_rng,
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
-                  ctx->d_oz_part};
+                  ctx->d_oz_part, ctx->d_kb_rs, ctx->d_kb_rc, ctx->d_gk, ctx->d_zsave};
   // a batch graph still holding the context: wait for its replays, drop the context from it
   for (sdft_batch *b : ctx->batches) batch_detach(b, ctx);
   ctx->batches.clear();
@@ -1175,6 +1177,62 @@ extern "C" int sdft_energy_chempot_dev(sdft_ctx *ctx, int nstate, int imu, doubl
   *energy_ke = occ * 0.5 * ek / nsto_total;
   *energy_pnl = occ * en / nsto_total;
   return SDFT_OK;
+}
+
+// KB nonlocal atomic forces of the filtered orbitals of chemical potential
+// imu (calcEnergyForce, stodft/calc-nuclei-force.c:33-480, its nonlocal part:
+// calcNlPseudoPostScf then occNumber / numStateStoUp).  dZ/dR_d is the
+// projection of i G_d c, so the force takes the same projection GEMM as H c:
+// once on c (Z, kept) and once per direction; a per-atom reduction in fixed
+// order forms F = -2 sum w Z dZ.
+extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_total, double *fatm,
+                                 double *energy_pnl) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nstate < 1 || nstate > ctx->filtered || imu < 0 || imu >= ctx->acc_nmu)
+    return set_error(SDFT_ERR_STATE, "nl_force_dev: no filtered orbitals");
+  if (nsto_total < 1 || !fatm) return set_error(SDFT_ERR_ARG, "nl_force_dev: bad argument");
+  if (ctx->P == 0) {
+    if (energy_pnl) *energy_pnl = 0.0;
+    return SDFT_OK;
+  }
+  cudaSetDevice(ctx->device);
+  int r;
+  const size_t zel = (size_t)ctx->s_pad * ctx->Ppad;
+  if (!ctx->d_zsave && (r = dmalloc(ctx, (void **)&ctx->d_zsave, zel * sizeof(double)))) return r;
+  double *d_f = nullptr;
+  if ((r = dev_alloc(ctx->device, ctx->st, (void **)&d_f, (size_t)3 * ctx->kb_natm * sizeof(double)))) return r;
+  const double *v = ctx->d_acc + (size_t)imu * ctx->vec_elems;
+  const double scale = occ / (double)nsto_total;
+  double en = 0.0;
+  std::vector<double> h((size_t)3 * ctx->kb_natm);
+  cudaError_t e = cudaSuccess;
+#define CKG(call)                       \
+  do {                                  \
+    if ((e = (call)) != cudaSuccess) goto out; \
+  } while (0)
+  if ((r = run_kb(ctx, v, nstate, true, false))) goto out;
+  CKG(cudaMemcpyAsync(ctx->d_zsave, ctx->d_z, (size_t)nstate * ctx->Ppad * sizeof(double), cudaMemcpyDeviceToDevice,
+                      ctx->st));
+  CKG(cudaMemcpyAsync(&en, ctx->d_enl, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  for (int d = 0; d < 3; d++) {
+    // i G_d c into the back-projection buffer, which this call does not otherwise use
+    launch_dcoef(v, nstate, ctx->ncoef, ctx->ngp, ctx->d_gk + (size_t)d * ctx->ngp, ctx->d_fnl, ctx->st);
+    ctx->launches++;
+    if ((r = run_kb(ctx, ctx->d_fnl, nstate, false, false))) goto out;
+    launch_nl_force_atoms(ctx->d_zsave, ctx->d_z, ctx->Ppad, ctx->d_w, ctx->d_kb_rs, ctx->d_kb_rc, ctx->kb_natm,
+                          nstate, scale, d, d_f, ctx->st);
+    ctx->launches++;
+  }
+  CKG(cudaMemcpyAsync(h.data(), d_f, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CKG(cudaGetLastError());
+  CKG(cudaStreamSynchronize(ctx->st));
+  std::memcpy(fatm, h.data(), h.size() * sizeof(double));
+  if (energy_pnl) *energy_pnl = scale * en;
+out:
+  dev_free(d_f, ctx->st);
+  if (!r && e != cudaSuccess) r = set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
+  return r;
+#undef CKG
 }
 
 extern "C" int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split) {

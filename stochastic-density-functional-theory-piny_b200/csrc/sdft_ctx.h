@@ -33,6 +33,11 @@ struct sdft_ctx {
   // KB
   int P = 0, Ppad = 0, Mpad2 = 0;
   double *d_pj = nullptr, *d_bk = nullptr, *d_w = nullptr, *d_z = nullptr, *d_zwork = nullptr;
+  // KB atomic forces: projector rows of each atom, G (cartesian, per coefficient), saved Z
+  int kb_natm = 0;
+  int *d_kb_rs = nullptr, *d_kb_rc = nullptr;
+  double *d_gk = nullptr;  // [3][ngp], G = 0 and padding 0
+  double *d_zsave = nullptr;
   size_t zwork_elems = 0;
   // orbital blocks
   double *d_chi = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_fnl = nullptr;

@@ -158,7 +158,7 @@ using namespace sdft;
 
 int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   // release a previous projector set
-  double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl};
+  double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl, &ctx->d_gk, &ctx->d_zsave};
   for (double **p : old)
     if (*p) { dev_free(*p, ctx->st); *p = nullptr; }
   void *oldo[] = {ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig, ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc,
@@ -168,6 +168,10 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->d_pj_sc = ctx->d_bk_sc = ctx->d_c_sc = ctx->d_z_sc = nullptr;
   ctx->d_rowmax = nullptr;
   ctx->d_oz_part = nullptr;
+  dev_free(ctx->d_kb_rs, ctx->st);
+  dev_free(ctx->d_kb_rc, ctx->st);
+  ctx->d_kb_rs = ctx->d_kb_rc = nullptr;
+  ctx->kb_natm = 0;
   ctx->P = 0;
   ctx->oz = false;
   if (!kb || kb->natm == 0) return SDFT_OK;
@@ -207,6 +211,7 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   // per-G tables
   std::vector<int> kv(3 * ncoef);
   std::vector<double> vtab((size_t)kb->ntype * lmax1 * ncoef, 0.0), ylm((size_t)10 * ncoef * 2, 0.0);
+  std::vector<double> gk((size_t)3 * ngp, 0.0);
   const double tpi = 2.0 * M_PI;
   for (int g = 0; g < ncoef; g++) {
     kv[3 * g] = ctx->ka[g]; kv[3 * g + 1] = ctx->kb[g]; kv[3 * g + 2] = ctx->kc[g];
@@ -216,6 +221,7 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     const double yk = (aka * hi[3] + akb * hi[4] + akc * hi[5]) * tpi;
     const double zk = (aka * hi[6] + akb * hi[7] + akc * hi[8]) * tpi;
     const double gg = std::sqrt(xk * xk + yk * yk + zk * zk);
+    gk[g] = xk; gk[(size_t)ngp + g] = yk; gk[(size_t)2 * ngp + g] = zk;
     double yr[10], yi[10];
     ylm_host(xk, yk, zk, gg, yr, yi);
     for (int i = 0; i < 10; i++) {
@@ -252,7 +258,13 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     ctx->zwork_elems = (size_t)16 * ctx->s_pad * Ppad;
     if ((r = dmalloc(ctx, (void **)&ctx->d_zwork, ctx->zwork_elems * sizeof(double)))) return r;
     if ((r = dmalloc(ctx, (void **)&ctx->d_fnl, ctx->vec_elems * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_gk, gk.size() * sizeof(double)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_kb_rs, rstart.size() * sizeof(int)))) return r;
+    if ((r = dmalloc(ctx, (void **)&ctx->d_kb_rc, rcount.size() * sizeof(int)))) return r;
   }
+  CKB(cudaMemcpyAsync(ctx->d_gk, gk.data(), gk.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(ctx->d_kb_rs, rstart.data(), rstart.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CKB(cudaMemcpyAsync(ctx->d_kb_rc, rcount.data(), rcount.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
   CKB(cudaMemsetAsync(ctx->d_pj, 0, (size_t)Ppad * K1 * sizeof(double), ctx->st));
   CKB(cudaMemsetAsync(ctx->d_bk, 0, (size_t)Mpad2 * Ppad * sizeof(double), ctx->st));
   CKB(cudaMemsetAsync(ctx->d_z, 0, (size_t)ctx->s_pad * Ppad * sizeof(double), ctx->st));
@@ -283,6 +295,7 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     CKB(cudaStreamSynchronize(ctx->st));
   }
   ctx->P = P;
+  ctx->kb_natm = kb->natm;
   ctx->Ppad = Ppad;
   ctx->Mpad2 = Mpad2;
   if ((ctx->prec == SDFT_PREC_MIXED || ctx->prec == SDFT_PREC_MIXED_FAST) && gemm_oz_available()) {

@@ -1,11 +1,12 @@
 // sdft_lanczos.cu -- vector kernels of the device Lanczos bounds and of the
-// filtered-orbital energies.
+// filtered-orbital energies and KB atomic forces.
 //
 // Vectors are one orbital row of the context layout: re[0, ncoef) then
 // im[0, ncoef) at offset ngp; G0 is entry ncoef - 1.  Reductions are
 // deterministic: kRedBlocks fixed block partials, each a fixed-order tree,
 // summed in block order by one thread.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "sdft_lanczos.h"
 
 namespace sdft {
@@ -104,6 +105,49 @@ __global__ void __launch_bounds__(kRedThreads) k_ekin_part(const double *__restr
   block_sum_to(s, part + blockIdx.x);
 }
 
+// i G_d c: the orbital whose KB projection is dZ/dR_d (get_nlmat,
+// energy/cp/cp_energy_eext_nonloc.c:648-748, accumulates the same sums with
+// the factor G_d and the Re/Im roles swapped)
+__global__ void k_dcoef(const double *__restrict__ v, int nstate, int ncoef, int ngp, const double *__restrict__ gk,
+                        double *__restrict__ out) {
+  const long long tot = (long long)nstate * ngp;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+    const int st = (int)(i / ngp), g = (int)(i - (long long)st * ngp);
+    const double *row = v + (size_t)st * 2 * ngp;
+    double *o = out + (size_t)st * 2 * ngp;
+    const double k = (g < ncoef - 1) ? gk[g] : 0.0;
+    const double re = (g < ncoef - 1) ? row[g] : 0.0, im = (g < ncoef - 1) ? row[ngp + g] : 0.0;
+    o[g] = -k * im;
+    o[ngp + g] = k * re;
+  }
+}
+
+// one block per atom: the force component d of getnl_pot_pv_fatm ->
+// sumnl_pot_pv_fatm_hess (cp_energy_eext_nonloc.c:1473-1500) over the merged
+// projector rows (w carries vnorm / vol and the doubled weight of a merged
+// conjugate pair, whose dZ obeys the same pairing as Z)
+__global__ void __launch_bounds__(kRedThreads) k_nl_force_atoms(const double *__restrict__ Z0,
+                                                                const double *__restrict__ Zd, int ldz,
+                                                                const double *__restrict__ w,
+                                                                const int *__restrict__ rs,
+                                                                const int *__restrict__ rc, int nstate, double scale,
+                                                                int d, double *__restrict__ f) {
+  const int a = blockIdx.x, u0 = rs[a], nu = rc[a];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nu * nstate; i += kRedThreads) {
+    const int s = i / nu, u = u0 + (i - s * nu);
+    acc += w[u] * Z0[(size_t)s * ldz + u] * Zd[(size_t)s * ldz + u];
+  }
+  __shared__ double sh[kRedThreads];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int h = kRedThreads / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) f[3 * a + d] = -2.0 * scale * sh[0];
+}
+
 inline int grid_for(int n) {
   int b = (n + 255) / 256;
   return b < 1 ? 1 : (b > 1024 ? 1024 : b);
@@ -138,6 +182,18 @@ void launch_ekin(const double *v, int nstate, int ncoef, int ngp, const double *
                  cudaStream_t st) {
   k_ekin_part<<<kRedBlocks, kRedThreads, 0, st>>>(v, nstate, ncoef, ngp, ak2, part);
   k_sum_fixed<<<1, 32, 0, st>>>(part, kRedBlocks, out);
+}
+
+void launch_dcoef(const double *v, int nstate, int ncoef, int ngp, const double *gk, double *out, cudaStream_t st) {
+  const long long tot = (long long)nstate * ngp;
+  const int b = (int)std::min<long long>(4 * 148, (tot + 255) / 256);
+  k_dcoef<<<b < 1 ? 1 : b, 256, 0, st>>>(v, nstate, ncoef, ngp, gk, out);
+}
+
+void launch_nl_force_atoms(const double *Z0, const double *Zd, int ldz, const double *w, const int *row_start,
+                           const int *row_count, int natm, int nstate, double scale, int d, double *f,
+                           cudaStream_t st) {
+  k_nl_force_atoms<<<natm, kRedThreads, 0, st>>>(Z0, Zd, ldz, w, row_start, row_count, nstate, scale, d, f);
 }
 
 // Extreme eigenvalues of the symmetric tridiagonal matrix (diagonal a[0..n),

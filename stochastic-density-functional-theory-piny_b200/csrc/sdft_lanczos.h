@@ -23,6 +23,13 @@ void launch_lz_div(double *c, const double *nrm2, int ncoef, int ngp, cudaStream
 // *out = sum over nstate rows, G != G0 of 2 ak2 (re^2 + im^2)
 void launch_ekin(const double *v, int nstate, int ncoef, int ngp, const double *ak2, double *part, double *out,
                  cudaStream_t st);
+// out = i G_d v per row (Re out = -G_d Im v, Im out = G_d Re v; G = 0 and
+// the row padding [ncoef, ngp) zero); gk: G_d per coefficient
+void launch_dcoef(const double *v, int nstate, int ncoef, int ngp, const double *gk, double *out, cudaStream_t st);
+// f[3 a + d] = -2 scale sum_{state, u in rows of atom a} w[u] Z0[s][u] Zd[s][u]
+void launch_nl_force_atoms(const double *Z0, const double *Zd, int ldz, const double *w, const int *row_start,
+                           const int *row_count, int natm, int nstate, double scale, int d, double *f,
+                           cudaStream_t st);
 // smallest and largest eigenvalue of the symmetric tridiagonal matrix
 // (diagonal a[0..n), off-diagonal b[0..n-1)), by Sturm bisection (host)
 void tridiag_extremes(const double *a, const double *b, int n, double *lo, double *hi);

@@ -4,7 +4,8 @@ Runs in the build container, where the reference tree exists and
 oracle/build_ref.sh has produced oracle/_ref/libpinyref.so (the reference's
 filter.c, normh.c, density.c, gen-noise.c, calc-chempot-chebyshev.c,
 coeff.c, ... compiled in place).  The fixture pins the oracle and the CUDA
-path on machines without the reference tree.
+path on machines without the reference tree (hpsi, the KB atomic forces of
+calcNlPseudoPostScf, filters, moments, coefficients, noise and density).
 
   python tests/golden/make_golden.py
 
@@ -43,6 +44,8 @@ def main():
     out.update(in_re=cr, in_im=ci)
     fr, fi, e = r.hpsi(cr, ci)
     out.update(hpsi_re=fr, hpsi_im=fi, hpsi_enl=np.array(e))
+    fa, ea = r.nl_force(cr, ci)  # calcNlPseudoPostScf: raw KB atomic forces and energy
+    out.update(nlforce=fa, nlforce_enl=np.array(ea))
     scale, em = 2.0 / (EMAX - EMIN), 0.5 * (EMAX + EMIN)
     mus = (0.2, 0.35)
     ec = np.stack([pkg.calcChebyCoeff(20, EMAX - EMIN, em, 1000.0, mu) for mu in mus], axis=1).ravel()

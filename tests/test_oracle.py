@@ -110,3 +110,27 @@ def test_chempot_bisection_monotone(pkg):
     n_lo = pkg.calcNumElecCheby(L, ed, em, 50.0, mu - 0.05, 2.0, m)
     n_hi = pkg.calcNumElecCheby(L, ed, em, 50.0, mu + 0.05, 2.0, m)
     assert n_lo < 40.0 < n_hi
+
+
+def test_oracle_nl_force_is_minus_energy_gradient(sys1):
+    """F_a = -dE_NL/dR_a by central differences (h = 1e-5 bohr) on a few
+    coordinates: the force sums are the derivative of the energy sums."""
+    ns, nc = 3, sys1["ncoef"]
+    rng = np.random.default_rng(5)
+    cr, ci = rng.standard_normal(ns * nc), rng.standard_normal(ns * nc)
+    ci.reshape(ns, nc)[:, -1] = 0.0
+    f, _ = O.OracleSys(sys1).nl_force(cr, ci)
+    p0 = np.asarray(sys1["kb_desc"]["pos"], float).reshape(-1)
+
+    def energy(pos):
+        s2 = dict(sys1)
+        s2["kb_desc"] = dict(sys1["kb_desc"], pos=pos)
+        return O.OracleSys(s2).nl_force(cr, ci)[1]
+
+    h = 1e-5
+    for a, d in ((0, 1), (3, 0), (5, 2)):
+        pp, pm = p0.copy(), p0.copy()
+        pp[3 * a + d] += h
+        pm[3 * a + d] -= h
+        fd = -(energy(pp) - energy(pm)) / (2 * h)
+        assert abs(fd - f[a, d]) < 1e-6 * np.abs(f).max()

@@ -47,6 +47,18 @@ def test_hpsi_pinned(both, sys1, ns):
     assert abs(ge - e) < 1e-13 * abs(e)
 
 
+@pytest.mark.parametrize("ns", [1, 5])
+def test_nl_force_pinned(both, sys1, ns):
+    """KB atomic forces: calcNlPseudoPostScf (control_ewd_non_loc / get_nlmat,
+    getnl_pot_pv_fatm) against the oracle's restatement."""
+    r, o = both
+    cr, ci = _rand(sys1["ncoef"], ns, 40 + ns)
+    fr, er = r.nl_force(cr, ci)
+    fo, eo = o.nl_force(cr, ci)
+    assert np.abs(fo - fr).max() < 1e-13 * np.abs(fr).max()
+    assert abs(eo - er) < 1e-13 * abs(er)
+
+
 def test_filter_cheby_pinned(pkg, both, sys1):
     r, o = both
     cr, ci = _rand(sys1["ncoef"], 5, 3)

@@ -2,8 +2,10 @@
 
 Each rank draws its own noise (np_states = 2, myid = rank), takes moments
 and the stochastic density of its orbitals with the CPU oracle, and sums
-them over the ranks with StateGroup; rank 0 checks the sums and the
-chemical potential against a single-process run over both ranks' orbitals.
+them over the ranks with StateGroup; rank 0 checks the sums, the chemical
+potential and the KB atomic forces (each rank's orbitals, summed as
+calcEnergyForce reduces them over comm_states) against a single-process run
+over both ranks' orbitals.
 """
 import os
 import socket
@@ -48,8 +50,10 @@ def _rank_main(rank, world, port, out_path):
         mom = o.moments(cr, ci, L, scale, em)
         mu, ne = grp.chem_pot(pkg, mom, 2 * NLOC, L, EMAX - EMIN, em, wl.BETA, wl.OCC, s["num_elec"], 0.2, 0.05)
         rho = grp.sum_array(o.density(cr, ci))
+        fa, _ = o.nl_force(cr, ci)
+        fa = grp.sum_array(fa * wl.OCC / (2 * NLOC))
         if rank == 0:
-            np.savez(out_path, mom=grp.sum_array(mom), mu=mu, ne=ne, rho=rho)
+            np.savez(out_path, mom=grp.sum_array(mom), mu=mu, ne=ne, rho=rho, force=fa)
         else:
             grp.sum_array(mom)
     finally:
@@ -67,10 +71,15 @@ def test_two_state_ranks_match_one_process(tmp_path, pkg, wl):
     scale, em = 2.0 / (EMAX - EMIN), 0.5 * (EMAX + EMIN)
     mom = np.zeros(L + 1)
     rho = np.zeros(int(np.prod(s["grid"])))
+    crs, cis = [], []
     for r in range(2):
         cr, ci = o.noise(NLOC, 10.0, np_states=2, myid=r)
         mom += o.moments(cr, ci, L, scale, em)
         rho += o.density(cr, ci)
+        crs.append(cr)
+        cis.append(ci)
+    force = o.nl_force(np.concatenate(crs), np.concatenate(cis))[0] * wl.OCC / (2 * NLOC)
+    assert np.abs(got["force"] - force).max() < 1e-13 * np.abs(force).max()
     mu, ne = pkg.calcChemPotCheby(L, EMAX - EMIN, em, wl.BETA, wl.OCC, mom / (2 * NLOC), s["num_elec"], 0.2, 0.05)
     assert np.allclose(got["mom"], mom, rtol=1e-13, atol=0)
     assert np.allclose(got["rho"], rho, rtol=1e-13, atol=1e-13 * np.abs(rho).max())

@@ -34,3 +34,28 @@ done
 gcc -c $CFLAGS $INC "$HERE/ref_harness.c" -o "$OUT/obj/ref_harness.o"
 gcc -shared -o "$OUT/libpinyref.so" $OBJS "$OUT/obj/ref_harness.o" -lm
 echo "$OUT/libpinyref.so"
+
+# The product's PINY adapter (csrc/piny/sdft_piny_adapter.c), compiled against
+# the reference headers and linked in place of the reference routines it
+# replaces: the same objects with those definitions made weak, the same
+# harness, and lib/libsdft_b200.so.  The reference's own callers (the
+# harness drives them) then run on the device path.
+PKG="$(cd "$HERE/.." && pwd)/stochastic-density-functional-theory-piny_b200"
+if [ -f "$PKG/lib/libsdft_b200.so" ]; then
+  mkdir -p "$OUT/obj_adapter"
+  WEAK=""
+  for sym in filterChebyPolyHerm filterNewtonPolyHerm normHCheby normHNewtonHerm calcChebyMoments \
+             calcCoefForceWrapSCF rhoCalcRealStoHybrid; do WEAK="$WEAK --weaken-symbol=$sym"; done
+  AOBJS=""
+  for o in $OBJS; do
+    w="$OUT/obj_adapter/$(basename "$o")"
+    objcopy $WEAK "$o" "$w"
+    AOBJS="$AOBJS $w"
+  done
+  gcc -c $CFLAGS -DSDFT_PINY_ADAPTER $INC -I"$REF/stodft" -I"$HERE/../include" \
+      "$PKG/csrc/piny/sdft_piny_adapter.c" -o "$OUT/obj_adapter/sdft_piny_adapter.o"
+  gcc -shared -o "$OUT/libpinyref_adapter.so" $AOBJS "$OUT/obj/ref_harness.o" \
+      "$OUT/obj_adapter/sdft_piny_adapter.o" -L"$PKG/lib" -lsdft_b200 \
+      -Wl,-rpath,'$ORIGIN/../../stochastic-density-functional-theory-piny_b200/lib' -lm
+  echo "$OUT/libpinyref_adapter.so"
+fi

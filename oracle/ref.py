@@ -9,19 +9,22 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libpinyref.so")
+# the same reference objects and harness with the product's PINY adapter
+# linked in place of the routines it replaces (oracle/build_ref.sh)
+LIB_ADAPTER = os.path.join(HERE, "_ref", "libpinyref_adapter.so")
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
-_lib = None
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB)
+def available(adapter=False):
+    return os.path.exists(LIB_ADAPTER if adapter else LIB)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        L = C.CDLL(LIB)
+def lib(adapter=False):
+    path = LIB_ADAPTER if adapter else LIB
+    if path not in _libs:
+        L = C.CDLL(path)
         L.ref_create.restype = C.c_void_p
         L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int, _dp,
                                  C.c_int, C.c_double, C.c_double, _dp, _dp, C.c_double, C.c_int]
@@ -44,8 +47,8 @@ def lib():
         L.ref_mix_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]
         L.ref_mix_checkpoint.restype = C.c_int
         L.ref_xc_lda.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, _dp, _dp]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _d(a):
@@ -67,7 +70,10 @@ def i32(a):
 class RefSys:
     """One system in the reference's own data structures (single type, s+p KB)."""
 
-    def __init__(self, s, nmax):
+    def __init__(self, s, nmax, adapter=False):
+        """adapter: drive the product's PINY adapter (device path) through
+        the same reference structures and callers."""
+        self._L = lib(adapter)
         kb = s["kb_desc"]
         self.ncoef = len(s["ka"])
         self.N = int(np.prod(s["grid"]))
@@ -76,7 +82,7 @@ class RefSys:
                      f64(np.asarray(s["hmat"], float).T.reshape(9)), f64(s["vks"]), f64(kb["pos"]), f64(kb["vps"]),
                      f64(kb["vpsnorm"])]
         ka, kb_, kc, b1, b2, h, v, pos, vps, vn = self.keep
-        self._p = C.c_void_p(lib().ref_create(*s["grid"], self.ncoef, _i(ka), _i(kb_), _i(kc), _i(b1), _i(b2), _d(h),
+        self._p = C.c_void_p(self._L.ref_create(*s["grid"], self.ncoef, _i(ka), _i(kb_), _i(kc), _i(b1), _i(b2), _d(h),
                                               _d(v), kb["natm"], _d(pos), kb["nsplin_g"], kb["gmin_spl"],
                                               kb["dg_spl"], _d(vps), _d(vn), float(kb["gzvps0"][0]), nmax))
 
@@ -84,7 +90,7 @@ class RefSys:
         cre, cim = f64(cre), f64(cim)
         fr, fi = np.zeros_like(cre), np.zeros_like(cim)
         e = C.c_double()
-        lib().ref_hpsi(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e))
+        self._L.ref_hpsi(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(fr), _d(fi), C.byref(e))
         return fr, fi, e.value
 
     def nl_force(self, cre, cim):
@@ -93,7 +99,7 @@ class RefSys:
         cre, cim = f64(cre), f64(cim)
         f = np.zeros(3 * self.natm)
         e = C.c_double()
-        lib().ref_nl_force(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(f), C.byref(e))
+        self._L.ref_nl_force(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(f), C.byref(e))
         return f.reshape(self.natm, 3), e.value
 
     def filter(self, cheby, cre, cim, ec, nmu, scale, emean, samp=None, moments=False):
@@ -102,7 +108,7 @@ class RefSys:
         sr, si = np.zeros(nmu * cre.size), np.zeros(nmu * cre.size)
         m = np.zeros(L + 1) if moments else None
         sp = f64(samp) if samp is not None else None
-        lib().ref_filter(self._p, 1 if cheby else 0, cre.size // self.ncoef, _d(cre), _d(cim), L, nmu, _d(ec),
+        self._L.ref_filter(self._p, 1 if cheby else 0, cre.size // self.ncoef, _d(cre), _d(cim), L, nmu, _d(ec),
                          _d(sp) if sp is not None else None, scale, emean, _d(sr), _d(si),
                          _d(m) if m is not None else None)
         out = (sr.reshape(nmu, -1), si.reshape(nmu, -1))
@@ -111,19 +117,19 @@ class RefSys:
     def noise(self, nstate, seed=10.0):
         re = np.zeros(nstate * self.ncoef)
         im = np.zeros(nstate * self.ncoef)
-        lib().ref_noise(self._p, nstate, seed, _d(re), _d(im))
+        self._L.ref_noise(self._p, nstate, seed, _d(re), _d(im))
         return re, im
 
     def density(self, cre, cim):
         cre, cim = f64(cre), f64(cim)
         rho = np.zeros(self.N)
-        lib().ref_density(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(rho))
+        self._L.ref_density(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(rho))
         return rho
 
     def moments(self, cre, cim, L, scale, emean):
         cre, cim = f64(cre), f64(cim)
         m = np.zeros(L + 1)
-        lib().ref_moments(self._p, cre.size // self.ncoef, _d(cre), _d(cim), L, scale, emean, _d(m))
+        self._L.ref_moments(self._p, cre.size // self.ncoef, _d(cre), _d(cim), L, scale, emean, _d(m))
         return m
 
 

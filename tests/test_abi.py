@@ -34,3 +34,37 @@ def test_no_device_is_reported_cleanly(pkg, sys1):
 def test_host_validation(pkg):
     with pytest.raises(pkg.SdftError):
         pkg.calcChebyCoeff(0, 1.0, 0.0, 1000.0, 0.0)
+
+
+ADAPTED = ("filterChebyPolyHerm", "filterNewtonPolyHerm", "normHCheby", "normHNewtonHerm", "calcChebyMoments",
+           "calcCoefForceWrapSCF", "rhoCalcRealStoHybrid")
+
+
+def test_piny_adapter_source_is_guarded():
+    """Without -DSDFT_PINY_ADAPTER the adapter translation unit is empty, so a
+    build without a PINY tree never needs PINY's headers."""
+    src = open(os.path.join(ROOT, "stochastic-density-functional-theory-piny_b200", "csrc", "piny",
+                            "sdft_piny_adapter.c")).read()
+    body = re.sub(r"/\*.*?\*/", "", src, flags=re.S).strip()
+    assert body.startswith("#ifdef SDFT_PINY_ADAPTER") and body.endswith("#endif")
+    for name in ADAPTED:
+        assert re.search(r"\nvoid " + name + r"\(", src), name
+
+
+def test_piny_adapter_replaces_the_reference_definitions():
+    """In the adapter test library (reference objects + adapter), each
+    replaced routine has exactly one strong definition: the adapter's."""
+    import subprocess
+    path = os.path.join(ROOT, "oracle", "_ref", "libpinyref_adapter.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref/libpinyref_adapter.so not built (needs the reference tree at build time)")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    kinds = {}
+    for line in out.splitlines():
+        parts = line.split()
+        if len(parts) == 3:
+            kinds.setdefault(parts[2], []).append(parts[1])
+    for name in ADAPTED:
+        assert kinds.get(name) == ["T"], (name, kinds.get(name))
+    # the library loads (the device library is found through its runpath)
+    ctypes.CDLL(path)

@@ -433,12 +433,29 @@ def run_ours(args):
                                      hi.reshape(ns, nc)[j]) for j in range(ns))
             return e * wl.OCC / (nsto * world)
         e64, em = band_energy(fr, fi), band_energy(mr, mi)
+
+        # nonlocal atomic forces of the same filtered orbitals (calcEnergyForce's
+        # KB part: four projection GEMMs), device time of one call per precision
+        def force_ms(c):
+            st = torch.cuda.ExternalStream(pkg.lib.sdft_ctx_stream(c._p), device=f"cuda:{local}")
+            c.nl_force_dev(nsto, 0, occ=wl.OCC, nsto_total=nsto * world)  # warm-up (allocates Z scratch)
+            ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ea.record(st)
+            f, _ = c.nl_force_dev(nsto, 0, occ=wl.OCC, nsto_total=nsto * world)
+            eb.record(st)
+            eb.synchronize()
+            return f, ea.elapsed_time(eb)
+        f64f, fms64 = force_ms(c64)
+        fmxf, fmsmx = force_ms(ctx)
+        nl_force = {"natm": int(f64f.shape[0]), "ms_fp64": fms64, "ms_mixed": fmsmx,
+                    "max_abs_err_mixed_vs_fp64_over_max_force":
+                        float(np.abs(fmxf - f64f).max() / max(1e-300, np.abs(f64f).max())) if f64f.size else 0.0}
         fp64 = {"orbitals_per_s": nsto * world / (ms64 / 1e3), "ms_per_step": ms64,
                 "mixed_speedup": (nsto * world / (ms64 / 1e3)) and value / (nsto * world / (ms64 / 1e3)),
                 "density_rel_l2_mixed_vs_fp64": float(np.linalg.norm(rhom - rho64) / np.linalg.norm(rho64)),
                 "band_energy_fp64": e64, "band_energy_mixed": em,
                 "energy_rel_err_mixed_vs_fp64": abs(em - e64) / abs(e64),
-                "num_elec_density": float(rho64.sum() / rho64.size)}
+                "num_elec_density": float(rho64.sum() / rho64.size), "nl_force": nl_force}
         c64.close()
 
     # ---- roofline: per kernel function, the dominant one first

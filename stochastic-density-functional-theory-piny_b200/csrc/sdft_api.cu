@@ -1198,7 +1198,10 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
   cudaSetDevice(ctx->device);
   int r;
   const size_t zel = (size_t)ctx->s_pad * ctx->Ppad;
-  if (!ctx->d_zsave && (r = dmalloc(ctx, (void **)&ctx->d_zsave, zel * sizeof(double)))) return r;
+  if (!ctx->d_zsave) {
+    if ((r = dmalloc(ctx, (void **)&ctx->d_zsave, zel * sizeof(double)))) return r;
+    ctx->kb_bytes += (long long)(zel * sizeof(double));  // released with the KB buffers
+  }
   double *d_f = nullptr;
   if ((r = dev_alloc(ctx->device, ctx->st, (void **)&d_f, (size_t)3 * ctx->kb_natm * sizeof(double)))) return r;
   const double *v = ctx->d_acc + (size_t)imu * ctx->vec_elems;

@@ -65,6 +65,7 @@ struct sdft_ctx {
   int filtered = 0;          // orbitals with results in d_acc
   long long launches = 0;
   long long dev_bytes = 0;
+  long long kb_bytes = 0;  // the part of dev_bytes held by the KB buffers (released by a rebuild)
   double gcut = 0.0;
   bool fast = false;  // compile-time-edge FFT kernels available
   bool fft64 = true;  // FFT scratch / V_KS in FP64 (plain form)

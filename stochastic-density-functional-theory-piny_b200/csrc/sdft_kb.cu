@@ -174,7 +174,15 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->kb_natm = 0;
   ctx->P = 0;
   ctx->oz = false;
+  ctx->dev_bytes -= ctx->kb_bytes;
+  ctx->kb_bytes = 0;
   if (!kb || kb->natm == 0) return SDFT_OK;
+  // whatever this build leaves allocated counts as KB bytes, on every return path
+  struct KbBytes {
+    sdft_ctx *c;
+    long long before;
+    ~KbBytes() { c->kb_bytes = c->dev_bytes - before; }
+  } kb_guard{ctx, ctx->dev_bytes};
   if (!kb->pos || !kb->type || !kb->lmax_type || !kb->vps || !kb->vpsnorm || !kb->gzvps0 || kb->ntype < 1 ||
       kb->nsplin_g < 1 || kb->dg_spl <= 0.0)
     return set_error(SDFT_ERR_ARG, "set_kb: incomplete projector description");

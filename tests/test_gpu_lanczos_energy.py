@@ -121,6 +121,8 @@ def test_nl_force_is_energy_gradient_64_atoms(pkg, wl, sys2):
     s, ns = sys2, 8
     ctx, *_ = _filtered_ctx(pkg, wl, s, pkg.SDFT_PREC_FP64, ns, 7, L=16)
     try:
+        ctx.energy_chempot_dev(ns, 0, occ=2.0, nsto_total=ns)  # allocates its reduction scratch
+        b0 = ctx.device_bytes
         f, _ = ctx.nl_force_dev(ns, 0, occ=2.0, nsto_total=ns)
         p0 = np.asarray(s["kb_desc"]["pos"], float).reshape(-1)
         h = 1e-4
@@ -133,6 +135,8 @@ def test_nl_force_is_energy_gradient_64_atoms(pkg, wl, sys2):
                 e.append(ctx.energy_chempot_dev(ns, 0, occ=2.0, nsto_total=ns)[1])
             fd = -(e[0] - e[1]) / (2 * h)
             assert abs(fd - f[a, d]) <= 1e-6 * np.abs(f).max(), (a, d, fd, f[a, d])
+        # rebuilding the projectors releases the old set (and the force's Z copy)
+        assert ctx.device_bytes == b0
     finally:
         ctx.close()
 

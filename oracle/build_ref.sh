@@ -52,7 +52,9 @@ if [ -f "$PKG/lib/libsdft_b200.so" ]; then
     objcopy $WEAK "$o" "$w"
     AOBJS="$AOBJS $w"
   done
-  gcc -c $CFLAGS -DSDFT_PINY_ADAPTER $INC -I"$REF/stodft" -I"$HERE/../include" \
+  # the harness supplies genNoiseOrbitalReal here (it injects chi into calcChebyMoments);
+  # the adapter's noise is reached through sdft_piny_noise
+  gcc -c $CFLAGS -DSDFT_PINY_ADAPTER -DSDFT_PINY_ADAPTER_NO_NOISE $INC -I"$REF/stodft" -I"$HERE/../include" \
       "$PKG/csrc/piny/sdft_piny_adapter.c" -o "$OUT/obj_adapter/sdft_piny_adapter.o"
   gcc -shared -o "$OUT/libpinyref_adapter.so" $AOBJS "$OUT/obj/ref_harness.o" \
       "$OUT/obj_adapter/sdft_piny_adapter.o" -L"$PKG/lib" -lsdft_b200 \

@@ -39,6 +39,7 @@ def lib(adapter=False):
         L.ref_newton.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.ref_gaussran2.argtypes = [C.c_int, _dp, _dp]
         L.ref_noise.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
+        L.ref_noise_adapter.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
         L.ref_density.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         L.ref_mix_create.restype = C.c_void_p
         L.ref_mix_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
@@ -118,6 +119,15 @@ class RefSys:
         re = np.zeros(nstate * self.ncoef)
         im = np.zeros(nstate * self.ncoef)
         self._L.ref_noise(self._p, nstate, seed, _d(re), _d(im))
+        return re, im
+
+    def noise_adapter(self, nstate, seed=10.0):
+        """The product adapter's genNoiseOrbitalReal on these structures
+        (adapter library only)."""
+        re = np.zeros(nstate * self.ncoef)
+        im = np.zeros(nstate * self.ncoef)
+        if self._L.ref_noise_adapter(self._p, nstate, seed, _d(re), _d(im)) != 0:
+            raise RuntimeError("the adapter's noise is only in the adapter library")
         return re, im
 
     def density(self, cre, cim):

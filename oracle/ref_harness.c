@@ -541,6 +541,20 @@ int ref_noise(RefSys *r, int ns, double seed, double *re, double *im) {
   return 0;
 }
 
+/* The product adapter's genNoiseOrbitalReal body (present only in the
+ * adapter test library) on the same structures as ref_noise. */
+void sdft_piny_noise(CP *, CPCOEFFS_POS *) __attribute__((weak));
+int ref_noise_adapter(RefSys *r, int ns, double seed, double *re, double *im) {
+  if (!sdft_piny_noise) return -1;
+  r->cp.cpcoeffs_info.nstate_up_proc = ns;
+  r->cp.cpcoeffs_info.nstate_up = ns;
+  r->sinfo.randSeed = seed;
+  sdft_piny_noise(&r->cp, &r->cpos);
+  memcpy(re, &r->cpos.cre_up[1], sizeof(double) * ns * r->ncoef);
+  memcpy(im, &r->cpos.cim_up[1], sizeof(double) * ns * r->ncoef);
+  return 0;
+}
+
 /* rhoCalcRealStoHybrid (stodft/density.c:43): sum_s |psi_s(r)|^2 */
 int ref_density(RefSys *r, int ns, const double *re, const double *im, double *rho) {
   load_states(r, ns, re, im);

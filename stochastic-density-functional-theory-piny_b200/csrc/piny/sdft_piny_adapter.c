@@ -10,6 +10,8 @@
  *   calcChebyMoments       stodft/calc-chempot-chebyshev.c:596
  *   calcCoefForceWrapSCF   stodft/reduced-energy/energy-wrapper-scf.c:1066
  *   rhoCalcRealStoHybrid   stodft/density.c:43
+ *   genNoiseOrbitalReal    stodft/gen-noise.c:162  (unless SDFT_PINY_ADAPTER_NO_NOISE;
+ *                          its body is also sdft_piny_noise)
  *
  * and leaves every caller unchanged.  The file is empty unless compiled with
  * -DSDFT_PINY_ADAPTER and a PINY tree on the include path:
@@ -27,11 +29,14 @@
  * kinetic cap from cpewald->gCutoffKe (when eCutoffKe >= 0), V_KS from
  * cpscr_rho.v_ks_up, Kleinman-Bylander tables from cp->pseudo and the atom
  * maps.  Later calls upload V_KS again only when it changed and rebuild the
- * projectors only when an atom moved.  The context grows when a call brings
- * more orbitals than it was made for.
+ * projectors only when an atom moved.  The context is made for this rank's
+ * share of the orbitals (nstate_up / np_states, or more when a call brings
+ * more; the spectral range runs with nstate_up_proc = 1) and grows when a
+ * call that carries the CLASS brings more than it holds.
  *
  * Environment: SDFT_PINY_PRECISION = fp64 | mixed (default) | mixed_fast;
- * SDFT_PINY_DEVICE = CUDA device ordinal (default 0).
+ * SDFT_PINY_DEVICE = CUDA device ordinal (default 0); SDFT_PINY_MAX_STATES =
+ * the least number of orbitals a context is made for.
  *
  * Supported as in the product: spin-unpolarised (cp_lsda = 0), one radial KB
  * projector per channel (n_rad_max = 1), l <= 2, the CP box equal to the cell
@@ -42,7 +47,8 @@
  * filterChebyPolyHerm / filterNewtonPolyHerm leave cre_up / cim_up holding
  * the input orbitals (the reference leaves the last polynomial vector
  * there); normHCheby / normHNewtonHerm do not add the KB energy of their
- * H c to stat_avg->cp_enl.
+ * H c to stat_avg->cp_enl; genNoiseOrbitalReal does not leave the per-rank
+ * seeds in stodftInfo->randSeedTot.
  */
 #ifdef SDFT_PINY_ADAPTER
 
@@ -234,8 +240,12 @@ static AdSys *ad_attach(CP *cp, CLASS *cl, GENERAL_DATA *gd, CLATOMS_POS *ap, in
       kc[i] = ew->kcstr_sm[i + 1];
     }
     ka[ncoef - 1] = kb[ncoef - 1] = kc[ncoef - 1] = 0; /* G = 0 last */
-    const char *dv = getenv("SDFT_PINY_DEVICE");
-    const int want = nstate > s->max_states ? nstate : s->max_states;
+    const char *dv = getenv("SDFT_PINY_DEVICE"), *ms = getenv("SDFT_PINY_MAX_STATES");
+    const int np = cp->communicate.np_states > 0 ? cp->communicate.np_states : 1;
+    int want = nstate > s->max_states ? nstate : s->max_states;
+    const int share = (cp->cpcoeffs_info.nstate_up + np - 1) / np;
+    if (share > want) want = share;
+    if (ms && atoi(ms) > want) want = atoi(ms);
     ad_ck(sdft_ctx_create(n1, n2, n3, ncoef, ka, kb, kc, &cell->hmat_cp[1], ad_precision(), want, dv ? atoi(dv) : 0,
                           &s->ctx),
           "sdft_ctx_create");
@@ -363,8 +373,8 @@ void calcChebyMoments(CP *cp, CLASS *class, GENERAL_DATA *general_data, int ip_n
   CPCOEFFS_POS *pos = &cp->cpcoeffs_pos[ip_now];
   const int ns = cp->cpcoeffs_info.nstate_up_proc;
   if (cp->cpopts.cp_lsda != 0) ad_die("calcChebyMoments", "spin-polarised runs (cp_lsda = 1) are not supported");
-  genNoiseOrbitalReal(cp, pos); /* PINY's own noise, as calc-chempot-chebyshev.c:685 */
   AdSys *s = ad_attach(cp, class, general_data, &class->clatoms_pos[ip_now], ns, "calcChebyMoments");
+  genNoiseOrbitalReal(cp, pos); /* the noise as calc-chempot-chebyshev.c:685 draws it */
   ad_ck(sdft_cheby_moments(s->ctx, ns, &pos->cre_up[1], &pos->cim_up[1], si->polynormLength,
                            si->chebyshevInfo->scale, si->energyMean, sp->chebyMomentsUp),
         "calcChebyMoments");
@@ -393,5 +403,28 @@ void rhoCalcRealStoHybrid(CPSCR *cpscr, CPCOEFFS_INFO *cpcoeffs_info, CELL *cell
   }
   ad_ck(sdft_density(s->ctx, nstate, &creal[1], &cimag[1], &rho_scr[1]), "rhoCalcRealStoHybrid");
 }
+
+/* genNoiseOrbitalReal (stodft/gen-noise.c:162-374), spin-unpolarised: the
+ * noise orbitals of state rank myid_state of np_states from
+ * stodftInfo->randSeed, generated on the device (the gaussran2 sign
+ * sequence, +-sqrt(N) in real space, transformed to G).  The signature
+ * carries no cell, so an earlier call with the CLASS must have made the
+ * system's context. */
+void sdft_piny_noise(CP *cp, CPCOEFFS_POS *cpcoeffs_pos) {
+  const int ns = cp->cpcoeffs_info.nstate_up_proc;
+  if (cp->cpopts.cp_lsda != 0) ad_die("genNoiseOrbitalReal", "spin-polarised runs (cp_lsda = 1) are not supported");
+  AdSys *s = ad_find(&cp->cp_sclr_fft_pkg3d_sm);
+  if (!s || !s->ctx)
+    ad_die("genNoiseOrbitalReal", "no device context for this system yet: an H application or filter creates it");
+  if (ns > s->max_states)
+    ad_die("genNoiseOrbitalReal", "more orbitals than the context was made for (set SDFT_PINY_MAX_STATES)");
+  ad_ck(sdft_noise_real(s->ctx, ns, cp->stodftInfo->randSeed, cp->communicate.np_states, cp->communicate.myid_state,
+                        &cpcoeffs_pos->cre_up[1], &cpcoeffs_pos->cim_up[1]),
+        "genNoiseOrbitalReal");
+}
+
+#ifndef SDFT_PINY_ADAPTER_NO_NOISE
+void genNoiseOrbitalReal(CP *cp, CPCOEFFS_POS *cpcoeffs_pos) { sdft_piny_noise(cp, cpcoeffs_pos); }
+#endif
 
 #endif /* SDFT_PINY_ADAPTER */

@@ -47,7 +47,7 @@ def test_piny_adapter_source_is_guarded():
                             "sdft_piny_adapter.c")).read()
     body = re.sub(r"/\*.*?\*/", "", src, flags=re.S).strip()
     assert body.startswith("#ifdef SDFT_PINY_ADAPTER") and body.endswith("#endif")
-    for name in ADAPTED:
+    for name in ADAPTED + ("genNoiseOrbitalReal", "sdft_piny_noise"):
         assert re.search(r"\nvoid " + name + r"\(", src), name
 
 

@@ -3,7 +3,9 @@ sdft_piny_adapter.c) as a drop-in: oracle/build_ref.sh links it into the
 reference's own objects in place of the routines it replaces
 (filterChebyPolyHerm, filterNewtonPolyHerm, normHCheby, normHNewtonHerm,
 calcChebyMoments, calcCoefForceWrapSCF, rhoCalcRealStoHybrid) and the same
-harness drives the reference's structures and callers.  Results are checked
+harness drives the reference's structures and callers.  The harness keeps its
+own genNoiseOrbitalReal there (it injects the orbitals of calcChebyMoments), so
+the adapter's noise is checked through its body, sdft_piny_noise.  Results are checked
 against the golden fixture, which the reference alone produced, in both
 precisions (the adapter reads SDFT_PINY_PRECISION when it creates a
 system's context)."""
@@ -71,6 +73,14 @@ def test_adapter_filters_and_moments(adsys, gold):
     assert rel_l2(_cat(nr[0], ni[0]), _cat(gold["newton_re"], gold["newton_im"])) < t
     m = r.moments(cr, ci, 16, SCALE, EMEAN)
     assert rel_l2(m[:17], gold["moments_L16"][:17]) < t
+
+
+def test_adapter_noise(adsys, gold):
+    """genNoiseOrbitalReal through the adapter: the reference's noise orbitals
+    from randSeed 10 (FP64 transforms in both precisions)."""
+    _, r, _ = adsys
+    nr, ni = r.noise_adapter(4, 10.0)
+    assert rel_l2(_cat(nr, ni), _cat(gold["noise_re"], gold["noise_im"])) < 1e-13
 
 
 def test_adapter_density(adsys, gold):

@@ -60,4 +60,7 @@ if [ -f "$PKG/lib/libsdft_b200.so" ]; then
       "$OUT/obj_adapter/sdft_piny_adapter.o" -L"$PKG/lib" -lsdft_b200 \
       -Wl,-rpath,'$ORIGIN/../../stochastic-density-functional-theory-piny_b200/lib' -lm
   echo "$OUT/libpinyref_adapter.so"
+  # the production form (with genNoiseOrbitalReal) compiles against the same headers
+  gcc -c $CFLAGS -DSDFT_PINY_ADAPTER $INC -I"$REF/stodft" -I"$HERE/../include" \
+      "$PKG/csrc/piny/sdft_piny_adapter.c" -o "$OUT/obj_adapter/sdft_piny_adapter_full.o"
 fi

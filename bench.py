@@ -534,7 +534,7 @@ class RefCpu:
     """The reference's CPU path on all host cores: one process per core, each
     filtering its own 2 orbitals (the reference spreads stochastic orbitals
     over MPI ranks, filter.c / gen-stodft-wf.c), k polynomial steps per
-    round, extrapolated linearly to order L."""
+    call, extrapolated linearly to order L."""
 
     def __init__(self, cfg_name, cores=None):
         import multiprocessing as mp

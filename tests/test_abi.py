@@ -68,3 +68,18 @@ def test_piny_adapter_replaces_the_reference_definitions():
         assert kinds.get(name) == ["T"], (name, kinds.get(name))
     # the library loads (the device library is found through its runpath)
     ctypes.CDLL(path)
+
+
+@pytest.mark.parametrize("grid,prec,ncut,code", [
+    ((25, 24, 24), 0, None, 5),    # an edge that is not 2^a 3^b
+    ((24, 24, 256), 0, None, 5),   # an edge above 128
+    ((24, 24, 24), 7, None, 1),    # no such precision mode
+    ((24, 24, 24), 0, 1, 1),       # a sphere of one coefficient
+])
+def test_context_arguments_checked_before_the_device(pkg, sys1, grid, prec, ncut, code):
+    """Sizes and modes the kernels do not cover are refused on the host, with
+    the reference-style status code, before any device is touched."""
+    ka, kb, kc = (sys1[k][:ncut] if ncut else sys1[k] for k in ("ka", "kb", "kc"))
+    with pytest.raises(pkg.SdftError) as e:
+        pkg.Context(*grid, ka, kb, kc, sys1["hmat"], precision=prec, max_states=2)
+    assert e.value.code == code

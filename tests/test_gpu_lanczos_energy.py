@@ -162,3 +162,26 @@ def test_nl_force_mixed_matches_fp64_64_atoms(pkg, sys2):
     (f64_, e64), (fmx, emx) = out
     assert np.abs(fmx - f64_).max() <= 1e-6 * np.abs(f64_).max()
     assert abs(emx - e64) <= 1e-7 * abs(e64)
+
+
+def test_nl_force_edges(pkg, wl, sys1):
+    """One orbital; no projectors (empty force, zero energy); no filtered
+    orbitals yet (an error, as energy_chempot_dev reports it)."""
+    s = sys1
+    ctx = _ctx(pkg, s, pkg.SDFT_PREC_FP64, 2)
+    try:
+        with pytest.raises(pkg.SdftError):
+            ctx.nl_force_dev(1, 0)
+        rng = np.random.default_rng(3)
+        cr, ci = rng.standard_normal(s["ncoef"]), rng.standard_normal(s["ncoef"])
+        ci[-1] = 0.0
+        ctx.upload(cr, ci)
+        ctx.filter_cheby_dev(1, np.array([1.0, 0.0]), 1, 0.1, 0.0)
+        f, e = ctx.nl_force_dev(1, 0, occ=2.0, nsto_total=1)
+        fo, eo = O.OracleSys(s).nl_force(cr, ci)
+        assert np.abs(f - 2.0 * fo).max() <= 1e-11 * np.abs(fo).max() and abs(e - 2.0 * eo) <= 1e-11 * abs(eo)
+        ctx.set_kb(None)
+        f0, e0 = ctx.nl_force_dev(1, 0)
+        assert f0.shape == (0, 3) and e0 == 0.0
+    finally:
+        ctx.close()

@@ -277,3 +277,32 @@ def test_mixed_newton_and_moments_close_to_fp64(pkg, sys1):
     assert np.max(np.abs(mm - md)) < 1e-6 * np.max(np.abs(md))
     cd.close()
     cm.close()
+
+
+def test_call_order_and_sizes_checked(pkg, sys1):
+    """Host-side refusals on a live context: no potential yet, nstate outside
+    1..max_states, a filter of fewer than two terms; the context stays usable."""
+    c = pkg.Context(*sys1["grid"], sys1["ka"], sys1["kb"], sys1["kc"], sys1["hmat"], max_states=2)
+    try:
+        nc = sys1["ncoef"]
+        z = np.zeros(nc)
+        with pytest.raises(pkg.SdftError) as e:
+            c.calc_coef_force(z, z)
+        assert e.value.code == 4  # SDFT_ERR_STATE: V_KS not set
+        c.set_vks(sys1["vks"])
+        c.set_kb(sys1["kb_desc"])
+        with pytest.raises(pkg.SdftError) as e:
+            c.calc_coef_force(np.zeros(3 * nc), np.zeros(3 * nc))
+        assert e.value.code == 1  # 3 orbitals > max_states 2
+        with pytest.raises(pkg.SdftError) as e:
+            c.upload(z, z)
+            c.filter_cheby_dev(1, np.zeros(0), 1, 0.1, 0.0)
+        assert e.value.code == 1
+        rng = np.random.default_rng(1)
+        cr, ci = rng.standard_normal(nc), rng.standard_normal(nc)
+        ci[-1] = 0.0
+        fr, fi = c.calc_coef_force(cr, ci)
+        gr, gi = O.OracleSys(sys1).hpsi(cr, ci)
+        assert rel_l2(np.concatenate([fr, fi]), np.concatenate([gr, gi])) < 1e-12
+    finally:
+        c.close()

@@ -447,9 +447,16 @@ def run_ours(args):
             return f, ea.elapsed_time(eb)
         f64f, fms64 = force_ms(c64)
         fmxf, fmsmx = force_ms(ctx)
+        # four projections (c and i G_d c, d = x, y, z), each 2 P S (2 ncoef) FP64-equivalent flops;
+        # the mixed ones execute 10 int8 digit products per FP64-equivalent multiply-add
+        pk, psrc = peaks()
+        f_flops = 4 * 2.0 * s["_P"] * nsto * 2 * s["ncoef"]
         nl_force = {"natm": int(f64f.shape[0]), "ms_fp64": fms64, "ms_mixed": fmsmx,
                     "max_abs_err_mixed_vs_fp64_over_max_force":
-                        float(np.abs(fmxf - f64f).max() / max(1e-300, np.abs(f64f).max())) if f64f.size else 0.0}
+                        float(np.abs(fmxf - f64f).max() / max(1e-300, np.abs(f64f).max())) if f64f.size else 0.0,
+                    "fp64_equiv_tflops_mixed": f_flops / (fmsmx * 1e-3) / 1e12,
+                    "frac_of_int8_peak_mixed": 10.0 * f_flops / (fmsmx * 1e-3) / 1e12 / (2.0 * pk["bf16_tflops"]),
+                    "peak_source": f"int8 dense = 2 x {psrc} bf16 burst ({pk['bf16_tflops']})"}
         fp64 = {"orbitals_per_s": nsto * world / (ms64 / 1e3), "ms_per_step": ms64,
                 "mixed_speedup": (nsto * world / (ms64 / 1e3)) and value / (nsto * world / (ms64 / 1e3)),
                 "density_rel_l2_mixed_vs_fp64": float(np.linalg.norm(rhom - rho64) / np.linalg.norm(rho64)),

@@ -280,6 +280,18 @@ static void ad_no_entropy(STODFTINFO *si, const char *where) {
   if (si->smearOpt > 0 && si->filterDiagFlag == 0) ad_die(where, "the entropy filter (smearOpt > 0) is not supported");
 }
 
+/* Releases every system's device context and host copies (for a caller's
+ * shutdown path; the next adapted call creates the context again). */
+void sdft_piny_adapter_finalize(void) {
+  for (int i = 0; i < AD_MAX_SYSTEMS; i++) {
+    AdSys *s = &g_sys[i];
+    if (s->ctx) sdft_ctx_destroy(s->ctx);
+    free(s->vks);
+    free(s->kbpos);
+    memset(s, 0, sizeof *s);
+  }
+}
+
 /* ---- the replaced routines ---------------------------------------------- */
 
 void calcCoefForceWrapSCF(CLASS *class, GENERAL_DATA *general_data, CP *cp, CPCOEFFS_POS *cpcoeffs_pos,

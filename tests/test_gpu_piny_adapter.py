@@ -87,3 +87,4 @@ def test_adapter_density(adsys, gold):
     prec, r, _ = adsys
     rho = r.density(gold["noise_re"], gold["noise_im"])
     assert rel_l2(rho, gold["density"]) < TOL[prec]["d"]
+

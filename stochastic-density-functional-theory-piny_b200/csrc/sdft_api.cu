@@ -262,7 +262,7 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   }
   if (want_enl) {
     launch_enl(ctx->d_z, Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
-    ctx->launches++;
+    ctx->launches += 2;
   }
   if (!back) return SDFT_OK;
   {
@@ -298,7 +298,7 @@ static int run_kb(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, b
   ctx->launches += split > 1 ? 2 : 1;
   if (want_enl) {
     launch_enl(ctx->d_z, ctx->Ppad, ctx->d_w, ctx->P, nstate, ctx->d_enl, ctx->st);
-    ctx->launches++;
+    ctx->launches += 2;
   }
   if (!back) return SDFT_OK;
   {
@@ -650,7 +650,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   CKF(cudaMemsetAsync(ctx->d_b1, 0, vb, ctx->st));
   CKF(cudaMemsetAsync(ctx->d_b2, 0, vb, ctx->st));
   DMF(ctx->d_dots, (size_t)ctx->npairs_max * g.nbatch * 3 * sizeof(double));
-  DMF(ctx->d_enl, sizeof(double));
+  DMF(ctx->d_enl, (1 + kEnlBlocks) * sizeof(double));  // E_NL, then its block partials
   DMF(ctx->d_err, sizeof(int));
   CKF(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->st));
   const size_t vsz = is_fp64(ctx) ? sizeof(double) : sizeof(float);
@@ -1216,7 +1216,6 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
   if ((r = run_kb(ctx, v, nstate, true, false))) goto out;
   CKG(cudaMemcpyAsync(ctx->d_zsave, ctx->d_z, (size_t)nstate * ctx->Ppad * sizeof(double), cudaMemcpyDeviceToDevice,
                       ctx->st));
-  CKG(cudaMemcpyAsync(&en, ctx->d_enl, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
   for (int d = 0; d < 3; d++) {
     // i G_d c into the back-projection buffer, which this call does not otherwise use
     launch_dcoef(v, nstate, ctx->ncoef, ctx->ngp, ctx->d_gk + (size_t)d * ctx->ngp, ctx->d_fnl, ctx->st);
@@ -1226,7 +1225,9 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
                           nstate, scale, d, d_f, ctx->st);
     ctx->launches++;
   }
+  // (the direction projections leave d_enl alone: it still holds E_NL of c)
   CKG(cudaMemcpyAsync(h.data(), d_f, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CKG(cudaMemcpyAsync(&en, ctx->d_enl, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
   CKG(cudaGetLastError());
   CKG(cudaStreamSynchronize(ctx->st));
   std::memcpy(fatm, h.data(), h.size() * sizeof(double));

@@ -514,23 +514,38 @@ __global__ void k_dots_reduce(const double *__restrict__ part, int nparts, int n
     for (int d = 0; d < ndots; d++) out[d] = sh[0][d];
 }
 
-__global__ void k_enl(const double *__restrict__ Z, int ldz, const double *__restrict__ w, int P,
-                      int nstate, double *__restrict__ out) {
+// E_NL partials: block b sums the rows [nstate b / kEnlBlocks, nstate (b+1) /
+// kEnlBlocks) in a fixed order (row by row, threads over the projector
+// channels, then a fixed tree), so the total does not depend on scheduling.
+__global__ void __launch_bounds__(256) k_enl_part(const double *__restrict__ Z, int ldz,
+                                                  const double *__restrict__ w, int P, int nstate,
+                                                  double *__restrict__ part) {
   __shared__ double sh[256];
+  const int r0 = (int)((long long)nstate * blockIdx.x / kEnlBlocks);
+  const int r1 = (int)((long long)nstate * (blockIdx.x + 1) / kEnlBlocks);
   double a = 0.0;
-  const size_t tot = (size_t)P * nstate;
-  for (size_t i = threadIdx.x; i < tot; i += blockDim.x) {
-    const int s = (int)(i / P), u = (int)(i - (size_t)s * P);
-    const double z = Z[(size_t)s * ldz + u];
-    a += w[u] * z * z;
+  for (int s = r0; s < r1; s++) {
+    const double *zr = Z + (size_t)s * ldz;
+    for (int u = threadIdx.x; u < P; u += blockDim.x) {
+      const double z = zr[u];
+      a += w[u] * z * z;
+    }
   }
   sh[threadIdx.x] = a;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *out = sh[0];
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_enl_sum(const double *__restrict__ part, double *__restrict__ out) {
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int b = 0; b < kEnlBlocks; b++) a += part[b];
+    *out = a;
+  }
 }
 
 __global__ void k_scale_copy(const double *__restrict__ src, double *__restrict__ dst, double a, size_t n) {
@@ -680,7 +695,8 @@ void launch_dots_reduce(const double *part, int nparts, int ndots, double *out, 
 }
 
 void launch_enl(const double *Z, int ldz, const double *w, int P, int nstate, double *out, cudaStream_t st) {
-  k_enl<<<1, 256, 0, st>>>(Z, ldz, w, P, nstate, out);
+  k_enl_part<<<kEnlBlocks, 256, 0, st>>>(Z, ldz, w, P, nstate, out + 1);
+  k_enl_sum<<<1, 32, 0, st>>>(out + 1, out);
 }
 
 void launch_scale_copy(const double *src, double *dst, double a, size_t n, cudaStream_t st) {

@@ -124,7 +124,9 @@ void launch_gemm_nt_f64(const double *A, int lda, const double *B, int ldb, doub
                         cudaStream_t st);
 
 void launch_dots_reduce(const double *part, int nparts, int ndots, double *out, cudaStream_t st);
-// E_NL = sum_u w[u] sum_{s<nstate} Z[s*ldz + u]^2 -> out (device scalar)
+// E_NL = sum_u w[u] sum_{s<nstate} Z[s*ldz + u]^2 -> out[0]; out[1 .. kEnlBlocks]
+// hold the partials (two launches)
+constexpr int kEnlBlocks = 128;
 void launch_enl(const double *Z, int ldz, const double *w, int P, int nstate, double *out,
                 cudaStream_t st);
 // dst[i] = a*src[i] over n doubles (acc init etc.)

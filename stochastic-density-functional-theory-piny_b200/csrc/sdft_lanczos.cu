@@ -108,15 +108,15 @@ __global__ void __launch_bounds__(kRedThreads) k_ekin_part(const double *__restr
 // i G_d c: the orbital whose KB projection is dZ/dR_d (get_nlmat,
 // energy/cp/cp_energy_eext_nonloc.c:648-748, accumulates the same sums with
 // the factor G_d and the Re/Im roles swapped)
-__global__ void k_dcoef(const double *__restrict__ v, int nstate, int ncoef, int ngp, const double *__restrict__ gk,
+// grid (x: coefficient blocks, y: orbital rows); no index division
+__global__ void k_dcoef(const double *__restrict__ v, int ncoef, int ngp, const double *__restrict__ gk,
                         double *__restrict__ out) {
-  const long long tot = (long long)nstate * ngp;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
-    const int st = (int)(i / ngp), g = (int)(i - (long long)st * ngp);
-    const double *row = v + (size_t)st * 2 * ngp;
-    double *o = out + (size_t)st * 2 * ngp;
-    const double k = (g < ncoef - 1) ? gk[g] : 0.0;
-    const double re = (g < ncoef - 1) ? row[g] : 0.0, im = (g < ncoef - 1) ? row[ngp + g] : 0.0;
+  const double *row = v + (size_t)blockIdx.y * 2 * ngp;
+  double *o = out + (size_t)blockIdx.y * 2 * ngp;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngp; g += gridDim.x * blockDim.x) {
+    const bool in = g < ncoef - 1;
+    const double k = in ? gk[g] : 0.0;
+    const double re = in ? row[g] : 0.0, im = in ? row[ngp + g] : 0.0;
     o[g] = -k * im;
     o[ngp + g] = k * re;
   }
@@ -185,9 +185,12 @@ void launch_ekin(const double *v, int nstate, int ncoef, int ngp, const double *
 }
 
 void launch_dcoef(const double *v, int nstate, int ncoef, int ngp, const double *gk, double *out, cudaStream_t st) {
-  const long long tot = (long long)nstate * ngp;
-  const int b = (int)std::min<long long>(4 * 148, (tot + 255) / 256);
-  k_dcoef<<<b < 1 ? 1 : b, 256, 0, st>>>(v, nstate, ncoef, ngp, gk, out);
+  const int bx = std::min(8, (ngp + 255) / 256);
+  for (int s0 = 0; s0 < nstate; s0 += 65535) {  // grid.y limit
+    const int n = std::min(65535, nstate - s0);
+    const size_t off = (size_t)s0 * 2 * ngp;
+    k_dcoef<<<dim3(bx < 1 ? 1 : bx, n), 256, 0, st>>>(v + off, ncoef, ngp, gk, out + off);
+  }
 }
 
 void launch_nl_force_atoms(const double *Z0, const double *Zd, int ldz, const double *w, const int *row_start,

@@ -231,9 +231,7 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
     TScope ts(ctx, 7);
     // row maxima: from the stage C that wrote `vec`, else one pass over it
     if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
-      // the pass takes the max into d_rowmax: clear maxima a stage C left there
-      if (ctx->rowmax_zero_n < nstate) CK(cudaMemsetAsync(ctx->d_rowmax, 0, (size_t)nstate * 8, ctx->st));
-      launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);
+      launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);  // clears the rows first
       ctx->launches++;
     }
     launch_oz_slice(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,

@@ -436,8 +436,9 @@ static int filter_cheby_core(sdft_ctx *ctx, int nstate, int L, int nmu, double s
     }
     if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
     if (store_moments) {
-      launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_mom + (size_t)k * 3, ctx->st);
-      ctx->launches++;
+      launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_dots + ctx->dots_cap * 3, ctx->d_mom + (size_t)k * 3,
+                         ctx->st);
+      ctx->launches += 2;
     }
     prev = cur;
     cur = out;
@@ -498,8 +499,9 @@ static int moments_core(sdft_ctx *ctx, int nstate, int L, double scale, double e
       e.PREV = prev;
     }
     if ((r = apply_h(ctx, cur, nstate, e, false))) return r;
-    launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_mom + (size_t)k * 3, ctx->st);
-    ctx->launches++;
+    launch_dots_reduce(ctx->d_dots, nparts, 3, ctx->d_dots + ctx->dots_cap * 3, ctx->d_mom + (size_t)k * 3,
+                       ctx->st);
+    ctx->launches += 2;
     prev = cur;
     cur = out;
   }
@@ -647,7 +649,9 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   CKF(cudaMemsetAsync(ctx->d_chi, 0, vb, ctx->st));
   CKF(cudaMemsetAsync(ctx->d_b1, 0, vb, ctx->st));
   CKF(cudaMemsetAsync(ctx->d_b2, 0, vb, ctx->st));
-  DMF(ctx->d_dots, (size_t)ctx->npairs_max * g.nbatch * 3 * sizeof(double));
+  // per-CTA moment partials, then kDotBlocks block sums of the fixed-order reduction
+  ctx->dots_cap = (size_t)ctx->npairs_max * g.nbatch;
+  DMF(ctx->d_dots, (ctx->dots_cap + kDotBlocks) * 3 * sizeof(double));
   DMF(ctx->d_enl, (1 + kEnlBlocks) * sizeof(double));  // E_NL, then its block partials
   DMF(ctx->d_err, sizeof(int));
   CKF(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->st));

@@ -49,6 +49,7 @@ struct sdft_ctx {
   void *d_x = nullptr;
   size_t x_bytes = 0;
   double *d_dots = nullptr;
+  size_t dots_cap = 0;  // CTA partial slots of d_dots (kDotBlocks*3 block sums follow them)
   double *d_mom = nullptr;
   size_t mom_cap = 0;
   double *d_rho_part = nullptr, *d_rho = nullptr;

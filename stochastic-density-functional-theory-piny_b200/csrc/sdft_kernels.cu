@@ -497,11 +497,16 @@ __global__ void k_split_reduce(const double *__restrict__ work, int split, size_
 // ============================================================================
 // small kernels
 // ============================================================================
-__global__ void k_dots_reduce(const double *__restrict__ part, int nparts, int ndots,
-                              double *__restrict__ out) {
+// Moment-dot partials (3 per stage-C CTA): block b sums the CTAs
+// [nparts b / kDotBlocks, nparts (b+1) / kDotBlocks) in a fixed order, then one
+// thread adds the kDotBlocks block sums in order (k_dots_sum).
+__global__ void __launch_bounds__(256) k_dots_reduce(const double *__restrict__ part, int nparts,
+                                                     double *__restrict__ blk) {
   __shared__ double sh[256][3];
+  const int i0 = (int)((long long)nparts * blockIdx.x / kDotBlocks);
+  const int i1 = (int)((long long)nparts * (blockIdx.x + 1) / kDotBlocks);
   double a[3] = {0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
     for (int d = 0; d < 3; d++) a[d] += part[(size_t)i * 3 + d];
   for (int d = 0; d < 3; d++) sh[threadIdx.x][d] = a[d];
   __syncthreads();
@@ -511,7 +516,15 @@ __global__ void k_dots_reduce(const double *__restrict__ part, int nparts, int n
     __syncthreads();
   }
   if (threadIdx.x == 0)
-    for (int d = 0; d < ndots; d++) out[d] = sh[0][d];
+    for (int d = 0; d < 3; d++) blk[blockIdx.x * 3 + d] = sh[0][d];
+}
+
+__global__ void k_dots_sum(const double *__restrict__ blk, int ndots, double *__restrict__ out) {
+  if (threadIdx.x < ndots) {
+    double a = 0.0;
+    for (int b = 0; b < kDotBlocks; b++) a += blk[b * 3 + threadIdx.x];
+    out[threadIdx.x] = a;
+  }
 }
 
 // E_NL partials: block b sums the rows [nstate b / kEnlBlocks, nstate (b+1) /
@@ -690,8 +703,9 @@ void launch_gemm_nt_f64(const double *A, int lda, const double *B, int ldb, doub
   }
 }
 
-void launch_dots_reduce(const double *part, int nparts, int ndots, double *out, cudaStream_t st) {
-  k_dots_reduce<<<1, 256, 0, st>>>(part, nparts, ndots, out);
+void launch_dots_reduce(const double *part, int nparts, int ndots, double *blk, double *out, cudaStream_t st) {
+  k_dots_reduce<<<kDotBlocks, 256, 0, st>>>(part, nparts, blk);
+  k_dots_sum<<<1, 32, 0, st>>>(blk, ndots, out);
 }
 
 void launch_enl(const double *Z, int ldz, const double *w, int P, int nstate, double *out, cudaStream_t st) {

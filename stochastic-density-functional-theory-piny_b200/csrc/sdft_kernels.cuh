@@ -123,7 +123,10 @@ void launch_gemm_nt_f64(const double *A, int lda, const double *B, int ldb, doub
                         int M, int N, int K, int Mst, int Nst, int split, double *work,
                         cudaStream_t st);
 
-void launch_dots_reduce(const double *part, int nparts, int ndots, double *out, cudaStream_t st);
+// sum over nparts CTA partials (3 doubles each) -> out[0, ndots); blk: kDotBlocks*3
+// doubles of scratch (two launches, fixed order)
+constexpr int kDotBlocks = 128;
+void launch_dots_reduce(const double *part, int nparts, int ndots, double *blk, double *out, cudaStream_t st);
 // E_NL = sum_u w[u] sum_{s<nstate} Z[s*ldz + u]^2 -> out[0]; out[1 .. kEnlBlocks]
 // hold the partials (two launches)
 constexpr int kEnlBlocks = 128;

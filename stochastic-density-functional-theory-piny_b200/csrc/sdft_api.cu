@@ -224,19 +224,29 @@ static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 // orbitals held in `vec`, mixed precision: INT8 Ozaki GEMMs on the digit
 // form of the orbitals; Z = Pj C is split over K with FP64 partial sums, the
 // reduction also produces the digit form of Z for FNL = Bk Z.
-static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true) {
+// gk (nullable): project i G_d vec instead of vec, formed inside the digit
+// passes (gk = G_d per coefficient)
+static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true,
+                     const double *gk = nullptr) {
   const int K1 = 2 * ctx->ngp, S = ctx->s_oz, Ppad = ctx->Ppad;
   const int N = (nstate + 127) / 128 * 128;
   {
     TScope ts(ctx, 7);
-    // row maxima: from the stage C that wrote `vec`, else one pass over it
-    if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
-      launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);  // clears the rows first
+    if (gk) {
+      launch_oz_rowmax_igc(vec, gk, ctx->ngp, ctx->ncoef, nstate, ctx->d_rowmax, ctx->st);
+      launch_oz_slice_igc(vec, gk, ctx->ngp, ctx->ncoef, nstate, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz,
+                          (size_t)S * ctx->kp_oz, ctx->d_c_sc, ctx->st);
+      ctx->launches += 2;
+    } else {
+      // row maxima: from the stage C that wrote `vec`, else one pass over it
+      if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
+        launch_oz_rowmax(vec, K1, nstate, K1, ctx->d_rowmax, ctx->st);  // clears the rows first
+        ctx->launches++;
+      }
+      launch_oz_slice(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,
+                      ctx->d_c_sc, ctx->st);
       ctx->launches++;
     }
-    launch_oz_slice(vec, K1, nstate, K1, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz, (size_t)S * ctx->kp_oz,
-                    ctx->d_c_sc, ctx->st);
-    ctx->launches++;
   }
   OzGemm g1 = ctx->om1, g2 = ctx->om2;
   g1.N = N; g1.Nst = nstate;
@@ -1219,10 +1229,15 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
   CKG(cudaMemcpyAsync(ctx->d_zsave, ctx->d_z, (size_t)nstate * ctx->Ppad * sizeof(double), cudaMemcpyDeviceToDevice,
                       ctx->st));
   for (int d = 0; d < 3; d++) {
-    // i G_d c into the back-projection buffer, which this call does not otherwise use
-    launch_dcoef(v, nstate, ctx->ncoef, ctx->ngp, ctx->d_gk + (size_t)d * ctx->ngp, ctx->d_fnl, ctx->st);
-    ctx->launches++;
-    if ((r = run_kb(ctx, ctx->d_fnl, nstate, false, false))) goto out;
+    const double *gk = ctx->d_gk + (size_t)d * ctx->ngp;
+    if (ctx->oz) {  // the digit passes form i G_d c from c themselves
+      if ((r = run_kb_oz(ctx, v, nstate, false, false, gk))) goto out;
+    } else {
+      // i G_d c into the back-projection buffer, which this call does not otherwise use
+      launch_dcoef(v, nstate, ctx->ncoef, ctx->ngp, gk, ctx->d_fnl, ctx->st);
+      ctx->launches++;
+      if ((r = run_kb(ctx, ctx->d_fnl, nstate, false, false))) goto out;
+    }
     launch_nl_force_atoms(ctx->d_zsave, ctx->d_z, ctx->Ppad, ctx->d_w, ctx->d_kb_rs, ctx->d_kb_rc, ctx->kb_natm,
                           nstate, scale, d, d_f, ctx->st);
     ctx->launches++;

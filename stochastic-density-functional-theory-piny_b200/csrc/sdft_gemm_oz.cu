@@ -344,11 +344,33 @@ __device__ __forceinline__ double absmax_key(double a) { return isfinite(a) ? fa
 
 // rowmax[row] = max |x[row][:]| (as the bit pattern of a non-negative double,
 // whose integer order is its numeric order); +inf if any entry is not finite.
-__global__ void k_row_absmax(const double *__restrict__ x, int ldx, int cols, unsigned long long *rowmax) {
+// Element sources of the digit passes: a stored row, or the row of i G_d c
+// formed on the fly from c (Re = -G_d Im c, Im = G_d Re c; G = 0 and the
+// padding give 0), the vector whose projection is dZ/dR_d.
+struct SrcRows {
+  const double *x;
+  int ldx;
+  __device__ __forceinline__ double operator()(int row, int c) const { return x[(size_t)row * ldx + c]; }
+};
+struct SrcIGc {
+  const double *v;  // rows of 2 ngp: re[0, ngp), im[ngp, 2 ngp)
+  const double *gk; // G_d per coefficient
+  int ngp, ncoef;
+  __device__ __forceinline__ double operator()(int row, int c) const {
+    const double *r = v + (size_t)row * 2 * ngp;
+    const bool im = c >= ngp;
+    const int g = im ? c - ngp : c;
+    if (g >= ncoef - 1) return 0.0;
+    return im ? gk[g] * r[g] : -gk[g] * r[ngp + g];
+  }
+};
+
+template <typename SRC>
+__global__ void k_row_absmax(SRC src, int cols, unsigned long long *rowmax) {
   const int row = blockIdx.x;
   double m = 0.0;
   for (int c = blockIdx.y * blockDim.x + threadIdx.x; c < cols; c += gridDim.y * blockDim.x)
-    m = fmax(m, absmax_key(x[(size_t)row * ldx + c]));
+    m = fmax(m, absmax_key(src(row, c)));
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   __shared__ double red[32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -388,10 +410,9 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 
 // digits of rows x cols doubles; 4 consecutive columns per thread, zero
 // digits for cols <= k < ld.
-template <int FMT>
-__global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, int cols,
-                             const unsigned long long *__restrict__ rowmax, int8_t *__restrict__ dig, int ld,
-                             size_t sstride, double *__restrict__ scale) {
+template <int FMT, typename SRC>
+__global__ void k_slice_rows(SRC src, int rows, int cols, const unsigned long long *__restrict__ rowmax,
+                             int8_t *__restrict__ dig, int ld, size_t sstride, double *__restrict__ scale) {
   constexpr int NS = OzF<FMT>::NS;
   const int g4 = ld >> 2;
   const size_t tot = (size_t)rows * g4;
@@ -405,7 +426,7 @@ __global__ void k_slice_rows(const double *__restrict__ x, int ldx, int rows, in
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const int c = c4 + e;
-      const double v = (c < cols && !bad) ? x[(size_t)row * ldx + c] : 0.0;
+      const double v = (c < cols && !bad) ? src(row, c) : 0.0;
       digits_of<FMT>(v * p, d[e]);
     }
 #pragma unroll
@@ -556,23 +577,45 @@ int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int
                          : run_gemm_oz_t<float, OZ_7x4>(g, split, out, split_stride, err, st);
 }
 
-void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {
+template <typename SRC>
+static void rowmax_of(SRC src, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {
   cudaMemsetAsync(rowmax, 0, (size_t)rows * sizeof(unsigned long long), st);
   int chunks = (cols + 255) / 256;  // grid = rows x chunks (rows on x: up to 2^31 - 1)
   if (chunks > 64) chunks = 64;
   if (chunks < 1) chunks = 1;
-  k_row_absmax<<<dim3(rows, chunks), 256, 0, st>>>(x, ldx, cols, rowmax);
+  k_row_absmax<SRC><<<dim3(rows, chunks), 256, 0, st>>>(src, cols, rowmax);
 }
 
-void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
-                     int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt) {
+template <typename SRC>
+static void slice_of(SRC src, int rows, int cols, const unsigned long long *rowmax, int8_t *dig, int ld,
+                     size_t slice_stride, double *scale, cudaStream_t st, int fmt) {
   const size_t tot = (size_t)rows * (ld / 4);
   int blocks = (int)((tot + 255) / 256);
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (fmt == OZ_8x3)
-    k_slice_rows<OZ_8x3><<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
+    k_slice_rows<OZ_8x3, SRC><<<blocks, 256, 0, st>>>(src, rows, cols, rowmax, dig, ld, slice_stride, scale);
   else
-    k_slice_rows<OZ_7x4><<<blocks, 256, 0, st>>>(x, ldx, rows, cols, rowmax, dig, ld, slice_stride, scale);
+    k_slice_rows<OZ_7x4, SRC><<<blocks, 256, 0, st>>>(src, rows, cols, rowmax, dig, ld, slice_stride, scale);
+}
+
+void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st) {
+  rowmax_of(SrcRows{x, ldx}, rows, cols, rowmax, st);
+}
+
+void launch_oz_rowmax_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,
+                          unsigned long long *rowmax, cudaStream_t st) {
+  rowmax_of(SrcIGc{v, gk, ngp, ncoef}, rows, 2 * ngp, rowmax, st);
+}
+
+void launch_oz_slice_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,
+                         const unsigned long long *rowmax, int8_t *dig, int ld, size_t slice_stride, double *scale,
+                         cudaStream_t st) {
+  slice_of(SrcIGc{v, gk, ngp, ncoef}, rows, 2 * ngp, rowmax, dig, ld, slice_stride, scale, st, OZ_7x4);
+}
+
+void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigned long long *rowmax, int8_t *dig,
+                     int ld, size_t slice_stride, double *scale, cudaStream_t st, int fmt) {
+  slice_of(SrcRows{x, ldx}, rows, cols, rowmax, dig, ld, slice_stride, scale, st, fmt);
 }
 
 void launch_oz_slice_rows(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, int8_t *dig,

@@ -790,6 +790,44 @@ def run_serve(args):
     print(json.dumps(out))
 
 
+def run_forces(args):
+    """The nonlocal atomic forces alone (sdft_nl_force_dev) on the config's
+    system: seeded random orbitals taken as the filtered ones (coefficients
+    [1, 0]), then `steps` timed calls after `warmup` untimed ones.  One JSON
+    line; a small, fixed command for profiling the force path."""
+    import torch
+    import __graft_entry__ as g
+    pkg = g.load_package()
+    wl, cfg, s = setup_system(args.config, 0)
+    nsto = cfg["nsto"] if args.nsto is None else args.nsto
+    prec = {"mixed": pkg.SDFT_PREC_MIXED, "mixed_fast": pkg.SDFT_PREC_MIXED_FAST, "fp64": pkg.SDFT_PREC_FP64}[args.prec]
+    ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=nsto)
+    ctx.set_vks(s["vks"])
+    ctx.set_kb(s["kb_desc"])
+    rng = np.random.default_rng(3)
+    cr = rng.standard_normal(nsto * s["ncoef"])
+    ci = rng.standard_normal(nsto * s["ncoef"])
+    ci.reshape(nsto, -1)[:, -1] = 0.0
+    ctx.upload(cr, ci)
+    ctx.filter_cheby_dev(nsto, np.array([1.0, 0.0]), 1, 0.1, 0.0)
+    st = torch.cuda.ExternalStream(pkg.lib.sdft_ctx_stream(ctx._p))
+    for _ in range(args.warmup):
+        ctx.nl_force_dev(nsto, 0, occ=wl.OCC, nsto_total=nsto)
+    ms = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        f, e = ctx.nl_force_dev(nsto, 0, occ=wl.OCC, nsto_total=nsto)
+        b.record(st)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    ctx.close()
+    print(json.dumps({"metric": "nonlocal atomic forces of filtered orbitals (ms per call)", "value": min(ms),
+                      "unit": "ms", "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+                      "config": {"workload": args.config, "orbitals": nsto, "natm": int(f.shape[0]),
+                                 "precision": args.prec}, "energy_pnl": e}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -811,8 +849,12 @@ def main():
     ap.add_argument("--no-priorities", action="store_true", help="cfg5: all request streams at default priority")
     ap.add_argument("--serve-eager", action="store_true",
                     help="cfg5: issue each request's kernels directly instead of as a captured CUDA graph")
+    ap.add_argument("--forces-only", action="store_true",
+                    help="time sdft_nl_force_dev alone on the config's system (profiling the force path)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.forces_only:
+        run_forces(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config == "cfg4":
         run_batch(args)

@@ -225,18 +225,17 @@ static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 // form of the orbitals; Z = Pj C is split over K with FP64 partial sums, the
 // reduction also produces the digit form of Z for FNL = Bk Z.
 // gk (nullable): project i G_d vec instead of vec, formed inside the digit
-// passes (gk = G_d per coefficient)
+// pass (gk = G_d per coefficient) under the row maxima gk_max
 static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true,
-                     const double *gk = nullptr) {
+                     const double *gk = nullptr, const unsigned long long *gk_max = nullptr) {
   const int K1 = 2 * ctx->ngp, S = ctx->s_oz, Ppad = ctx->Ppad;
   const int N = (nstate + 127) / 128 * 128;
   {
     TScope ts(ctx, 7);
     if (gk) {
-      launch_oz_rowmax_igc(vec, gk, ctx->ngp, ctx->ncoef, nstate, ctx->d_rowmax, ctx->st);
-      launch_oz_slice_igc(vec, gk, ctx->ngp, ctx->ncoef, nstate, ctx->d_rowmax, ctx->d_c_dig, ctx->kp_oz,
+      launch_oz_slice_igc(vec, gk, ctx->ngp, ctx->ncoef, nstate, gk_max, ctx->d_c_dig, ctx->kp_oz,
                           (size_t)S * ctx->kp_oz, ctx->d_c_sc, ctx->st);
-      ctx->launches += 2;
+      ctx->launches++;
     } else {
       // row maxima: from the stage C that wrote `vec`, else one pass over it
       if (!(ctx->track_omax && ctx->omax_vec == vec && ctx->omax_n == nstate)) {  // (set only when oz)
@@ -687,7 +686,7 @@ extern "C" int sdft_ctx_destroy(sdft_ctx *ctx) {
                   ctx->d_enl, ctx->d_red, ctx->d_kb_rng,
                   ctx->d_err, ctx->d_pj_dig, ctx->d_bk_dig, ctx->d_c_dig,
                   ctx->d_z_dig, ctx->d_pj_sc, ctx->d_bk_sc, ctx->d_c_sc, ctx->d_z_sc, ctx->d_rowmax,
-                  ctx->d_oz_part, ctx->d_kb_rs, ctx->d_kb_rc, ctx->d_gk, ctx->d_zsave};
+                  ctx->d_oz_part, ctx->d_kb_rs, ctx->d_kb_rc, ctx->d_gk, ctx->d_zsave, ctx->d_rowmax3};
   // a batch graph still holding the context: wait for its replays, drop the context from it
   for (sdft_batch *b : ctx->batches) batch_detach(b, ctx);
   ctx->batches.clear();
@@ -1214,6 +1213,11 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
     if ((r = dmalloc(ctx, (void **)&ctx->d_zsave, zel * sizeof(double)))) return r;
     ctx->kb_bytes += (long long)(zel * sizeof(double));  // released with the KB buffers
   }
+  if (ctx->oz && !ctx->d_rowmax3) {
+    const size_t b = (size_t)3 * ctx->s_pad * sizeof(unsigned long long);
+    if ((r = dmalloc(ctx, (void **)&ctx->d_rowmax3, b))) return r;
+    ctx->kb_bytes += (long long)b;
+  }
   double *d_f = nullptr;
   if ((r = dev_alloc(ctx->device, ctx->st, (void **)&d_f, (size_t)3 * ctx->kb_natm * sizeof(double)))) return r;
   const double *v = ctx->d_acc + (size_t)imu * ctx->vec_elems;
@@ -1228,10 +1232,14 @@ extern "C" int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ,
   if ((r = run_kb(ctx, v, nstate, true, false))) goto out;
   CKG(cudaMemcpyAsync(ctx->d_zsave, ctx->d_z, (size_t)nstate * ctx->Ppad * sizeof(double), cudaMemcpyDeviceToDevice,
                       ctx->st));
+  if (ctx->oz) {  // row maxima of the three i G_d c in one pass over c
+    launch_oz_rowmax_igc3(v, ctx->d_gk, ctx->ngp, ctx->ncoef, nstate, ctx->d_rowmax3, ctx->st);
+    ctx->launches++;
+  }
   for (int d = 0; d < 3; d++) {
     const double *gk = ctx->d_gk + (size_t)d * ctx->ngp;
-    if (ctx->oz) {  // the digit passes form i G_d c from c themselves
-      if ((r = run_kb_oz(ctx, v, nstate, false, false, gk))) goto out;
+    if (ctx->oz) {  // the digit pass forms i G_d c from c itself
+      if ((r = run_kb_oz(ctx, v, nstate, false, false, gk, ctx->d_rowmax3 + (size_t)d * nstate))) goto out;
     } else {
       // i G_d c into the back-projection buffer, which this call does not otherwise use
       launch_dcoef(v, nstate, ctx->ncoef, ctx->ngp, gk, ctx->d_fnl, ctx->st);

@@ -38,6 +38,7 @@ struct sdft_ctx {
   int *d_kb_rs = nullptr, *d_kb_rc = nullptr;
   double *d_gk = nullptr;  // [3][ngp], G = 0 and padding 0
   double *d_zsave = nullptr;
+  unsigned long long *d_rowmax3 = nullptr;  // row maxima of i G_d c, d = x, y, z (3 s_pad words)
   size_t zwork_elems = 0;
   // orbital blocks
   double *d_chi = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_fnl = nullptr;

@@ -602,9 +602,41 @@ void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned lon
   rowmax_of(SrcRows{x, ldx}, rows, cols, rowmax, st);
 }
 
-void launch_oz_rowmax_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,
-                          unsigned long long *rowmax, cudaStream_t st) {
-  rowmax_of(SrcIGc{v, gk, ngp, ncoef}, rows, 2 * ngp, rowmax, st);
+// Row maxima of i G_d c for d = x, y, z in one pass over c: |Re| = |G_d| |Im c|
+// and |Im| = |G_d| |Re c|, so each coefficient contributes |G_d| max(|Re c|,
+// |Im c|) (G = 0 and the padding contribute 0).  rowmax3: 3 rows-long words.
+__global__ void k_row_absmax_igc3(const double *__restrict__ v, const double *__restrict__ gk, int ngp, int ncoef,
+                                  int rows, unsigned long long *rowmax3) {
+  const int row = blockIdx.x;
+  const double *r = v + (size_t)row * 2 * ngp;
+  double m[3] = {0.0, 0.0, 0.0};
+  for (int g = blockIdx.y * blockDim.x + threadIdx.x; g < ncoef - 1; g += gridDim.y * blockDim.x) {
+    const double a = fmax(absmax_key(r[g]), absmax_key(r[ngp + g]));
+#pragma unroll
+    for (int d = 0; d < 3; d++) m[d] = fmax(m[d], absmax_key(gk[(size_t)d * ngp + g] * a));
+  }
+  __shared__ double red[3][32];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    for (int o = 16; o > 0; o >>= 1) m[d] = fmax(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
+    if ((threadIdx.x & 31) == 0) red[d][threadIdx.x >> 5] = m[d];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    double x = red[d][0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = fmax(x, red[d][w]);
+    atomicMax(rowmax3 + (size_t)d * rows + row, (unsigned long long)__double_as_longlong(x));
+  }
+}
+
+void launch_oz_rowmax_igc3(const double *v, const double *gk, int ngp, int ncoef, int rows,
+                           unsigned long long *rowmax3, cudaStream_t st) {
+  cudaMemsetAsync(rowmax3, 0, (size_t)3 * rows * sizeof(unsigned long long), st);
+  int chunks = (ncoef + 255) / 256;
+  if (chunks > 64) chunks = 64;
+  if (chunks < 1) chunks = 1;
+  k_row_absmax_igc3<<<dim3(rows, chunks), 256, 0, st>>>(v, gk, ngp, ncoef, rows, rowmax3);
 }
 
 void launch_oz_slice_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,

@@ -61,8 +61,9 @@ void launch_oz_slice(const double *x, int ldx, int rows, int cols, const unsigne
 // the same two passes for the rows of i G_d c formed from c on the fly
 // (v: rows of 2 ngp, re then im; gk: G_d per coefficient; 28-bit digits of
 // 2 ngp columns), the vector whose projection is dZ/dR_d
-void launch_oz_rowmax_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,
-                          unsigned long long *rowmax, cudaStream_t st);
+// rowmax3[d rows + r] for d = x, y, z in one pass over c (gk: 3 ngp, G_x then G_y, G_z)
+void launch_oz_rowmax_igc3(const double *v, const double *gk, int ngp, int ncoef, int rows,
+                           unsigned long long *rowmax3, cudaStream_t st);
 void launch_oz_slice_igc(const double *v, const double *gk, int ngp, int ncoef, int rows,
                          const unsigned long long *rowmax, int8_t *dig, int ld, size_t slice_stride, double *scale,
                          cudaStream_t st);

@@ -170,7 +170,9 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->d_oz_part = nullptr;
   dev_free(ctx->d_kb_rs, ctx->st);
   dev_free(ctx->d_kb_rc, ctx->st);
+  dev_free(ctx->d_rowmax3, ctx->st);
   ctx->d_kb_rs = ctx->d_kb_rc = nullptr;
+  ctx->d_rowmax3 = nullptr;
   ctx->kb_natm = 0;
   ctx->P = 0;
   ctx->oz = false;

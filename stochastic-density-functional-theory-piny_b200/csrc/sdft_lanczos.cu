@@ -88,19 +88,22 @@ __global__ void k_lz_div(double *__restrict__ c, const double *__restrict__ nrm2
   }
 }
 
-// sum over nstate rows and G != G0 of 2 ak2(G) (re^2 + im^2)
+// sum over nstate rows and G != G0 of 2 ak2(G) (re^2 + im^2); block b takes
+// the rows [nstate b / kRedBlocks, nstate (b+1) / kRedBlocks), threads the G
+// vectors of each row (a fixed order, no index division)
 __global__ void __launch_bounds__(kRedThreads) k_ekin_part(const double *__restrict__ v, int nstate, int ncoef,
                                                            int ngp, const double *__restrict__ ak2,
                                                            double *__restrict__ part) {
   double s = 0.0;
   const int ng = ncoef - 1;
-  const long long tot = (long long)nstate * ng;
-  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < tot;
-       i += (long long)kRedBlocks * kRedThreads) {
-    const int st = (int)(i / ng), g = (int)(i - (long long)st * ng);
+  const int r0 = (int)((long long)nstate * blockIdx.x / kRedBlocks);
+  const int r1 = (int)((long long)nstate * (blockIdx.x + 1) / kRedBlocks);
+  for (int st = r0; st < r1; st++) {
     const double *row = v + (size_t)st * 2 * ngp;
-    const double re = row[g], im = row[ngp + g];
-    s += 2.0 * ak2[g] * (re * re + im * im);
+    for (int g = threadIdx.x; g < ng; g += kRedThreads) {
+      const double re = row[g], im = row[ngp + g];
+      s += 2.0 * ak2[g] * (re * re + im * im);
+    }
   }
   block_sum_to(s, part + blockIdx.x);
 }

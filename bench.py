@@ -158,13 +158,36 @@ KERNEL_OF = {"stage_a_pack_cfft": "kf_stage_a", "stage_b_plane_fft_vks": "kf_sta
              "density_planes": "kf_stage_b_density"}
 
 
-def rooflines(timing, s, nsto, mixed, back_products=10):
+def fp64_gemm_peak(local):
+    """Measured FP64 tensor-core (DMMA) rate of this GPU: cuBLAS DGEMM
+    (torch.matmul, float64) 8192^3, best of 5 by CUDA events; TFLOP/s."""
+    import torch
+    dev = f"cuda:{local}"
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def rooflines(timing, s, nsto, mixed, back_products=10, fp64_peak=None):
     """Roofline of every kernel function with an algorithmic model, largest
     total time first.  Tensor: the KB GEMMs (projection and back projection,
     one kernel) -- mixed: int8 tcgen05 ops (10 digit products per FP64-
     equivalent multiply-add) against 2 x the measured bf16 burst peak (B200's
     dense int8 rate is twice its bf16 rate); FP64: DMMA flops against the
-    nominal 40 TFLOP/s FP64 tensor rate.  HBM: algorithmic bytes (algorithmic())
+    FP64 tensor (DMMA) rate measured by fp64_gemm_peak (fp64_peak), else the
+    nominal 40 TFLOP/s.  HBM: algorithmic bytes (algorithmic())
     against the measured copy bandwidth.  back_products: int8 digit products
     of the back projection (10, or 6 with the 24-bit digits of mixed_fast)."""
     pk, src = peaks()
@@ -201,8 +224,9 @@ def rooflines(timing, s, nsto, mixed, back_products=10):
                 name = "kb_gemm (k_gemm_oz8, int8 tcgen05)"
             else:
                 ach = work / t / 1e12
-                peak = 40.0
-                psrc = "nominal FP64 tensor (DMMA) rate"
+                peak = fp64_peak or 40.0
+                psrc = ("measured cuBLAS DGEMM 8192^3 (torch.matmul float64, best of 5) on this GPU"
+                        if fp64_peak else "nominal FP64 tensor (DMMA) rate")
                 name = "kb_gemm (k_gemm_nt_f64, DMMA)"
             out.append({"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                         "frac": ach / peak, "traffic": PROFILED_GEMM_TRAFFIC.get((tuple(s["grid"]), mixed, nsto)),
@@ -413,6 +437,20 @@ def run_ours(args):
             b64.close()
         c64.sync()
         ms64 = a.elapsed_time(b)
+        # the FP64 step once more, issued eagerly with per-kernel event timing:
+        # the kernel table and rooflines of the plain form (the denominator of
+        # the mixed speed-up), its DMMA GEMM against the measured DGEMM rate
+        c64.read_timing()
+        c64.set_timing(True)
+        c64.filter_cheby_dev(nsto, ec, 1, scale, emean)
+        c64.density_dev(nsto, 0, occ_over, want=False)
+        c64.sync()
+        t64 = c64.read_timing()
+        c64.set_timing(False)
+        f64peak = fp64_gemm_peak(local)
+        roof64 = rooflines(t64, s, nsto, False, fp64_peak=f64peak)
+        tot64 = max(1e-9, sum(x[0] for x in t64.values()))
+        ktab64 = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / tot64} for k, v in t64.items() if v[1]}
         rho64 = c64.density_dev(nsto, 0, occ_over)
         ctx.filter_cheby_dev(nsto, ec, 1, scale, emean)
         rhom = ctx.density_dev(nsto, 0, occ_over)
@@ -462,7 +500,8 @@ def run_ours(args):
                 "density_rel_l2_mixed_vs_fp64": float(np.linalg.norm(rhom - rho64) / np.linalg.norm(rho64)),
                 "band_energy_fp64": e64, "band_energy_mixed": em,
                 "energy_rel_err_mixed_vs_fp64": abs(em - e64) / abs(e64),
-                "num_elec_density": float(rho64.sum() / rho64.size), "nl_force": nl_force}
+                "num_elec_density": float(rho64.sum() / rho64.size), "nl_force": nl_force,
+                "kernels": ktab64, "roofline_kernels": roof64, "fp64_dgemm_tflops_measured": f64peak}
         c64.close()
 
     # ---- roofline: per kernel function, the dominant one first
@@ -502,16 +541,49 @@ def run_ours(args):
         print(json.dumps(out))
 
 
+def _workload_standalone():
+    """workload.py (the seeded synthetic Si builder; numpy only) loaded on
+    its own, without the package, so that the reference's CPU arm maps none
+    of the product's libraries."""
+    import importlib.util
+    name = "sdft_synthetic_si"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        "stochastic-density-functional-theory-piny_b200", "workload.py")
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sys.modules[name] = mod
+    return mod
+
+
+def _ref_gvec(hmat, ecut, kmax):
+    """The half G sphere from the reference's own setkvec3d_sm (oracle/_ref),
+    its length counted by the oracle; the oracle's list where the reference
+    build is absent."""
+    from oracle import oracle as O
+    from oracle import ref as R
+    og = O.gvec(hmat, ecut, kmax)
+    return R.gvec(hmat, ecut, kmax, len(og[0])) if R.available() else og
+
+
+def ref_setup_system(cfg_name):
+    """setup_system for the reference arm: the same seeded workload, built
+    without the product library."""
+    wl = _workload_standalone()
+    cfg = wl.CONFIGS[cfg_name]
+    return wl, cfg, wl.make_system(cfg["nrep"], cfg["grid"], gvec=_ref_gvec)
+
+
 def _ref_worker_init(cfg_name):
     """Worker of the reference CPU arm: silence the reference's own timer
     printouts (stdout) and build the system once."""
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     global _W
-    import __graft_entry__ as g
-    wl = g.load_workload()
-    cfg = wl.CONFIGS[cfg_name]
-    _W = {"s": wl.make_system(cfg["nrep"], cfg["grid"]), "wl": wl}
+    wl, _, s = ref_setup_system(cfg_name)
+    _W = {"s": s, "wl": wl}
 
 
 def _ref_worker_run(task):
@@ -586,9 +658,12 @@ def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import __graft_entry__ as g
-    pkg = g.load_package()
-    wl, cfg, s = setup_system(args.config, rank)
+    # nothing of the product is loaded on this arm: the workload comes from
+    # the numpy builder with the reference's setkvec3d_sm, the coefficients
+    # from the reference's calcChebyCoeff (stodft/coeff.c:1093), both in oracle/_ref
+    from oracle import oracle as O
+    from oracle import ref as R
+    wl, cfg, s = ref_setup_system(args.config)
     nsto = cfg["nsto"] if args.nsto is None else args.nsto
     L = cfg["L"] if args.L is None else args.L
     # spectral window and coefficients as the GPU arm uses (Lanczos bounds of
@@ -596,7 +671,8 @@ def run_reference(args):
     emin, emax = -0.9735, 9.8349
     ediff, emean = emax - emin, 0.5 * (emin + emax)
     scale = 2.0 / ediff
-    ec = pkg.calcChebyCoeff(L, ediff, emean, wl.BETA, -0.677, fun_flag=2)
+    ec = (R.cheby_coeff(L, ediff, emean, wl.BETA, -0.677, 2) if R.available()
+          else O.cheby_coeff(L, ediff, emean, wl.BETA, -0.677, 2))
     rc = RefCpu(args.config)
     k = args.cpu_steps
     vals, ms = [], []

@@ -305,15 +305,18 @@ int sdft_batch_destroy(sdft_batch *b);
 
 /* ---- allocation-free device helper ------------------------------------ */
 /* No counterpart in the reference.  Per-orbital half-sphere inner products
- *   out[s] = sum_{G!=0} 2 (a_re b_re + a_im b_im) + a_re(G0) b_re(G0)
+ *   out[s] = 2 sum_G (a_re b_re + a_im b_im) - a_re(G0) b_re(G0)
+ * (the sum over all ncoef stored coefficients, as the reference's ddot
+ * forms it in stodft/filter.c:492 and calc-chempot-chebyshev.c:725)
  * of nstate orbitals of ncoef coefficients (G0 last), all five arrays in
  * device memory of the calling thread's current device; queued on `stream`
  * (a cudaStream_t, NULL = default stream) and asynchronous.  Allocates
  * nothing: for callers whose device memory is fully owned by their own pool
  * or fixed in size.  Partial sums live in a static 64 KB device array
  * compiled into the library; nstate above 1024 is rejected
- * (SDFT_ERR_ARG).  The first call on a device looks that array up and
- * should come before any stream capture.  Calls that may overlap on one
+ * (SDFT_ERR_ARG).  The first call on a device loads the kernels there
+ * and should come before any stream capture; every call looks the array's
+ * address up in the current context.  Calls that may overlap on one
  * device race on the array: order them on one stream.                    */
 int sdft_half_dots_noalloc(const double *a_re, const double *a_im,
                            const double *b_re, const double *b_im,

@@ -48,6 +48,10 @@ def lib(adapter=False):
         L.ref_mix_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]
         L.ref_mix_checkpoint.restype = C.c_int
         L.ref_xc_lda.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, _dp, _dp]
+        L.ref_chempot.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        L.ref_num_elec.restype = C.c_double
+        L.ref_num_elec.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, C.c_double]
         _libs[path] = L
     return _libs[path]
 
@@ -136,6 +140,16 @@ class RefSys:
         self._L.ref_density(self._p, cre.size // self.ncoef, _d(cre), _d(cim), _d(rho))
         return rho
 
+    def chem_pot(self, cre, cim, L, emin, emax, beta, occ, num_elec, chem_pot_init, gap_init):
+        """calcChemPotCheby on these orbitals as the noise: the reference
+        computes their moments itself and bisects N(mu) = num_elec.
+        Returns (mu, N(mu))."""
+        cre, cim = f64(cre), f64(cim)
+        mu, ne = C.c_double(), C.c_double()
+        self._L.ref_chempot(self._p, cre.size // self.ncoef, _d(cre), _d(cim), L, emin, emax, beta, occ, num_elec,
+                            chem_pot_init, gap_init, C.byref(mu), C.byref(ne))
+        return mu.value, ne.value
+
     def moments(self, cre, cim, L, scale, emean):
         cre, cim = f64(cre), f64(cim)
         m = np.zeros(L + 1)
@@ -208,3 +222,10 @@ def xc_lda(kind, rho, vks, vol):
     exc, muxc = C.c_double(0.0), C.c_double(0.0)
     lib().ref_xc_lda(int(kind), rho.size, _d(rho), _d(v), float(vol), C.byref(exc), C.byref(muxc))
     return v, exc.value, muxc.value
+
+
+def num_elec(L, emin, emax, beta, occ, moments_normalised, mu):
+    """calcNumElecCheby: occ * sum_{k<L} c_k(mu) m_k with the Chebyshev
+    coefficients of F on [emin, emax]."""
+    m = f64(moments_normalised)
+    return lib().ref_num_elec(L, emin, emax, beta, occ, _d(m), mu)

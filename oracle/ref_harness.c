@@ -39,6 +39,8 @@ void normHNewtonHerm(CP *, CLASS *, GENERAL_DATA *, CPCOEFFS_POS *, CLATOMS_POS 
 void filterChebyPolyHerm(CP *, CLASS *, GENERAL_DATA *, int);
 void filterNewtonPolyHerm(CP *, CLASS *, GENERAL_DATA *, int);
 void calcChebyMoments(CP *, CLASS *, GENERAL_DATA *, int);
+void calcChemPotCheby(CP *, CLASS *, GENERAL_DATA *, int);
+double calcNumElecCheby(CP *, double, double *);
 void calcChebyCoeff(STODFTINFO *, STODFTCOEFPOS *, double *, double *, int, double);
 void genSampNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
 void genCoeffNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
@@ -466,6 +468,99 @@ int ref_moments(RefSys *r, int ns, const double *re, const double *im, int L, do
   r->scoef.chebyMomentsUp = d1(L + 1);
   calcChebyMoments(&r->cp, &r->cls, &r->gd, 0);
   memcpy(moments, r->scoef.chebyMomentsUp, sizeof(double) * (L + 1));
+  return 0;
+}
+
+/* The stodftInfo fields that calcChemPotCheby and calcNumElecCheby read
+ * (stodft/calc-chempot-chebyshev.c:30-95, :918-930), spin-unpolarised. */
+static void set_chempot_info(RefSys *r, int ns, int L, double emin, double emax, double beta, double occ,
+                             double num_elec, double chem_pot_init, double gap_init) {
+  STODFTINFO *si = &r->sinfo;
+  set_poly(r, L, 1, NULL, 2.0 / (emax - emin), 0.5 * (emin + emax), 1);
+  si->energyDiff = emax - emin;
+  si->energyMin = emin;
+  si->energyMax = emax;
+  si->beta = beta;
+  si->occNumber = (int)occ;
+  si->numElecTrue = num_elec;
+  si->chemPotInit = chem_pot_init;
+  si->gapInit = gap_init;
+  si->numStateStoUp = ns;
+  si->numStateStoDn = 0;
+  si->printChebyMoment = 0;
+  si->iScf = 1;
+  if (!r->scoef.chemPot) r->scoef.chemPot = (double *)calloc(4, sizeof(double));
+}
+
+/* calcNumElecCheby (stodft/calc-chempot-chebyshev.c:918) at mu with the
+ * moments in cp->stodftCoefPos->chebyMomentsUp: the Chebyshev grid and the
+ * forward FFT plan that calcChemPotCheby sets up around it (:109-116). */
+static double num_elec_with(CP *cp, int L, double mu) {
+  STODFTINFO *si = cp->stodftInfo;
+  STODFTCOEFPOS *sc = cp->stodftCoefPos;
+  si->numChebyGrid = roundFFT(32 * L);
+  sc->funValGridFFT = fftw_malloc(sizeof(fftw_complex) * si->numChebyGrid);
+  sc->chebyCoeffsFFT = fftw_malloc(sizeof(fftw_complex) * si->numChebyGrid);
+  si->fftwPlanForward = fftw_plan_dft_1d(si->numChebyGrid, sc->funValGridFFT, sc->chebyCoeffsFFT, FFTW_FORWARD, 0);
+  double *coeffs = (double *)calloc(L, sizeof(double));
+  double n = calcNumElecCheby(cp, mu, coeffs);
+  free(coeffs);
+  fftw_destroy_plan(si->fftwPlanForward);
+  fftw_free(sc->funValGridFFT);
+  fftw_free(sc->chebyCoeffsFFT);
+  return n;
+}
+
+static double ref_num_elec_on(RefSys *r, int L, double mu) { return num_elec_with(&r->cp, L, mu); }
+
+/* calcNumElecCheby on given normalised moments (moments[0..L-1] enter the
+ * sum), without a system: only the fields it reads are set. */
+double ref_num_elec(int L, double emin, double emax, double beta, double occ, const double *moments, double mu) {
+  CP cp;
+  STODFTINFO si;
+  STODFTCOEFPOS sc;
+  CHEBYSHEVINFO ch;
+  memset(&cp, 0, sizeof cp); memset(&si, 0, sizeof si); memset(&sc, 0, sizeof sc); memset(&ch, 0, sizeof ch);
+  cp.stodftInfo = &si;
+  cp.stodftCoefPos = &sc;
+  cp.communicate.numThreads = 1;
+  si.chebyshevInfo = &ch;
+  si.polynormLength = L;
+  si.energyDiff = emax - emin;
+  si.energyMean = 0.5 * (emin + emax);
+  si.beta = beta;
+  si.occNumber = (int)occ;
+  si.fermiFunctionReal = fermiExpReal;
+  sc.chebyMomentsUp = (double *)moments;
+  return num_elec_with(&cp, L, mu);
+}
+
+/* calcChemPotCheby (stodft/calc-chempot-chebyshev.c:30) on the loaded
+ * states: the routine computes their Chebyshev moments itself
+ * (calcChebyMoments, whose noise call the harness answers with the injected
+ * chi), divides them by numStateStoUp, brackets N(mu) = Ne from
+ * chemPotInit +- gapInit/2 (widening by gapInit), takes one secant step and
+ * bisects to 1e-11 Ne.  Out: chemPot[0] and N(mu) at that mu. */
+int ref_chempot(RefSys *r, int ns, const double *re, const double *im, int L, double emin, double emax,
+                double beta, double occ, double num_elec, double chem_pot_init, double gap_init, double *mu,
+                double *ne) {
+  load_states(r, ns, re, im);
+  g_inj_re = re; g_inj_im = im; g_inj_n = ns * r->ncoef;
+  set_chempot_info(r, ns, L, emin, emax, beta, occ, num_elec, chem_pot_init, gap_init);
+  calcChemPotCheby(&r->cp, &r->cls, &r->gd, 0);
+  *mu = r->scoef.chemPot[0];
+  if (ne) {
+    /* N(mu) through calcNumElecCheby on the routine's own normalised moments:
+     * recomputed here, since calcChemPotCheby frees them */
+    double *m = d1(L + 1);
+    r->scoef.chebyMomentsUp = m;
+    r->sinfo.numChebyMoments = (L % 2 == 0) ? (L / 2 + 1) : ((L + 1) / 2);
+    calcChebyMoments(&r->cp, &r->cls, &r->gd, 0);
+    for (int i = 0; i <= L; i++) m[i] /= (double)ns;
+    *ne = ref_num_elec_on(r, L, *mu);
+    free(m);
+    r->scoef.chebyMomentsUp = NULL;
+  }
   return 0;
 }
 

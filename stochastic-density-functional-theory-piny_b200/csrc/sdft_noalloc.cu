@@ -10,10 +10,12 @@
 // calls an allocating routine.
 //
 // The sums are the ones the Chebyshev moments path forms in the epilogue of
-// its last FFT stage (calc-chempot-chebyshev.c:722-842 in the reference
-// takes them with ddot over the half sphere): for orbital s,
-//     out[s] = sum_{G != 0} 2 (a_re b_re + a_im b_im) + a_re(G0) b_re(G0),
-// G0 being the last coefficient of each orbital.
+// its last FFT stage (the reference takes them with ddot over the half
+// sphere, stodft/filter.c:492-496 and calc-chempot-chebyshev.c:725-729):
+// for orbital s, over all ncoef stored coefficients,
+//     out[s] = 2 sum_G (a_re b_re + a_im b_im) - a_re(G0) b_re(G0),
+// G0 being the last coefficient of each orbital.  The G0 imaginary parts
+// enter the doubled sum as they stand (PINY keeps them at zero).
 //
 // Scratch: g_partials below holds one partial sum per (orbital, slice of
 // the coefficient range).  Every slot a call reads was written earlier in
@@ -66,25 +68,32 @@ __global__ void k_half_dot_finish(const double *__restrict__ part, int nstate, d
 }
 
 std::mutex g_setup_mu;
-double *g_scratch[kMaxDevices] = {};
+bool g_loaded[kMaxDevices] = {};
 
-// Device address of g_partials on the current device, looked up once per
-// device.  The lookup (and the module load it may trigger) happens on the
-// first call on that device, so that first call should come before any
-// stream capture the caller starts.
+// Device address of g_partials in the current device's context.  The first
+// call on a device also loads this file's kernels there (the module load
+// that the first lookup may trigger), so that first call should come before
+// any stream capture the caller starts.  The address itself is looked up on
+// every call, not cached: it belongs to the context current now, and a host
+// that reset the device, or calls from another context, gets the address
+// that is valid there.  The lookup is a host-side query, not a stream
+// operation.
 int scratch_for(int dev, double **p) {
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch[dev]) {
-    double *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_partials);
-    if (e != cudaSuccess) return sdft::set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
-    cudaFuncAttributes fa;
-    if ((e = cudaFuncGetAttributes(&fa, k_half_dot_partials)) != cudaSuccess ||
-        (e = cudaFuncGetAttributes(&fa, k_half_dot_finish)) != cudaSuccess)
-      return sdft::set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
-    g_scratch[dev] = ptr;
+  {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!g_loaded[dev]) {
+      cudaFuncAttributes fa;
+      cudaError_t e;
+      if ((e = cudaFuncGetAttributes(&fa, k_half_dot_partials)) != cudaSuccess ||
+          (e = cudaFuncGetAttributes(&fa, k_half_dot_finish)) != cudaSuccess)
+        return sdft::set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
+      g_loaded[dev] = true;
+    }
   }
-  *p = g_scratch[dev];
+  double *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_partials);
+  if (e != cudaSuccess) return sdft::set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
+  *p = ptr;
   return SDFT_OK;
 }
 

@@ -59,11 +59,18 @@ def diamond_positions(nrep, a0=A0_SI):
 
 
 def make_system(nrep=1, grid=(24, 24, 24), a0=A0_SI, strain=(0.0, 0.0, 0.0), disp_sigma=0.0, seed=0,
-                ecut=ECUT_HA, with_kb=True):
+                ecut=ECUT_HA, with_kb=True, gvec=None):
     """Orthorhombic Si supercell (nrep: n or (n1, n2, n3) conventional cells).
     Returns a dict with the cell, G sphere, V_KS (filter layout), KB
-    description and electron count."""
-    from . import setkvec3d_sm  # noqa: PLC0415  (package-relative)
+    description and electron count.
+
+    gvec(hmat, ecut, kmax) -> (ka, kb, kc, ibreak1, ibreak2) lists the half
+    G sphere in PINY order; the default is the library's setkvec3d_sm.  This
+    module needs nothing else from the package, so a caller that must not
+    load the library (the reference's CPU arm of the benchmark) can load it
+    on its own and pass its own G-vector routine."""
+    if gvec is None:
+        from . import setkvec3d_sm as gvec  # noqa: PLC0415  (package-relative)
     rng = np.random.default_rng(seed)
     r = _reps(nrep)
     L = np.array([a0 * r[i] * (1.0 + strain[i]) for i in range(3)])
@@ -74,7 +81,7 @@ def make_system(nrep=1, grid=(24, 24, 24), a0=A0_SI, strain=(0.0, 0.0, 0.0), dis
         pos = pos + rng.normal(0.0, disp_sigma, size=pos.shape)
     n1, n2, n3 = grid
     kmax = [int(math.ceil(math.sqrt(2 * ecut) * Li / (2 * math.pi))) + 1 for Li in L]
-    ka, kb, kc, ib1, ib2 = setkvec3d_sm(hmat, ecut, kmax)
+    ka, kb, kc, ib1, ib2 = gvec(hmat, ecut, kmax)
     v = local_potential(pos, L, grid)
     kbd = kb_projectors(pos, ecut, L) if with_kb else None
     return dict(hmat=hmat, L=L, pos=pos, natm=len(pos), grid=tuple(grid), ka=ka, kb=kb, kc=kc, ib1=ib1, ib2=ib2,

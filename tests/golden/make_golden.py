@@ -5,7 +5,8 @@ oracle/build_ref.sh has produced oracle/_ref/libpinyref.so (the reference's
 filter.c, normh.c, density.c, gen-noise.c, calc-chempot-chebyshev.c,
 coeff.c, ... compiled in place).  The fixture pins the oracle and the CUDA
 path on machines without the reference tree (hpsi, the KB atomic forces of
-calcNlPseudoPostScf, filters, moments, coefficients, noise and density).
+calcNlPseudoPostScf, filters, moments, the chemical potential of
+calcChemPotCheby, coefficients, noise and density).
 
   python tests/golden/make_golden.py
 
@@ -61,6 +62,13 @@ def main():
     out.update(noise_re=nr, noise_im=ni, density=r.density(nr, ni))
     out.update(coeff_cheby_L64=R.cheby_coeff(64, 40.0, 19.0, 1000.0, 0.2, 1),
                coeff_cheby_L128_sqrt=R.cheby_coeff(128, 40.0, 19.0, 1000.0, 0.2, 2))
+    # mu by the reference's calcChemPotCheby on the moments of 8 noise orbitals
+    nr8, ni8 = r.noise(8, 10.0)
+    cemin, cemax, cL = -1.2, 42.0, 64
+    mu, ne = r.chem_pot(nr8, ni8, cL, cemin, cemax, 1000.0, 2.0, s["num_elec"], 0.2, 0.05)
+    out.update(chempot_moments=r.moments(nr8, ni8, cL, 2.0 / (cemax - cemin), 0.5 * (cemin + cemax)) / 8,
+               chempot_args=np.array([cL, cemin, cemax, 1000.0, 2.0, s["num_elec"], 0.2, 0.05]),
+               chempot_mu=np.array(mu), chempot_ne=np.array(ne))
     gs, q = R.gaussran2(1001, 10.0)
     out.update(gaussran2_seed10=gs, gaussran2_seed10_next=np.array(q),
                round_fft=np.array([[n, R.round_fft(n)] for n in (1000, 2048, 8192, 16384)]))

@@ -1,0 +1,208 @@
+"""GPU parity at the headline size: the 512-atom Si cell on the 96^3 grid.
+
+These runs go through the kernel instances that the 512-atom workload uses:
+- the 96-point column FFTs of stages A and C, FP64 and FP32;
+- the 96x96 plane FFTs of stage B, and the density and noise plane kernels;
+- the KB GEMMs at full shape: 2048 projectors, K = 2 * 52208, 512 orbitals,
+  with the split-K that the cost model picks for that shape.
+
+Each filtered orbital depends on its own input orbital only. So the device
+processes all 512 orbitals in one call, and a sample of them is checked
+against the CPU oracle, which runs on the sampled orbitals alone (one thread
+per orbital pair; the oracle's ctypes calls release the interpreter lock).
+
+Tolerances (rel-L2 against the oracle):
+- FP64: H.psi 1e-12, the nonlocal energy 1e-12, filter 1e-10, noise 1e-13,
+  density 1e-12;
+- mixed precision: H.psi 2e-7, filter 1e-6.
+"""
+import concurrent.futures as cf
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+NSTO = 512
+# orbital pairs sampled from the first, a middle and the last 128-orbital GEMM tile
+SAMPLE_PAIRS = (0, 127, 255)
+
+
+@pytest.fixture(scope="module")
+def sys3(wl):
+    return wl.make_system(4, (96, 96, 96))
+
+
+@pytest.fixture(scope="module")
+def oracles(sys3):
+    """One oracle object per sampled pair, so that the threads share no scratch."""
+    return [O.OracleSys(sys3) for _ in SAMPLE_PAIRS]
+
+
+def _ctx(pkg, s, prec):
+    c = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=NSTO)
+    c.set_vks(s["vks"])
+    c.set_kb(s["kb_desc"])
+    return c
+
+
+def _rand(nc, ns, seed):
+    rng = np.random.default_rng(seed)
+    cr = rng.standard_normal(ns * nc)
+    ci = rng.standard_normal(ns * nc)
+    ci.reshape(ns, nc)[:, -1] = 0.0
+    return cr, ci
+
+
+def _pair(a, nc, p):
+    return a[2 * p * nc:(2 * p + 2) * nc]
+
+
+def _sample(a, nc):
+    return np.concatenate([_pair(a, nc, p) for p in SAMPLE_PAIRS])
+
+
+def _on_sample(oracles, fn):
+    """fn(oracle, pair) for every sampled pair, in threads; results in pair order."""
+    with cf.ThreadPoolExecutor(len(SAMPLE_PAIRS)) as ex:
+        return list(ex.map(fn, oracles, SAMPLE_PAIRS))
+
+
+@pytest.fixture(scope="module")
+def orbitals(sys3):
+    return _rand(sys3["ncoef"], NSTO, 96)
+
+
+@pytest.fixture(scope="module")
+def oracle_hpsi(sys3, oracles, orbitals):
+    nc = sys3["ncoef"]
+    cr, ci = orbitals
+    res = _on_sample(oracles, lambda o, p: o.hpsi(_pair(cr, nc, p), _pair(ci, nc, p), want_enl=True))
+    return (np.concatenate([r[0] for r in res]), np.concatenate([r[1] for r in res]), sum(r[2] for r in res))
+
+
+def test_hpsi_96_fp64(pkg, sys3, orbitals, oracle_hpsi):
+    """FP64 H.psi of 512 orbitals at 96^3 (config-3 GEMM shapes)."""
+    nc = sys3["ncoef"]
+    c = _ctx(pkg, sys3, pkg.SDFT_PREC_FP64)
+    try:
+        fr, fi = c.calc_coef_force(*orbitals)
+        orr, oi, oe = oracle_hpsi
+        assert rel_l2(np.concatenate([_sample(fr, nc), _sample(fi, nc)]), np.concatenate([orr, oi])) < 1e-12
+        # the nonlocal energy of the sampled orbitals alone
+        _, _, e = c.calc_coef_force(_sample(orbitals[0], nc), _sample(orbitals[1], nc), want_enl=True)
+        assert abs(e - oe) < 1e-12 * abs(oe)
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("prec_name", ["SDFT_PREC_MIXED", "SDFT_PREC_MIXED_FAST"])
+def test_hpsi_96_mixed(pkg, sys3, orbitals, oracle_hpsi, prec_name):
+    """Mixed H.psi of 512 orbitals at 96^3: FP32 plane/column FFTs, the
+    INT8 Ozaki tcgen05 GEMMs at 2048 projectors x K = 2 * 52208 x 512 orbitals."""
+    nc = sys3["ncoef"]
+    c = _ctx(pkg, sys3, getattr(pkg, prec_name))
+    try:
+        fr, fi = c.calc_coef_force(*orbitals)
+        orr, oi, _ = oracle_hpsi
+        tol = 2e-7 if prec_name == "SDFT_PREC_MIXED" else 6e-7
+        assert rel_l2(np.concatenate([_sample(fr, nc), _sample(fi, nc)]), np.concatenate([orr, oi])) < tol
+        c.sync()
+    finally:
+        c.close()
+
+
+def test_noise_96(pkg, sys3, oracles):
+    """Device noise for 512 orbitals at 96^3; the first four orbitals of the
+    sequential stream against the oracle's genNoiseOrbitalReal."""
+    nc = sys3["ncoef"]
+    c = _ctx(pkg, sys3, pkg.SDFT_PREC_FP64)
+    try:
+        cr, ci = c.genNoiseOrbitalReal(NSTO, seed=10.0)
+        orr, oi = oracles[0].noise(4, seed=10.0)
+        assert rel_l2(np.concatenate([cr[:4 * nc], ci[:4 * nc]]), np.concatenate([orr, oi])) < 1e-13
+    finally:
+        c.close()
+
+
+def test_density_96(pkg, sys3, oracles):
+    """Density of 64 orbitals at 96^3 (32 pair partials in the fixed-order
+    reduction) against the oracle, summed over four threads' shares."""
+    nc = sys3["ncoef"]
+    cr, ci = _rand(nc, 64, 7)
+    c = _ctx(pkg, sys3, pkg.SDFT_PREC_FP64)
+    try:
+        rho = c.rhoCalcRealStoHybrid(cr, ci)
+    finally:
+        c.close()
+    chunks = [slice(16 * k * nc, 16 * (k + 1) * nc) for k in range(4)]
+    objs = oracles + [O.OracleSys(sys3)]
+    with cf.ThreadPoolExecutor(4) as ex:
+        parts = list(ex.map(lambda o, sl: o.density(cr[sl], ci[sl]), objs[:4], chunks))
+    orho = parts[0] + parts[1] + parts[2] + parts[3]
+    assert rel_l2(rho, orho) < 1e-12
+    # Parseval: sum(rho)/N equals the summed half-sphere norms
+    tot = sum(2 * np.dot(cr[i * nc:(i + 1) * nc], cr[i * nc:(i + 1) * nc]) +
+              2 * np.dot(ci[i * nc:(i + 1) * nc], ci[i * nc:(i + 1) * nc]) - cr[i * nc + nc - 1] ** 2
+              for i in range(64))
+    assert abs(rho.sum() / rho.size - tot) < 1e-10 * tot
+
+
+L96 = 8
+
+
+@pytest.fixture(scope="module")
+def filter_inputs(pkg, sys3):
+    emin, emax = -1.0, 45.0
+    scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+    ec = pkg.calcChebyCoeff(L96, emax - emin, em, 1000.0, 0.2)
+    c = _ctx(pkg, sys3, pkg.SDFT_PREC_FP64)
+    try:
+        cr, ci = c.genNoiseOrbitalReal(NSTO, seed=3.0)
+    finally:
+        c.close()
+    return cr, ci, ec, scale, em
+
+
+@pytest.fixture(scope="module")
+def oracle_filter(sys3, oracles, filter_inputs):
+    nc = sys3["ncoef"]
+    cr, ci, ec, scale, em = filter_inputs
+    res = _on_sample(oracles, lambda o, p: o.filter_cheby(_pair(cr, nc, p), _pair(ci, nc, p), ec, 1, scale, em))
+    return np.concatenate([r[0][0] for r in res]), np.concatenate([r[1][0] for r in res])
+
+
+@pytest.mark.parametrize("prec_name,tol", [("SDFT_PREC_FP64", 1e-10), ("SDFT_PREC_MIXED", 1e-6)])
+def test_filter_cheby_96(pkg, sys3, oracles, filter_inputs, oracle_filter, prec_name, tol):
+    """Chebyshev filter (L = 8) of 512 noise orbitals at 96^3: stage A once,
+    then the fused stage B / hot stage C loop with the recurrence and the
+    filter sum, and the density of the sampled filtered orbitals."""
+    nc = sys3["ncoef"]
+    cr, ci, ec, scale, em = filter_inputs
+    c = _ctx(pkg, sys3, getattr(pkg, prec_name))
+    try:
+        (sr,), (si,) = c.filterChebyPolyHerm(cr, ci, ec, 1, scale, em)
+        osr, osi = oracle_filter
+        gr, gi = _sample(sr, nc), _sample(si, nc)
+        assert rel_l2(np.concatenate([gr, gi]), np.concatenate([osr, osi])) < tol
+        if prec_name == "SDFT_PREC_FP64":
+            rho = c.rhoCalcRealStoHybrid(gr, gi)
+            assert rel_l2(rho, oracles[0].density(osr, osi)) < 1e-10
+    finally:
+        c.close()
+
+
+def test_moments_96(pkg, sys3, oracles, filter_inputs):
+    """Chebyshev moments (L = 8) of two noise orbitals at 96^3."""
+    nc = sys3["ncoef"]
+    cr, ci, _, scale, em = filter_inputs
+    c = _ctx(pkg, sys3, pkg.SDFT_PREC_FP64)
+    try:
+        m = c.calcChebyMoments(cr[:2 * nc], ci[:2 * nc], L96, scale, em)
+    finally:
+        c.close()
+    om = oracles[0].moments(cr[:2 * nc], ci[:2 * nc], L96, scale, em)
+    assert rel_l2(m, om) < 1e-10

@@ -132,3 +132,25 @@ def test_noise_and_density_pinned(wl, grid, strain):
     rho_r = r.density(*b)
     rho_o = o.density(*b)
     assert rel_l2(rho_o, rho_r) < 1e-14
+
+
+@pytest.mark.parametrize("init,gap", [(0.2, 0.05), (1.5, 0.1), (-0.8, 0.1), (0.25, 0.4)])
+def test_chempot_pinned(pkg, wl, sys1, init, gap):
+    """mu by the reference's own calcChemPotCheby (calc-chempot-chebyshev.c:30-314:
+    its own moments of the noise, the bracket widened down from 0.2 and 1.5
+    and up from -0.8, one secant step, bisection to 1e-11 Ne) against
+    sdft_chempot_cheby on the same normalised moments; calcNumElecCheby
+    (:918-971) against sdft_num_elec_cheby at mu and two other points."""
+    r = R.RefSys(sys1, 8)
+    cr, ci = r.noise(8, 10.0)
+    emin, emax, L = -1.2, 42.0, 64
+    ediff, em = emax - emin, 0.5 * (emin + emax)
+    mu_r, ne_r = r.chem_pot(cr, ci, L, emin, emax, wl.BETA, wl.OCC, sys1["num_elec"], init, gap)
+    m = r.moments(cr, ci, L, 2.0 / ediff, em) / 8
+    mu, ne = pkg.calcChemPotCheby(L, ediff, em, wl.BETA, wl.OCC, m, sys1["num_elec"], init, gap)
+    assert abs(mu - mu_r) <= 1e-14 * abs(mu_r)
+    assert abs(ne - ne_r) <= 1e-13 * ne_r
+    for x in (mu_r, 0.1, 0.3):
+        a = R.num_elec(L, emin, emax, wl.BETA, wl.OCC, m, x)
+        b = pkg.calcNumElecCheby(L, ediff, em, wl.BETA, x, wl.OCC, m)
+        assert abs(a - b) <= 1e-13 * abs(a)

@@ -48,3 +48,30 @@ def test_half_dots_noalloc_matches_moments(pkg, sys1):
     # more orbitals than the static scratch holds: rejected before any launch
     rc = fn(a_re.data_ptr(), a_im.data_ptr(), a_re.data_ptr(), a_im.data_ptr(), 1, 1025, out.data_ptr(), stream)
     assert rc == 1 and b"1024" in pkg.lib.sdft_last_error()
+
+
+def test_half_dots_noalloc_at_the_limit(pkg):
+    """1024 orbitals (the whole static scratch) of 5000 coefficients, which is
+    not a multiple of the 8 x 256 coefficients one pass of the slices covers,
+    so the last slice of every orbital is partial; against the weighted sum
+    in numpy, twice in a row."""
+    import torch
+
+    ns, nc = 1024, 5000
+    rng = np.random.default_rng(11)
+    host = [rng.standard_normal(ns * nc) for _ in range(4)]
+    ar, ai, br, bi = (h.reshape(ns, nc) for h in host)
+    ref = 2.0 * (np.einsum("sg,sg->s", ar, br) + np.einsum("sg,sg->s", ai, bi)) - ar[:, -1] * br[:, -1]
+    scale = 2.0 * (np.abs(ar * br).sum(axis=1) + np.abs(ai * bi).sum(axis=1))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = [torch.tensor(h, dtype=torch.float64, device=dev) for h in host]
+    out = torch.empty(ns, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for _ in range(2):
+        out.fill_(float("nan"))
+        rc = pkg.lib.sdft_half_dots_noalloc(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), nc,
+                                            ns, out.data_ptr(), stream)
+        assert rc == 0, pkg.lib.sdft_last_error()
+        torch.cuda.synchronize(dev)
+        got = out.cpu().numpy()
+        assert np.all(np.abs(got - ref) <= 1e-13 * scale)

@@ -839,6 +839,15 @@ def run_serve(args):
     errs = [float(np.linalg.norm(a["density"] - b["density"]) / np.linalg.norm(b["density"]))
             for a, b in zip(recs["mixed"], recs["fp64"])]
     m = out_runs["mixed"]
+    # saturation: the mix's service rate with every request queued at once;
+    # then a sustained Poisson stream at 85 % of it (mixed precision)
+    srv = serve.Server(pkg, wl, pkg.SDFT_PREC_MIXED, hbm_budget=150e9, slots=args.slots, workers=args.workers,
+                       priorities=not args.no_priorities, graph=not args.serve_eager)
+    sat_reqs = serve.poisson_requests(wl, args.sat_requests, 1.0, seed=7, big_fraction=0.1)
+    _, sat = srv.run([dict(r, arrival=0.0) for r in sat_reqs], keep_density=False)
+    sat_rate = sat["requests_per_s"]
+    sus_reqs = serve.poisson_requests(wl, args.sustained_requests, 0.85 * sat_rate, seed=9, big_fraction=0.1)
+    _, sus = srv.run(sus_reqs, keep_density=False)
     lat_small = [r["latency"] for r in recs["mixed"] if r["natm"] < 512]
     lat_big = [r["latency"] for r in recs["mixed"] if r["natm"] >= 512]
     out = {
@@ -858,6 +867,12 @@ def run_serve(args):
                        "p50_below_512_atoms": float(np.percentile(lat_small, 50) * 1e3) if lat_small else None,
                        "max_512_atoms": float(max(lat_big) * 1e3) if lat_big else None},
         "mixed": m, "fp64": out_runs["fp64"],
+        "saturation": {"requests": len(sat_reqs), "requests_per_s": sat_rate,
+                       "orbitals_per_s": sat["orbitals_per_s"], "note": "all requests queued at t = 0"},
+        "sustained": {"rate_req_per_s": 0.85 * sat_rate, "fraction_of_saturation": 0.85, "requests": len(sus_reqs),
+                      "completed": sus["completed"], "refused": sus["refused"], "failed": sus["failed"],
+                      "p50_ms": sus.get("p50_ms"), "p99_ms": sus.get("p99_ms"), "mean_ms": sus.get("mean_ms"),
+                      "orbitals_per_s": sus.get("orbitals_per_s")},
         "mixed_speedup": m["orbitals_per_s"] / out_runs["fp64"]["orbitals_per_s"],
         "density_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
                                          "per_request": [[int(recs["mixed"][i]["natm"]), int(reqs[i]["nsto"]),
@@ -921,6 +936,10 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="time the eager step only")
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
+    ap.add_argument("--sat-requests", type=int, default=64,
+                    help="cfg5: requests queued at once to measure the saturation rate")
+    ap.add_argument("--sustained-requests", type=int, default=200,
+                    help="cfg5: requests of the Poisson stream at 85 %% of the saturation rate")
     ap.add_argument("--workers", type=int, default=16, help="cfg5: host threads preparing requests")
     ap.add_argument("--no-priorities", action="store_true", help="cfg5: all request streams at default priority")
     ap.add_argument("--serve-eager", action="store_true",

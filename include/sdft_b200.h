@@ -186,7 +186,44 @@ int sdft_download_filtered(sdft_ctx *ctx, int nstate, int imu, double *re, doubl
 /* The last density computed on the context (by sdft_density_dev or a batch
  * replay), copied to host or device memory without recomputing it. */
 int sdft_download_density(sdft_ctx *ctx, double *rho);
+/* Waits for the context's stream.  SDFT_ERR_TIMEOUT when a bounded wait in
+ * a tensor-core GEMM gave up since the last sync (that work's results are
+ * not valid); the error word is then cleared, so the context serves later
+ * calls.  No counterpart in the reference (its calls are synchronous).  */
 int sdft_sync(sdft_ctx *ctx);
+/* Diagnostic without a counterpart in the reference: one kernel on the
+ * context's stream waits on an mbarrier that nothing arrives at, through
+ * the GEMMs' bounded-wait helper capped at `polls` polls (1..2^22), gives
+ * up and sets the context's error word; the next sdft_sync reports
+ * SDFT_ERR_TIMEOUT.  Shows on a device that a wait which runs out ends with
+ * an error status the host reads and leaves the context usable. */
+int sdft_ctx_selftest_wait(sdft_ctx *ctx, long long polls);
+/* Cap on the device memory this library allocates on `device`: contexts,
+ * mixers and scratch together, bytes; 0 removes the cap.  An allocation
+ * that would pass it fails with SDFT_ERR_NOMEM like one the device refuses:
+ * the call that needed it returns the error and its context stays usable.
+ * A serving loop with a fixed HBM budget sets it so that an estimate that
+ * was too small cannot take memory from other requests.  No counterpart in
+ * the reference (PINY allocates host memory only). */
+int sdft_set_device_memory_limit(int device, long long bytes);
+/* Bytes this library holds on `device` now (-1 for a bad index).       */
+long long sdft_device_memory_in_use(int device);
+
+/* ---- events (host code that times and orders device work) ------------- */
+/* No counterpart in the reference.  For callers that drive the library
+ * without another CUDA binding (the serving loop, the autotuner):
+ * sdft_set_device makes `device` current for the calling thread;
+ * an event is created with timing on `device`, recorded on a stream (a
+ * context's or batch's stream, NULL = the legacy default stream), queried
+ * (*done = 1 once the work before it has finished, 0 before), waited for,
+ * and two recorded events give the elapsed device time in ms.          */
+int sdft_set_device(int device);
+int sdft_event_create(int device, void **ev);
+int sdft_event_record(void *ev, void *stream);
+int sdft_event_query(void *ev, int *done);
+int sdft_event_synchronize(void *ev);
+int sdft_event_elapsed_ms(void *ev0, void *ev1, float *ms);
+int sdft_event_destroy(void *ev);
 /* Kernel launches issued by the context since creation (own kernels only). */
 long long sdft_launch_count(const sdft_ctx *ctx);
 /* Per-kernel device timing with CUDA events on the context stream.

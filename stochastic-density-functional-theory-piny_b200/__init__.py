@@ -43,6 +43,8 @@ SDFT_PREC_MIXED = 1
 SDFT_PREC_MIXED_FAST = 2
 
 _ERRNAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "STATE", 5: "UNSUPPORTED", 6: "NODEVICE", 7: "TIMEOUT"}
+SDFT_ERR_ARG, SDFT_ERR_CUDA, SDFT_ERR_NOMEM, SDFT_ERR_STATE = 1, 2, 3, 4
+SDFT_ERR_UNSUPPORTED, SDFT_ERR_NODEVICE, SDFT_ERR_TIMEOUT = 5, 6, 7
 
 
 class SdftError(RuntimeError):
@@ -113,6 +115,16 @@ _sig("sdft_cheby_moments_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_
 _sig("sdft_density_dev", C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _dp])
 _sig("sdft_download_filtered", C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp])
 _sig("sdft_sync", C.c_int, [_vp])
+_sig("sdft_ctx_selftest_wait", C.c_int, [_vp, C.c_longlong])
+_sig("sdft_set_device_memory_limit", C.c_int, [C.c_int, C.c_longlong])
+_sig("sdft_device_memory_in_use", C.c_longlong, [C.c_int])
+_sig("sdft_set_device", C.c_int, [C.c_int])
+_sig("sdft_event_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)])
+_sig("sdft_event_record", C.c_int, [_vp, _vp])
+_sig("sdft_event_query", C.c_int, [_vp, C.POINTER(C.c_int)])
+_sig("sdft_event_synchronize", C.c_int, [_vp])
+_sig("sdft_event_elapsed_ms", C.c_int, [_vp, _vp, C.POINTER(C.c_float)])
+_sig("sdft_event_destroy", C.c_int, [_vp])
 _sig("sdft_launch_count", C.c_longlong, [_vp])
 _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
@@ -238,6 +250,62 @@ def genCoeffNewtonHermit(L, chem_pot, beta, samp, samp_unscale):
     return ec
 
 
+def set_device_memory_limit(device, nbytes):
+    """Cap (bytes) on the device memory the library allocates on `device`;
+    0 removes it.  Allocations past the cap raise SdftError(SDFT_ERR_NOMEM)."""
+    _chk(lib.sdft_set_device_memory_limit(int(device), int(nbytes)))
+
+
+def device_memory_in_use(device=0):
+    """Bytes the library holds on `device`."""
+    return int(lib.sdft_device_memory_in_use(int(device)))
+
+
+def set_device(device):
+    """Make `device` the calling thread's current CUDA device."""
+    _chk(lib.sdft_set_device(int(device)))
+
+
+class Event:
+    """A CUDA event (timing enabled) through the library's C ABI."""
+
+    def __init__(self, device=0):
+        p = C.c_void_p()
+        _chk(lib.sdft_event_create(int(device), C.byref(p)))
+        self._p = p
+
+    def record(self, stream_ptr=0):
+        """Record on a stream (an int handle such as Context.stream_ptr; 0 =
+        the legacy default stream)."""
+        _chk(lib.sdft_event_record(self._p, C.c_void_p(int(stream_ptr or 0))))
+        return self
+
+    def query(self):
+        done = C.c_int(0)
+        _chk(lib.sdft_event_query(self._p, C.byref(done)))
+        return bool(done.value)
+
+    def synchronize(self):
+        _chk(lib.sdft_event_synchronize(self._p))
+
+    def elapsed_ms(self, later):
+        """Device milliseconds from this event to `later`."""
+        ms = C.c_float(0.0)
+        _chk(lib.sdft_event_elapsed_ms(self._p, later._p, C.byref(ms)))
+        return float(ms.value)
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib.sdft_event_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def gaussran2(nran, seed):
     q = C.c_double(seed)
     out = np.zeros(max(nran, 1))
@@ -280,6 +348,7 @@ class Context:
         self.hmat = np.asarray(hmat, dtype=np.float64).reshape(3, 3)
         h = _f64(self.hmat.T.reshape(9))
         self.precision = precision
+        self.device = int(device)
         self.max_states = int(max_states)
         p = _vp()
         _chk(lib.sdft_ctx_create(n1, n2, n3, self.ncoef, _i(self.ka), _i(self.kb), _i(self.kc), _d(h), precision,
@@ -329,6 +398,11 @@ class Context:
 
     def sync(self):
         _chk(lib.sdft_sync(self._p))
+
+    def selftest_wait(self, polls=1000):
+        """Queue the bounded-wait self-test (a wait that runs out after
+        `polls` polls); the next sync() raises SdftError(SDFT_ERR_TIMEOUT)."""
+        _chk(lib.sdft_ctx_selftest_wait(self._p, int(polls)))
 
     def set_timing(self, on=True):
         _chk(lib.sdft_ctx_set_timing(self._p, 1 if on else 0))

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 #include <mutex>
+#include <unordered_map>
 #include <algorithm>
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
@@ -76,22 +77,64 @@ static cudaMemPool_t pool_of(int device) {
   return pools[device];
 }
 
+// Bytes this library holds on each device (every allocation goes through
+// dev_alloc / dev_free) and the optional cap of sdft_set_device_memory_limit.
+struct DevAccount {
+  std::mutex mu;
+  std::unordered_map<void *, std::pair<int, size_t>> live;  // pointer -> (device, bytes)
+  long long used[64] = {}, limit[64] = {};
+};
+static DevAccount &dev_account() {
+  static DevAccount a;
+  return a;
+}
+
 int dev_alloc(int device, void *stream, void **p, size_t bytes) {
+  *p = nullptr;
+  if (device < 0 || device >= 64) return set_error(SDFT_ERR_ARG, "device index >= 64");
+  DevAccount &acc = dev_account();
+  {
+    std::lock_guard<std::mutex> lk(acc.mu);
+    if (acc.limit[device] > 0 && acc.used[device] + (long long)bytes > acc.limit[device]) {
+      char b[256];
+      snprintf(b, sizeof b, "device allocation of %zu bytes refused: %lld of the %lld-byte limit in use", bytes,
+               acc.used[device], acc.limit[device]);
+      return set_error(SDFT_ERR_NOMEM, b);
+    }
+    acc.used[device] += (long long)bytes;  // reserved before the allocation, released on failure
+  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaMemPool_t pool = pool_of(device);
   cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaErrorMemoryAllocation;
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // usable from any stream on return
   if (e != cudaSuccess) {
+    if (*p) cudaFreeAsync(*p, st);
     *p = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(acc.mu);
+      acc.used[device] -= (long long)bytes;
+    }
     char b[256];
     snprintf(b, sizeof b, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     return set_error(SDFT_ERR_NOMEM, b);
   }
+  std::lock_guard<std::mutex> lk(acc.mu);
+  acc.live[*p] = {device, bytes};
   return SDFT_OK;
 }
 
 void dev_free(void *p, void *stream) {
-  if (p) cudaFreeAsync(p, reinterpret_cast<cudaStream_t>(stream));
+  if (!p) return;
+  {
+    DevAccount &acc = dev_account();
+    std::lock_guard<std::mutex> lk(acc.mu);
+    auto it = acc.live.find(p);
+    if (it != acc.live.end()) {
+      acc.used[it->second.first] -= (long long)it->second.second;
+      acc.live.erase(it);
+    }
+  }
+  cudaFreeAsync(p, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int dmalloc(sdft_ctx *c, void **p, size_t bytes) {
@@ -156,12 +199,28 @@ static int build_columns(sdft_ctx *ctx, std::vector<int> &cp_gstart, std::vector
   return SDFT_OK;
 }
 
+// Replace the block *p (have bytes) by one of need bytes.  The new block is
+// allocated first, so a refused allocation leaves *p, its contents and the
+// caller's recorded capacity as they were; the old block is freed in stream
+// order after the work queued on it.
+static int grow(sdft_ctx *ctx, void **p, size_t have, size_t need) {
+  void *q = nullptr;
+  int r = dmalloc(ctx, &q, need);
+  if (r) return r;
+  if (*p) {
+    dev_free(*p, ctx->st);
+    ctx->dev_bytes -= (long long)have;
+  }
+  *p = q;
+  return SDFT_OK;
+}
+
 static int ensure_x(sdft_ctx *ctx, int npairs) {
   const size_t csz = ctx->fft64 ? sizeof(double2) : sizeof(float2);
   const size_t need = (size_t)npairs * ctx->n3 * ctx->cols.ncols_pad * csz;
   if (need <= ctx->x_bytes) return SDFT_OK;
-  if (ctx->d_x) { dev_free(ctx->d_x, ctx->st); ctx->dev_bytes -= (long long)ctx->x_bytes; ctx->d_x = nullptr; }
-  DM(ctx->d_x, need);
+  int r = grow(ctx, &ctx->d_x, ctx->x_bytes, need);
+  if (r) return r;
   ctx->x_bytes = need;
   return SDFT_OK;
 }
@@ -179,16 +238,17 @@ static int fp64_chunk(sdft_ctx *ctx, int npairs, int *chunk) {
 
 static int ensure_coef(sdft_ctx *ctx, size_t n) {
   if (n <= ctx->coef_cap) return SDFT_OK;
-  if (ctx->d_coef) { dev_free(ctx->d_coef, ctx->st); ctx->dev_bytes -= (long long)(ctx->coef_cap * 8); }
-  DM(ctx->d_coef, n * sizeof(double));
+  int r = grow(ctx, (void **)&ctx->d_coef, ctx->coef_cap * 8, n * sizeof(double));
+  if (r) return r;
   ctx->coef_cap = n;
   return SDFT_OK;
 }
 
 static int ensure_acc(sdft_ctx *ctx, int nmu) {
   if (nmu <= ctx->acc_nmu) return SDFT_OK;
-  if (ctx->d_acc) { dev_free(ctx->d_acc, ctx->st); ctx->dev_bytes -= (long long)(ctx->acc_nmu * ctx->vec_elems * 8); }
-  DM(ctx->d_acc, (size_t)nmu * ctx->vec_elems * sizeof(double));
+  int r = grow(ctx, (void **)&ctx->d_acc, (size_t)ctx->acc_nmu * ctx->vec_elems * 8,
+               (size_t)nmu * ctx->vec_elems * sizeof(double));
+  if (r) return r;
   CK(cudaMemsetAsync(ctx->d_acc, 0, (size_t)nmu * ctx->vec_elems * sizeof(double), ctx->st));
   ctx->acc_nmu = nmu;
   return SDFT_OK;
@@ -196,8 +256,8 @@ static int ensure_acc(sdft_ctx *ctx, int nmu) {
 
 static int ensure_mom(sdft_ctx *ctx, size_t n) {
   if (n <= ctx->mom_cap) return SDFT_OK;
-  if (ctx->d_mom) { dev_free(ctx->d_mom, ctx->st); ctx->dev_bytes -= (long long)(ctx->mom_cap * 8); }
-  DM(ctx->d_mom, n * sizeof(double));
+  int r = grow(ctx, (void **)&ctx->d_mom, ctx->mom_cap * 8, n * sizeof(double));
+  if (r) return r;
   ctx->mom_cap = n;
   return SDFT_OK;
 }
@@ -650,6 +710,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
     CKF(cudaStreamSynchronize(ctx->st));  // (rng is a local)
     g.kb_rng = ctx->d_kb_rng;
   }
+
   // orbital blocks (zero padded)
   const size_t vb = ctx->vec_elems * sizeof(double);
   DMF(ctx->d_chi, vb);
@@ -768,7 +829,94 @@ extern "C" int sdft_sync(sdft_ctx *ctx) {
   int e = 0;
   CK(cudaMemcpyAsync(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
-  if (e) return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
+  if (e) {
+    // reported once: the word is cleared, so the context serves later calls
+    // (the results of the work that timed out are not valid)
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return set_error(SDFT_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core GEMM pipeline)");
+  }
+  return SDFT_OK;
+}
+
+// ---- events and the calling thread's device (host code without another CUDA binding)
+extern "C" int sdft_set_device(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(SDFT_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return set_error(SDFT_ERR_ARG, "set_device: device index");
+  CK(cudaSetDevice(device));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_create(int device, void **ev) {
+  if (!ev) return set_error(SDFT_ERR_ARG, "event_create: null");
+  *ev = nullptr;
+  int r = sdft_set_device(device);
+  if (r) return r;
+  cudaEvent_t e = nullptr;
+  CK(cudaEventCreateWithFlags(&e, cudaEventDefault));
+  *ev = (void *)e;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_record(void *ev, void *stream) {
+  if (!ev) return set_error(SDFT_ERR_ARG, "event_record: null event");
+  CK(cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_query(void *ev, int *done) {
+  if (!ev || !done) return set_error(SDFT_ERR_ARG, "event_query: null");
+  const cudaError_t e = cudaEventQuery((cudaEvent_t)ev);
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();  // not-ready is not an error of the context
+    *done = 0;
+    return SDFT_OK;
+  }
+  CK(e);
+  *done = 1;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_synchronize(void *ev) {
+  if (!ev) return set_error(SDFT_ERR_ARG, "event_synchronize: null");
+  CK(cudaEventSynchronize((cudaEvent_t)ev));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_elapsed_ms(void *ev0, void *ev1, float *ms) {
+  if (!ev0 || !ev1 || !ms) return set_error(SDFT_ERR_ARG, "event_elapsed: null");
+  CK(cudaEventElapsedTime(ms, (cudaEvent_t)ev0, (cudaEvent_t)ev1));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_event_destroy(void *ev) {
+  if (ev) CK(cudaEventDestroy((cudaEvent_t)ev));
+  return SDFT_OK;
+}
+
+extern "C" int sdft_set_device_memory_limit(int device, long long bytes) {
+  if (device < 0 || device >= 64 || bytes < 0) return set_error(SDFT_ERR_ARG, "memory limit: device 0..63, bytes >= 0");
+  DevAccount &acc = dev_account();
+  std::lock_guard<std::mutex> lk(acc.mu);
+  acc.limit[device] = bytes;
+  return SDFT_OK;
+}
+
+extern "C" long long sdft_device_memory_in_use(int device) {
+  if (device < 0 || device >= 64) return -1;
+  DevAccount &acc = dev_account();
+  std::lock_guard<std::mutex> lk(acc.mu);
+  return acc.used[device];
+}
+
+extern "C" int sdft_ctx_selftest_wait(sdft_ctx *ctx, long long polls) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (polls < 1 || polls > kSelftestMaxPolls) return set_error(SDFT_ERR_ARG, "selftest_wait: polls in 1..2^22");
+  cudaSetDevice(ctx->device);
+  launch_selftest_wait(ctx->d_err, polls, ctx->st);
+  ctx->launches++;
+  CK(cudaGetLastError());
   return SDFT_OK;
 }
 
@@ -981,8 +1129,9 @@ static int density_core(sdft_ctx *ctx, const double *vec, int nstate, double sca
   if ((r = fp64_chunk(ctx, npairs, &chunk))) return r;
   const int nsplit = npairs;  // one |psi|^2 plane set per pair, summed in pair order
   if (nsplit > ctx->rho_split) {
-    if (ctx->d_rho_part) { dev_free(ctx->d_rho_part, ctx->st); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
-    DM(ctx->d_rho_part, (size_t)nsplit * ctx->N * sizeof(double));
+    if ((r = grow(ctx, (void **)&ctx->d_rho_part, (size_t)ctx->rho_split * ctx->N * 8,
+                  (size_t)nsplit * ctx->N * sizeof(double))))
+      return r;
     ctx->rho_split = nsplit;
   }
   if (!ctx->d_rho) DM(ctx->d_rho, (size_t)ctx->N * sizeof(double));
@@ -1043,8 +1192,8 @@ static int noise_core(sdft_ctx *ctx, int nstate, double seed, int np_states, int
   double q = seeds[myid];
   const size_t n = (size_t)nstate * ctx->N;
   if (n > ctx->neg_cap) {
-    if (ctx->d_neg) { dev_free(ctx->d_neg, ctx->st); ctx->dev_bytes -= (long long)ctx->neg_cap; }
-    DM(ctx->d_neg, n);
+    int r0 = grow(ctx, (void **)&ctx->d_neg, ctx->neg_cap, n);
+    if (r0) return r0;
     ctx->neg_cap = n;
   }
   if (!ctx->d_noise_scratch) DM(ctx->d_noise_scratch, noise_scratch_bytes());
@@ -1314,9 +1463,9 @@ static int prepare_filter(sdft_ctx *ctx, int nstate, int L) {
   const int npairs = (nstate + 1) / 2;
   if ((r = ensure_x(ctx, std::max(npairs, 2)))) return r;  // as fp64_chunk needs it
   if (npairs > ctx->rho_split) {
-    if (ctx->d_rho_part) { dev_free(ctx->d_rho_part, ctx->st); ctx->dev_bytes -= (long long)ctx->rho_split * ctx->N * 8; }
-    ctx->d_rho_part = nullptr;
-    if ((r = dmalloc(ctx, (void **)&ctx->d_rho_part, (size_t)npairs * ctx->N * sizeof(double)))) return r;
+    if ((r = grow(ctx, (void **)&ctx->d_rho_part, (size_t)ctx->rho_split * ctx->N * 8,
+                  (size_t)npairs * ctx->N * sizeof(double))))
+      return r;
     ctx->rho_split = npairs;
   }
   if (!ctx->d_rho && (r = dmalloc(ctx, (void **)&ctx->d_rho, (size_t)ctx->N * sizeof(double)))) return r;

@@ -667,4 +667,17 @@ void launch_oz_reduce_slice(const double *part, int split, size_t stride, int ld
                                                  zero_rowmax);
 }
 
+// The bounded wait of the GEMM pipeline, made to run out on purpose: an
+// mbarrier initialised for one arrival that never comes.  mbar_wait polls it
+// `polls` times, sets the error word and returns; the kernel then ends.
+__global__ void k_selftest_wait(int *err, long long polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  const uint32_t a = smem_u32(&bar);
+  mbar_init(a, 1);
+  mbar_wait(a, 0, err, polls);
+}
+
+void launch_selftest_wait(int *err, long long polls, cudaStream_t st) { k_selftest_wait<<<1, 32, 0, st>>>(err, polls); }
+
 }  // namespace sdft

@@ -52,6 +52,11 @@ int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, in
 int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st);
 // split count for `tiles` output tiles over `ktiles` K tiles (<= max_split)
 int oz_choose_split(int tiles, int ktiles, int max_split);
+// Bounded-wait self-test: one thread waits on an mbarrier that nothing
+// arrives at, through the GEMMs' mbar_wait capped at `polls` polls; it gives
+// up and sets *err (the GEMMs' device error word).  polls <= kSelftestMaxPolls.
+constexpr long long kSelftestMaxPolls = 1ll << 22;
+void launch_selftest_wait(int *err, long long polls, cudaStream_t st);
 // rowmax[r] = bits of max_k |x[r][k]| (zeroed first); rows x cols, pitch ldx
 void launch_oz_rowmax(const double *x, int ldx, int rows, int cols, unsigned long long *rowmax, cudaStream_t st);
 // digits (row pitch ld, slice pitch slice_stride bytes) + scales of rows x

@@ -156,8 +156,8 @@ using namespace sdft;
     if (e__ != cudaSuccess) { rc = set_error(SDFT_ERR_CUDA, cudaGetErrorString(e__)); goto done; } \
   } while (0)
 
-int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
-  // release a previous projector set
+// Release the context's projector set (all KB arrays, P = 0).
+static void kb_release(sdft_ctx *ctx) {
   double **old[] = {&ctx->d_pj, &ctx->d_bk, &ctx->d_w, &ctx->d_z, &ctx->d_zwork, &ctx->d_fnl, &ctx->d_gk, &ctx->d_zsave};
   for (double **p : old)
     if (*p) { dev_free(*p, ctx->st); *p = nullptr; }
@@ -178,6 +178,9 @@ int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   ctx->oz = false;
   ctx->dev_bytes -= ctx->kb_bytes;
   ctx->kb_bytes = 0;
+}
+
+static int kb_build(sdft_ctx *ctx, const sdft_kb_desc *kb) {
   if (!kb || kb->natm == 0) return SDFT_OK;
   // whatever this build leaves allocated counts as KB bytes, on every return path
   struct KbBytes {
@@ -368,5 +371,15 @@ done:
                   (void *)d_gz, (void *)d_rows})
     dev_free(p, ctx->st);
   cudaStreamSynchronize(ctx->st);
+  return rc;
+}
+
+// A previous set is released first; a build that fails part way (an
+// allocation refused, say) is released too, so the context is left without
+// projectors -- never with a projector count whose arrays are missing.
+int sdft_build_kb_device(sdft_ctx *ctx, const sdft_kb_desc *kb) {
+  kb_release(ctx);
+  const int rc = kb_build(ctx, kb);
+  if (rc) kb_release(ctx);
   return rc;
 }

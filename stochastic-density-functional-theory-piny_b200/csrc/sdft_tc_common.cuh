@@ -29,8 +29,8 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, int *err) {
-  for (long long i = 0; i < kWaitLimit; i++)
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, int *err, long long limit = kWaitLimit) {
+  for (long long i = 0; i < limit; i++)
     if (mbar_try(a, parity)) return true;
   atomicExch(err, 1);
   return false;

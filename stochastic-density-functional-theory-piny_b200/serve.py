@@ -6,7 +6,8 @@ every request the server
 
 1. waits until a slot is free and its device memory fits in the HBM budget
    (admission); memory is reserved from an estimate and corrected to the
-   context's measured footprint once it exists;
+   context's measured footprint once it exists; a request that could not
+   fit even on an idle device is refused;
 2. prepares it on its own context: V_KS, KB projectors, 20-step Lanczos
    bounds (device resident), noise orbitals generated on the device, Chebyshev moments, mu by
    the FP64 bisection (calcChemPotCheby) and the filter coefficients;
@@ -108,12 +109,34 @@ def estimate_bytes(s, nsto):
     return _bytes(s["grid"], s["ncoef"], cols, s["natm"], nsto)
 
 
+def admission(est, used, budget, busy):
+    """Admission decision for the request at the head of the queue:
+    'refuse' if its estimated footprint alone exceeds the budget (it could
+    never run), 'wait' while it does not fit beside the requests already
+    holding memory, else 'admit'.  An idle device admits whatever fits the
+    budget on its own."""
+    if est > budget:
+        return "refuse"
+    if used + est > budget and busy:
+        return "wait"
+    return "admit"
+
+
 class Server:
     """Continuous-batching loop over a list of timed requests.  Admission and
     completion run on the calling thread; preparation (host set-up, moments,
     capture, launch) runs on a pool of `workers` threads, so the host work of
     new requests overlaps the device work of running ones (the library's calls
-    release the interpreter lock)."""
+    release the interpreter lock).  Device events and the calling threads'
+    device come from the library's C ABI; nothing here needs another CUDA
+    binding.
+
+    While it runs, the library's device memory on the server's device is
+    capped at what it held at the start plus the HBM budget
+    (sdft_set_device_memory_limit), so a request whose footprint was
+    underestimated fails alone with SDFT_ERR_NOMEM instead of taking memory
+    from the others.  Requests whose estimate exceeds the whole budget are
+    refused at admission; both outcomes are recorded per request."""
 
     def __init__(self, pkg, wl, precision, hbm_budget=150e9, slots=16, device=0, tuner=None, workers=4,
                  priorities=True, graph=True):
@@ -127,52 +150,59 @@ class Server:
         self.tuner = tuner
         self.workers = int(workers)
 
-    def _start(self, i, r, t0, t0_ev):
-        import torch
-        torch.cuda.set_device(self.device)
+    def _start(self, i, r, t0):
+        pkg = self.pkg
+        pkg.set_device(self.device)
         t_adm = time.perf_counter() - t0
         tb = time.perf_counter()
         s = self.wl.build_spec(r["spec"])
         build_s = time.perf_counter() - tb
         prio = request_priority(s["grid"], r["nsto"], r["L"]) if self.priorities else None
-        p = prepare(self.pkg, self.wl, s, r["nsto"], r["L"], self.precision, r["seed"], self.device, self.tuner,
+        p = prepare(pkg, self.wl, s, r["nsto"], r["L"], self.precision, r["seed"], self.device, self.tuner,
                     mu=r.get("mu"), priority=prio)
         ctx = p["ctx"]
-        tc = time.perf_counter()
-        if self.graph:  # one captured graph per request, replayed once
-            b = self.pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
-            if prio is not None:
-                b.set_priority(prio)
-            st = torch.cuda.ExternalStream(b.stream_ptr)
-            b.launch()
-        else:  # the same kernels issued directly on the context's stream (no capture / instantiation)
-            b = None
-            st = torch.cuda.ExternalStream(ctx.stream_ptr)
-            ctx.filter_cheby_dev(r["nsto"], p["ec"], 1, p["scale"], p["emean"])
-            ctx.density_dev(r["nsto"], 0, p["occ_over"], want=False)
-        p["phases"].update(build_s=build_s, launch_s=time.perf_counter() - tc)
-        ev = torch.cuda.Event(enable_timing=True)
-        ev.record(st)
+        try:
+            tc = time.perf_counter()
+            if self.graph:  # one captured graph per request, replayed once
+                b = pkg.Batch([ctx], [r["nsto"]], [r["L"]], [p["ec"]], [p["scale"]], [p["emean"]], [p["occ_over"]])
+                if prio is not None:
+                    b.set_priority(prio)
+                st = b.stream_ptr
+                b.launch()
+            else:  # the same kernels issued directly on the context's stream (no capture / instantiation)
+                b = None
+                st = ctx.stream_ptr
+                ctx.filter_cheby_dev(r["nsto"], p["ec"], 1, p["scale"], p["emean"])
+                ctx.density_dev(r["nsto"], 0, p["occ_over"], want=False)
+            p["phases"].update(build_s=build_s, launch_s=time.perf_counter() - tc)
+            ev = pkg.Event(self.device).record(st)
+        except BaseException:
+            ctx.close()
+            raise
         return dict(i=i, ctx=ctx, batch=b, ev=ev, mem=ctx.device_bytes, t_adm=t_adm, prep=p, natm=s["natm"])
 
     def run(self, requests, keep_density=True):
         """requests: list of dicts with arrival (s), spec, nsto, L, seed and
-        optionally mu.  Returns per-request records (latency, orbitals,
-        density ...) and a summary.  Times are seconds from the start of the
-        run: arrivals and admissions on the host clock, completions from CUDA
-        events."""
-        import torch
+        optionally mu.  Returns per-request records and a summary.  A record
+        has status 'done' (latency, orbitals, density ...), 'refused' (its
+        estimate exceeds the budget) or 'failed' (the library refused it, e.g.
+        SDFT_ERR_NOMEM under the cap; error holds the message).  Times are
+        seconds from the start of the run: arrivals and admissions on the
+        host clock, completions from CUDA events."""
         from concurrent.futures import ThreadPoolExecutor
+        pkg = self.pkg
+        pkg.set_device(self.device)
         order = sorted(range(len(requests)), key=lambda i: requests[i]["arrival"])
         pending = deque(order)
         waiting = deque()
         starting, active = [], []
         used = 0.0
         rec = [None] * len(requests)
-        side = torch.cuda.Stream(device=self.device)
-        t0_ev = torch.cuda.Event(enable_timing=True)
+        t0_ev = pkg.Event(self.device)
         t0 = time.perf_counter()
-        t0_ev.record(side)
+        t0_ev.record(0)
+        held0 = pkg.device_memory_in_use(self.device)
+        pkg.set_device_memory_limit(self.device, int(held0 + self.budget))
         peak_active, peak_used = 0, 0.0
         pool = ThreadPoolExecutor(max_workers=self.workers)
         try:
@@ -185,20 +215,32 @@ class Server:
                     i = waiting[0]
                     r = requests[i]
                     est = estimate_spec_bytes(r["spec"], r["nsto"])
-                    if used + est > self.budget and (active or starting):
+                    d = admission(est, used, self.budget, bool(active or starting))
+                    if d == "wait":
                         break
                     waiting.popleft()
+                    if d == "refuse":
+                        rec[i] = dict(status="refused", arrival=r["arrival"], nsto=r["nsto"], L=r["L"],
+                                      reason=f"estimated {est / 1e9:.2f} GB > budget {self.budget / 1e9:.2f} GB")
+                        continue
                     used += est
-                    starting.append((est, pool.submit(self._start, i, r, t0, t0_ev)))
+                    starting.append((i, est, pool.submit(self._start, i, r, t0)))
                 # started requests become active (reservation -> measured footprint)
                 keep = []
-                for est, fut in starting:
+                for i, est, fut in starting:
                     if fut.done():
-                        a = fut.result()
+                        try:
+                            a = fut.result()
+                        except pkg.SdftError as e:
+                            used -= est
+                            r = requests[i]
+                            rec[i] = dict(status="failed", arrival=r["arrival"], nsto=r["nsto"], L=r["L"],
+                                          error=str(e), code=e.code)
+                            continue
                         used += a["mem"] - est
                         active.append(a)
                     else:
-                        keep.append((est, fut))
+                        keep.append((i, est, fut))
                 starting = keep
                 peak_active = max(peak_active, len(active))
                 peak_used = max(peak_used, used)
@@ -212,9 +254,10 @@ class Server:
                             a["ctx"].sync()
                         i = a["i"]
                         rho = a["ctx"].download_density() if keep_density else None
-                        t_done = t0_ev.elapsed_time(a["ev"]) / 1e3
+                        t_done = t0_ev.elapsed_ms(a["ev"]) / 1e3
+                        a["ev"].close()
                         r = requests[i]
-                        rec[i] = dict(arrival=r["arrival"], admitted=a["t_adm"], done=t_done,
+                        rec[i] = dict(status="done", arrival=r["arrival"], admitted=a["t_adm"], done=t_done,
                                       latency=t_done - r["arrival"], nsto=r["nsto"], L=r["L"], natm=a["natm"],
                                       mu=a["prep"]["mu"],
                                       num_elec=float(rho.sum() / rho.size) if rho is not None else None, density=rho,
@@ -229,15 +272,30 @@ class Server:
                 time.sleep(0.0005)
         finally:
             pool.shutdown(wait=True)
-        lat = np.array([r["latency"] for r in rec])
-        span = max(r["done"] for r in rec) - min(r["arrival"] for r in rec)
-        summary = dict(requests=len(rec), orbitals=int(sum(r["nsto"] for r in rec)),
-                       orbitals_per_s=float(sum(r["nsto"] for r in rec) / span), span_s=float(span),
-                       p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
-                       mean_ms=float(lat.mean() * 1e3), peak_active=peak_active, peak_reserved_gb=peak_used / 1e9,
-                       workers=self.workers, slots=self.slots,
-                       prep_mean_s={k: float(np.mean([r["phases"][k] for r in rec])) for k in rec[0]["phases"]})
-        return rec, summary
+            pkg.set_device_memory_limit(self.device, 0)
+            t0_ev.close()
+        return rec, summarize(rec, peak_active, peak_used, self.workers, self.slots)
+
+
+def summarize(rec, peak_active=0, peak_used=0.0, workers=None, slots=None):
+    """Throughput and latency percentiles over the completed requests, with
+    the counts of refused and failed ones."""
+    done = [r for r in rec if r and r.get("status") == "done"]
+    out = dict(requests=len(rec), completed=len(done),
+               refused=sum(1 for r in rec if r and r.get("status") == "refused"),
+               failed=sum(1 for r in rec if r and r.get("status") == "failed"),
+               peak_active=peak_active, peak_reserved_gb=peak_used / 1e9, workers=workers, slots=slots)
+    if not done:
+        return out
+    lat = np.array([r["latency"] for r in done])
+    span = max(r["done"] for r in done) - min(r["arrival"] for r in done)
+    out.update(orbitals=int(sum(r["nsto"] for r in done)),
+               orbitals_per_s=float(sum(r["nsto"] for r in done) / span), span_s=float(span),
+               requests_per_s=float(len(done) / span),
+               p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+               mean_ms=float(lat.mean() * 1e3),
+               prep_mean_s={k: float(np.mean([r["phases"][k] for r in done])) for k in done[0]["phases"]})
+    return out
 
 
 def poisson_requests(wl, n, rate, seed=5, big_fraction=0.1):

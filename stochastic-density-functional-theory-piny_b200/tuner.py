@@ -7,7 +7,8 @@ how many of the 148 SMs work.  The built-in wave-quantisation cost model
 (choice 0) is one candidate; fixed splits are the others.  Each candidate is
 timed on a short Chebyshev filter of the context's resident orbitals (the
 filter kernels themselves, device time by CUDA events on the context
-stream), and the fastest is set on the context.  Results are cached per
+stream, through the library's own event calls), and the fastest is set on
+the context.  Results are cached per
 problem shape (grid, projectors, orbital tiles of 128, precision), in
 memory and optionally in a JSON file.
 
@@ -42,18 +43,19 @@ class Tuner:
         return f"{ctx.n[0]}x{ctx.n[1]}x{ctx.n[2]}/P{nproj}/N{(nstate + 127) // 128}/prec{ctx.precision}"
 
     def _time(self, ctx, nstate, split, scale, emean):
-        import torch
         ctx.set_gemm_split(split)
         ec = np.full(self.steps + 1, 1.0 / (self.steps + 1))
-        ext = torch.cuda.ExternalStream(ctx.stream_ptr)
         ctx.filter_cheby_dev(nstate, ec, 1, scale, emean)  # warm (buffers, caches)
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(ext)
-        ctx.filter_cheby_dev(nstate, ec, 1, scale, emean)
-        b.record(ext)
-        ctx.sync()
-        return a.elapsed_time(b)
+        a, b = self.pkg.Event(ctx.device), self.pkg.Event(ctx.device)
+        try:
+            a.record(ctx.stream_ptr)
+            ctx.filter_cheby_dev(nstate, ec, 1, scale, emean)
+            b.record(ctx.stream_ptr)
+            ctx.sync()
+            return a.elapsed_ms(b)
+        finally:
+            a.close()
+            b.close()
 
     def tune(self, ctx, nstate, nproj, scale=0.1, emean=0.0):
         """Pick and set the projection split-K for (ctx, nstate); returns it."""

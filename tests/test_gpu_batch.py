@@ -56,3 +56,25 @@ def test_serving_same_result_alone_and_in_mix(pkg, wl, graph):
         alone, _ = srv.run([dict(r, arrival=0.0)])
         assert rel_l2(mix[i]["density"], alone[0]["density"]) < 1e-14
         assert abs(mix[i]["num_elec"] - alone[0]["num_elec"]) < 1e-12 * abs(alone[0]["num_elec"])
+
+
+def test_serving_refuses_oversize_and_serves_the_rest(pkg, wl):
+    """Under a 0.5 GB budget the 512-atom request can never fit: it is
+    refused at admission, the small ones complete, and their densities equal
+    the same requests served under the full budget."""
+    serve = _serve_mod(pkg)
+    big = dict(nrep=(4, 4, 4), grid=(96, 96, 96), strain=(0.0, 0.0, 0.0), disp_seed=1, nsto=64, L=16)
+    reqs = [dict(arrival=0.0, spec=SPECS[0], nsto=6, L=24, seed=40.0),
+            dict(arrival=0.0, spec=big, nsto=64, L=16, seed=41.0),
+            dict(arrival=0.001, spec=SPECS[2], nsto=4, L=20, seed=42.0)]
+    assert serve.estimate_spec_bytes(big, 64) > 0.5e9 > serve.estimate_spec_bytes(SPECS[0], 6)
+    small = serve.Server(pkg, wl, pkg.SDFT_PREC_MIXED, hbm_budget=0.5e9, slots=4)
+    rec, summ = small.run(reqs)
+    assert [r["status"] for r in rec] == ["done", "refused", "done"]
+    assert (summ["completed"], summ["refused"], summ["failed"]) == (2, 1, 0)
+    assert "budget" in rec[1]["reason"]
+    assert pkg.device_memory_in_use(0) < 0.5e9  # every completed request released its context
+    full = serve.Server(pkg, wl, pkg.SDFT_PREC_MIXED, hbm_budget=150e9, slots=4)
+    ref, _ = full.run([reqs[0], reqs[2]])
+    assert rel_l2(rec[0]["density"], ref[0]["density"]) < 1e-14
+    assert rel_l2(rec[2]["density"], ref[1]["density"]) < 1e-14

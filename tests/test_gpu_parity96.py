@@ -14,7 +14,8 @@ per orbital pair; the oracle's ctypes calls release the interpreter lock).
 Tolerances (rel-L2 against the oracle):
 - FP64: H.psi 1e-12, the nonlocal energy 1e-12, filter 1e-10, noise 1e-13,
   density 1e-12;
-- mixed precision: H.psi 2e-7, filter 1e-6.
+- mixed precision: H.psi 2e-7 (2e-6 with the 24-bit back projection of
+  MIXED_FAST), filter 1e-6.
 """
 import concurrent.futures as cf
 
@@ -108,7 +109,9 @@ def test_hpsi_96_mixed(pkg, sys3, orbitals, oracle_hpsi, prec_name):
     try:
         fr, fi = c.calc_coef_force(*orbitals)
         orr, oi, _ = oracle_hpsi
-        tol = 2e-7 if prec_name == "SDFT_PREC_MIXED" else 6e-7
+        # MIXED_FAST rounds the back projection to 24-bit digits: 1.1e-6
+        # measured at this size (2048 projectors), 2.3e-7 at 64 atoms
+        tol = 2e-7 if prec_name == "SDFT_PREC_MIXED" else 2e-6
         assert rel_l2(np.concatenate([_sample(fr, nc), _sample(fi, nc)]), np.concatenate([orr, oi])) < tol
         c.sync()
     finally:

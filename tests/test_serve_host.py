@@ -46,3 +46,40 @@ def test_poisson_requests_are_seeded_and_ordered(serve, wl):
     assert np.all(np.diff(t) > 0) and [r["seed"] for r in a] == [r["seed"] for r in b]
     assert [r["nsto"] for r in a] == [r["nsto"] for r in b]
     assert all(r["nsto"] % 2 == 0 and r["L"] % 2 == 0 for r in a)
+
+
+def test_admission_refuses_what_never_fits(serve):
+    gb = 1e9
+    assert serve.admission(151 * gb, 0.0, 150 * gb, busy=False) == "refuse"
+    assert serve.admission(151 * gb, 10 * gb, 150 * gb, busy=True) == "refuse"
+    assert serve.admission(100 * gb, 60 * gb, 150 * gb, busy=True) == "wait"
+    assert serve.admission(100 * gb, 60 * gb, 150 * gb, busy=False) == "admit"  # idle: whatever fits alone
+    assert serve.admission(10 * gb, 60 * gb, 150 * gb, busy=True) == "admit"
+
+
+def test_summary_counts_refused_and_failed(serve):
+    rec = [dict(status="done", arrival=0.0, done=2.0, latency=2.0, nsto=16, phases={"x": 1.0}),
+           dict(status="done", arrival=1.0, done=3.0, latency=2.0, nsto=32, phases={"x": 3.0}),
+           dict(status="refused", arrival=1.5, nsto=256, L=512, reason="too big"),
+           dict(status="failed", arrival=1.7, nsto=64, L=128, error="nomem", code=3)]
+    s = serve.summarize(rec)
+    assert (s["requests"], s["completed"], s["refused"], s["failed"]) == (4, 2, 1, 1)
+    assert s["orbitals"] == 48 and abs(s["orbitals_per_s"] - 16.0) < 1e-12
+    assert s["p50_ms"] == 2000.0 and s["prep_mean_s"] == {"x": 2.0}
+    assert serve.summarize([rec[2]])["completed"] == 0
+
+
+@pytest.mark.parametrize("mod", ["serve", "tuner"])
+def test_serving_and_tuning_need_no_torch(pkg, mod):
+    """The serving loop and the autotuner time and order device work through
+    the library's own event calls: neither imports torch."""
+    import ast
+    import os
+    src = open(os.path.join(os.path.dirname(pkg.__file__), mod + ".py")).read()
+    names = set()
+    for node in ast.walk(ast.parse(src)):
+        if isinstance(node, ast.Import):
+            names.update(a.name.split(".")[0] for a in node.names)
+        elif isinstance(node, ast.ImportFrom) and node.module:
+            names.add(node.module.split(".")[0])
+    assert "torch" not in names

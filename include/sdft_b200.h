@@ -30,6 +30,10 @@
  *   sdft_nl_force_dev                 <- calcEnergyForce stodft/calc-nuclei-force.c:33 (nonlocal part:
  *                                        calcNlPseudoPostScf stodft/reduced-energy/energy-wrapper-post-scf.c:224)
  *   sdft_xc_lda_dev                   <- excpot_pz_lda / excpot_pw_lda energy/cp/xc_functionals.c:268,378
+ *   sdft_vks_from_rho                 <- calcRhoStoRecipFullg stodft/density.c:699 + cpGetVksStodft
+ *                                        stodft/reduced-energy/cp-energy-ee-rho-stodft.c:644
+ *   sdft_vks_set_local                <- controlEwdLocPreScf's vext(G) loop
+ *                                        stodft/reduced-energy/cp-energy-eext-stodft.c:340-470
  *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
  *                                        stodft/checkpointIO.c:32,218
  */
@@ -276,6 +280,41 @@ int sdft_nl_force_dev(sdft_ctx *ctx, int nstate, int imu, double occ, int nsto_t
  * rho and vks are device pointers; runs on `stream` and synchronises it. */
 int sdft_xc_lda_dev(int kind, long long n, const double *rho, double *vks, double vol, double *exc,
                     double *muxc, void *stream);
+
+/* ---- the Kohn-Sham potential from the density (SCF caller) ------------- */
+/* A density grid: the half sphere of the density cutoff (0.5|G|^2 <= 4 Ecut,
+ * setkvec3d of interface/cp_ewald/set_cp_ewald.c:525, PINY order, G = 0
+ * last) on an nkf1 x nkf2 x nkf3 grid (edges 2^a 3^b <= 128) that holds it.
+ * hmat as for sdft_ctx_create. */
+typedef struct sdft_vks sdft_vks;
+int sdft_vks_create(int nkf1, int nkf2, int nkf3, const double *hmat, int ncoef, const int *ka,
+                    const int *kb, const int *kc, int device, sdft_vks **out);
+int sdft_vks_destroy(sdft_vks *v);
+/* The local pseudopotential on the density sphere, as controlEwdLocPreScf
+ * forms vext (cp-energy-eext-stodft.c:412-413, 449-455) for a periodic
+ * cell whose local tables carry the whole local potential:
+ *   vext(G) = (1/vol) sum_a v_t(a)(|G|) (cos, -sin)(2 pi k.s_a),
+ *   vext(0) = (1/vol) sum_a gzvps[t(a)],
+ * s_a = h^-1 r_a; v_t by get_vpsnow's cubic on the per-knot Taylor table
+ * vloc[(t*4 + d)*nsplin + knot] (d = 0..3), knots gmin + k dg.  pos is
+ * natm x 3 cartesian (bohr), type[a] in 0..ntype-1 (host arrays).        */
+int sdft_vks_set_local(sdft_vks *v, int natm, const double *pos, int ntype, const int *type, int nsplin,
+                       double gmin_spl, double dg_spl, const double *vloc, const double *gzvps);
+/* calcRhoStoRecipFullg followed by cpGetVksStodft (cp_dual_grid_opt 0,
+ * periodic, LDA or none): rho is nkf1*nkf2*nkf3 doubles in the package
+ * layout (a fastest), the density times the cell volume as the reference
+ * passes it (host or device memory).  rho(G) = (1/N) sum_r rho(r) e^{iG.r}
+ * on the half sphere; V(G) = vext(G) + 4 pi rho(G)/(|G|^2 vol) (G != 0),
+ * V(0) = vext(0); V(r) = sum_G V(G) e^{-iG.r} over G and -G; plus V_xc of
+ * rho/vol when xc_kind is SDFT_XC_PZ_LDA or SDFT_XC_PW_LDA (0: none).
+ * vks_filter receives V_KS in the filter layout, c fastest (host or device
+ * memory: pass it to sdft_ctx_set_vks); rho_g (nullable) receives rho(G),
+ * re[ncoef] then im[ncoef]; energies (nullable) = {E_H, E_ext, E_xc,
+ * mu_xc} as cp_ehart, cp_eext, cp_exc, cp_muxc.  Synchronous.           */
+int sdft_vks_from_rho(sdft_vks *v, const double *rho, int xc_kind, double *vks_filter, double *rho_g,
+                      double *energies);
+/* vext(G) of the last sdft_vks_set_local: re[ncoef], im[ncoef] (host).  */
+int sdft_vks_get_vext(sdft_vks *v, double *re, double *im);
 
 /* ---- density mixing and checkpoint files -------------------------------- */
 /* genDensityMix (stodft/diis.c:34-464) with the densities on the device,

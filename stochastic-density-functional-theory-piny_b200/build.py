@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "lib", "libsdft_b200.so")
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["sdft_host.cpp", "sdft_api.cu", "sdft_kernels.cu", "sdft_kernels2.cu", "sdft_kb.cu", "sdft_gemm_oz.cu",
            "sdft_noalloc.cu", "sdft_noise.cu", "sdft_lanczos.cu",
-           "sdft_mixer.cu", "sdft_xc.cu"]
+           "sdft_mixer.cu", "sdft_xc.cu", "sdft_vks.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-O3"]
 

@@ -67,6 +67,9 @@ def test_allocation_cap_reports_nomem_and_context_stays_usable(pkg, sys1):
         scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
         ec2 = np.stack([pkg.calcChebyCoeff(12, emax - emin, em, 1000.0, mu) for mu in (0.2, 0.3)], axis=1).ravel()
         cr, ci = c.genNoiseOrbitalReal(6, seed=5.0)
+        o = O.OracleSys(sys1)
+        oa, ob = o.filter_cheby(cr, ci, ec2[0::2], 1, scale, em)
+        (a,), (b,) = c.filterChebyPolyHerm(cr, ci, ec2[0::2], 1, scale, em)  # its buffers now exist
         # the two-potential filter needs a second accumulator block: refused under the cap
         held = pkg.device_memory_in_use(dev)
         pkg.set_device_memory_limit(dev, held + 1024)
@@ -84,11 +87,10 @@ def test_allocation_cap_reports_nomem_and_context_stays_usable(pkg, sys1):
             _ctx(pkg, sys1, 6)
         assert e.value.code == pkg.SDFT_ERR_NOMEM
         assert pkg.device_memory_in_use(dev) == after
-        # the context still computes what fits (one potential)
+        # the context still computes what fits (one potential, no new allocation)
         (a,), (b,) = c.filterChebyPolyHerm(cr, ci, ec2[0::2], 1, scale, em)
-        o = O.OracleSys(sys1)
-        oa, ob = o.filter_cheby(cr, ci, ec2[0::2], 1, scale, em)
         assert rel_l2(np.concatenate([a, b]), np.concatenate([oa[0], ob[0]])) < 1e-10
+        assert pkg.device_memory_in_use(dev) == after
         # cap lifted: the refused call now runs and is correct
         pkg.set_device_memory_limit(dev, 0)
         sr, si = c.filterChebyPolyHerm(cr, ci, ec2, 2, scale, em)

@@ -303,9 +303,9 @@ int sdft_vks_set_local(sdft_vks *v, int natm, const double *pos, int ntype, cons
 /* calcRhoStoRecipFullg followed by cpGetVksStodft (cp_dual_grid_opt 0,
  * periodic, LDA or none): rho is nkf1*nkf2*nkf3 doubles in the package
  * layout (a fastest), the density times the cell volume as the reference
- * passes it (host or device memory).  rho(G) = (1/N) sum_r rho(r) e^{iG.r}
+ * passes it (host or device memory).  rho(G) = (1/N) sum_r rho(r) e^{-iG.r}
  * on the half sphere; V(G) = vext(G) + 4 pi rho(G)/(|G|^2 vol) (G != 0),
- * V(0) = vext(0); V(r) = sum_G V(G) e^{-iG.r} over G and -G; plus V_xc of
+ * V(0) = vext(0); V(r) = sum_G V(G) e^{+iG.r} over G and -G; plus V_xc of
  * rho/vol when xc_kind is SDFT_XC_PZ_LDA or SDFT_XC_PW_LDA (0: none).
  * vks_filter receives V_KS in the filter layout, c fastest (host or device
  * memory: pass it to sdft_ctx_set_vks); rho_g (nullable) receives rho(G),

@@ -48,6 +48,9 @@ def lib(adapter=False):
         L.ref_mix_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double]
         L.ref_mix_checkpoint.restype = C.c_int
         L.ref_xc_lda.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, _dp, _dp]
+        L.ref_vks.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_double, _dp, C.c_double, C.c_int, _dp,
+                              C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                              _dp, _dp]
         L.ref_chempot.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
         L.ref_num_elec.restype = C.c_double
@@ -149,6 +152,36 @@ class RefSys:
         self._L.ref_chempot(self._p, cre.size // self.ncoef, _d(cre), _d(cim), L, emin, emax, beta, occ, num_elec,
                             chem_pot_init, gap_init, C.byref(mu), C.byref(ne))
         return mu.value, ne.value
+
+    def vks(self, ecut, vloc, gmin, dg, gzvps_loc, xc, rho_in, cap=1 << 22, q=None, q_pseud=0.0, alp_ewd=1.0):
+        """The reference's density side of the SCF step on this system's
+        cell, atoms and grid (ref_vks): the density sphere (ka, kb, kc),
+        vext, rho(G), V_KS (filter layout) and [E_H, E_ext, E_xc, mu_xc].
+        With atom charges q: also the local-pseudopotential + Ewald
+        reciprocal forces [natm, 3] and [vrecip, vself, vbgr]."""
+        rho_in = f64(rho_in)
+        n = C.c_int(0)
+        ka, kb, kc = (np.zeros(cap, np.int32) for _ in range(3))
+        vr, vi, rr, ri = (np.zeros(cap) for _ in range(4))
+        v = np.zeros(self.N)
+        e = np.zeros(4)
+        vloc = f64(vloc)
+        qa = f64(q) if q is not None else None
+        f = np.zeros(3 * self.natm)
+        ee = np.zeros(3)
+        rc = self._L.ref_vks(self._p, ecut, vloc.size // 4, gmin, dg, _d(vloc), gzvps_loc, int(xc), _d(rho_in), cap,
+                             C.byref(n), _i(ka),
+                             _i(kb), _i(kc), _d(vr), _d(vi), _d(rr), _d(ri), _d(v), _d(e),
+                             _d(qa) if qa is not None else None, q_pseud, alp_ewd,
+                             _d(f) if qa is not None else None, _d(ee))
+        if rc:
+            raise RuntimeError("ref_vks: density sphere larger than cap")
+        k = n.value
+        out = dict(ka=ka[:k], kb=kb[:k], kc=kc[:k], vext_re=vr[:k], vext_im=vi[:k], rhog_re=rr[:k],
+                   rhog_im=ri[:k], vks=v, energies=e)
+        if qa is not None:
+            out.update(force=f.reshape(self.natm, 3), ewald=ee)
+        return out
 
     def moments(self, cre, cim, L, scale, emean):
         cre, cim = f64(cre), f64(cim)

@@ -41,6 +41,20 @@ void filterNewtonPolyHerm(CP *, CLASS *, GENERAL_DATA *, int);
 void calcChebyMoments(CP *, CLASS *, GENERAL_DATA *, int);
 void calcChemPotCheby(CP *, CLASS *, GENERAL_DATA *, int);
 double calcNumElecCheby(CP *, double, double *);
+void countkvec3d(int *, double, int *, double *);
+void setkvec3d(int, double, int *, double *, int *, int *, int *, int *, int *, int, double *, double *, double *);
+void controlEwdLocPreScf(CLATOMS_INFO *, CLATOMS_POS *, CELL *, PTENS *, EWALD *, CPEWALD *, CPSCR *, PSEUDO *,
+                         EWD_SCR *, CPOPTS *, ATOMMAPS *, double *, double *, COMMUNICATE *, FOR_SCR *, int, int);
+void calcRhoStoRecipFullg(CPEWALD *, CPSCR *, CPCOEFFS_INFO *, EWALD *, CELL *, double *, double *, double *,
+                          double *, double *, double *, double *, double *, double *, int, int, int, COMMUNICATE *,
+                          PARA_FFT_PKG3D *, PARA_FFT_PKG3D *);
+void control_ewd_loc(CLATOMS_INFO *, CLATOMS_POS *, CELL *, PTENS *, EWALD *, CPEWALD *, CPSCR *, PSEUDO *, EWD_SCR *,
+                     CPOPTS *, ATOMMAPS *, double *, double *, COMMUNICATE *, FOR_SCR *, int, int);
+void ewald3d_selfbgr_cp(CLATOMS_INFO *, EWALD *, PTENS *, double, double *, double *, int);
+double getdeth(double *);
+void cpGetVksStodft(CPOPTS *, CPSCR *, CPEWALD *, EWALD *, COMMUNICATE *, CP_COMM_STATE_PKG *, CP_COMM_STATE_PKG *,
+                    STAT_AVG *, double *, CELL *, char *, double *, double, double, int, int, int, int, int, int,
+                    PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, int);
 void calcChebyCoeff(STODFTINFO *, STODFTCOEFPOS *, double *, double *, int, double);
 void genSampNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
 void genCoeffNewtonHermit(STODFTINFO *, STODFTCOEFPOS *);
@@ -818,4 +832,162 @@ void ref_xc_lda(int kind, int n, double *rho, double *vks, double vol, double *e
   *muxc = 0.0;
   if (kind == 1) excpot_pz_lda(vks - 1, rho - 1, exc, muxc, 2 * n, 2 * n, vol, 0, 0, pvten, 0);
   else excpot_pw_lda(vks - 1, rho - 1, exc, muxc, 2 * n, 2 * n, vol, 0, 0, pvten, 0);
+}
+
+/* ====================================================================== */
+/* The density side of the SCF step: vext, rho(G), V_KS                   */
+/* ====================================================================== */
+/* On the system's cell, atoms and grid (the reference uses one grid for the
+ * wave functions and the density when cp_dual_grid_opt is 0):
+ *   1. the density sphere 0.5|G|^2 <= 4 ecut by the reference's own
+ *      countkvec3d / setkvec3d (interface/cp_ewald/set_cp_ewald.c:401,525),
+ *      G = 0 appended last, and the FFT package on it
+ *      (create_para_fft_pkg3d / para_fft_gen3d_init);
+ *   2. controlEwdLocPreScf (stodft/reduced-energy/cp-energy-eext-stodft.c:35)
+ *      for vext(G): the local channel is stored as the l = 2 block of the
+ *      spline tables (loc_opt 2), charges zero (no charge correction);
+ *   3. calcRhoStoRecipFullg (stodft/density.c:699) on rho_in (the density
+ *      times the volume, package layout) and cpGetVksStodft
+ *      (stodft/reduced-energy/cp-energy-ee-rho-stodft.c:644) with
+ *      cp_dual_grid_opt 0, periodic, LDA (xc 1 pz_lda, 2 pw_lda).
+ * The system's own V_KS array is left as it was.  Outputs (cap >= ncoef_l):
+ * the sphere, vext, rho(G), V_KS in the filter layout and
+ * energies = {cp_ehart, cp_eext, cp_exc, cp_muxc}. */
+int ref_vks(RefSys *r, double ecut, int nsp_loc, double gmin_loc, double dg_loc,
+            const double *vloc /*[4][nsp_loc]*/, double gzvps_loc, int xc,
+            const double *rho_in, int cap, int *ncoef_out, int *ka, int *kb, int *kc, double *vext_re,
+            double *vext_im, double *rhog_re, double *rhog_im, double *vks, double *energies,
+            const double *q, double q_pseud, double alp_ewd, double *force, double *ewald_e) {
+  CP *cp = &r->cp;
+  CELL *cell = &r->gd.cell;
+  PARA_FFT_PKG3D *sm = &cp->cp_sclr_fft_pkg3d_sm;
+  const int n1 = sm->nkf1, n2 = sm->nkf2, n3 = sm->nkf3, N = n1 * n2 * n3;
+  /* 1. density sphere */
+  int kmaxv[4] = {0, n1, n2, n3};
+  int nktot = 0;
+  countkvec3d(&nktot, ecut, kmaxv, cell->hmati);
+  const int ncoef = nktot + 1;
+  *ncoef_out = ncoef;
+  if (ncoef > cap) return 1;
+  EWALD *ew = &r->gd.ewald;
+  ew->nktot = nktot;
+  ew->kastr = i1(ncoef); ew->kbstr = i1(ncoef); ew->kcstr = i1(ncoef);
+  ew->ibrk1 = i1(ncoef); ew->ibrk2 = i1(ncoef);
+  double gmin_spl, gmin_true, gmax_spl;
+  setkvec3d(nktot, ecut, kmaxv, cell->hmati, ew->kastr, ew->kbstr, ew->kcstr, ew->ibrk1, ew->ibrk2, 1, &gmin_spl,
+            &gmin_true, &gmax_spl);
+  ew->kastr[ncoef] = ew->kbstr[ncoef] = ew->kcstr[ncoef] = 0;
+  for (int i = 0; i < ncoef; i++) { ka[i] = ew->kastr[i + 1]; kb[i] = ew->kbstr[i + 1]; kc[i] = ew->kcstr[i + 1]; }
+  PARA_FFT_PKG3D lg;
+  memset(&lg, 0, sizeof lg);
+  lg.comm = 0; lg.num_proc = 1; lg.myid = 0;
+  lg.nktot = nktot; lg.ncoef = ncoef; lg.nkf1 = n1; lg.nkf2 = n2; lg.nkf3 = n3;
+  lg.threadFlag = 2; lg.igeneric_opt = 0; lg.numThreads = 1; lg.numThreadsFFTW3 = 1;
+  create_para_fft_pkg3d(&lg, ew->kastr, ew->kbstr, ew->kcstr, 0);
+  para_fft_gen3d_init(&lg);
+  /* 2. vext */
+  CPEWALD *cpew = &cp->cpewald;
+  double *ak2_keep = cpew->ak2;
+  cpew->ak2 = d1(ncoef);
+  CPSCR *scr = &cp->cpscr;
+  scr->cpscr_loc.vextr = d1(ncoef); scr->cpscr_loc.vexti = d1(ncoef);
+  scr->cpscr_loc.vextr_loc = d1(ncoef); scr->cpscr_loc.vexti_loc = d1(ncoef);
+  scr->cpscr_loc.dvextr = d1(ncoef); scr->cpscr_loc.dvexti = d1(ncoef);
+  scr->cpscr_rho.rhocr_up = d1(ncoef); scr->cpscr_rho.rhoci_up = d1(ncoef);
+  PSEUDO *ps = &cp->pseudo;
+  /* the spline tables of this call: the local channel's own knots (the KB
+   * knots stop short of the density cutoff); the s and p blocks are not read */
+  const int nsp = nsp_loc;
+  const int nsp_keep = ps->nsplin_g;
+  const double gmin_keep = ps->gmin_spl, dg_keep = ps->dg_spl;
+  ps->nsplin_g = nsp; ps->gmin_spl = gmin_loc; ps->dg_spl = dg_loc;
+  double *keep[8] = {ps->vps0, ps->vps1, ps->vps2, ps->vps3, ps->dvps0, ps->dvps1, ps->dvps2, ps->dvps3};
+  const int nang_keep = ps->n_ang_max;
+  double *nv[4];
+  for (int d = 0; d < 4; d++) {
+    nv[d] = d1(3 * nsp);
+    memcpy(&nv[d][1 + 2 * nsp], vloc + (size_t)d * nsp, sizeof(double) * nsp);  /* local block (l = 2) */
+  }
+  ps->vps0 = nv[0]; ps->vps1 = nv[1]; ps->vps2 = nv[2]; ps->vps3 = nv[3];
+  ps->dvps0 = d1(3 * nsp); ps->dvps1 = d1(3 * nsp); ps->dvps2 = d1(3 * nsp); ps->dvps3 = d1(3 * nsp);
+  ps->n_ang_max = 2;
+  ps->loc_opt = i1(2); ps->loc_opt[1] = 2;
+  ps->q_pseud = d1(2);
+  const double gz_keep = ps->gzvps[1];
+  ps->gzvps[1] = gzvps_loc;
+  r->cls.for_scr.index_atm = i1(4);
+  r->gd.ewald.alp_ewd = 1.0;
+  cp->cpopts.cp_ptens_calc = 0;
+  double vrecip = 0.0, hess = 0.0;
+  controlEwdLocPreScf(&r->cls.clatoms_info, &r->apos, cell, &r->gd.ptens, ew, cpew, scr, ps, &r->cls.ewd_scr,
+                      &cp->cpopts, &r->cls.atommaps, &vrecip, &hess, &cp->communicate, &r->cls.for_scr, 0, 0);
+  for (int i = 0; i < ncoef; i++) { vext_re[i] = scr->cpscr_loc.vextr[i + 1]; vext_im[i] = scr->cpscr_loc.vexti[i + 1]; }
+  /* 3. rho(G) and V_KS */
+  scr->cpscr_rho.rho_up = d1(N);
+  memcpy(&scr->cpscr_rho.rho_up[1], rho_in, sizeof(double) * N);
+  double *vks_keep = scr->cpscr_rho.v_ks_up;
+  scr->cpscr_rho.v_ks_up = d1(N);
+  CPCOEFFS_INFO *ci = &cp->cpcoeffs_info;
+  ci->cp_elf_calc_frq = 0; ci->cp_laplacian_on = 0;
+  calcRhoStoRecipFullg(cpew, scr, ci, ew, cell, scr->cpscr_rho.rhocr_up, scr->cpscr_rho.rhoci_up,
+                       scr->cpscr_rho.rho_up, NULL, NULL, NULL, NULL, NULL, NULL, 0, 0, 1, &cp->communicate, &lg, &lg);
+  for (int i = 0; i < ncoef; i++) { rhog_re[i] = scr->cpscr_rho.rhocr_up[i + 1]; rhog_im[i] = scr->cpscr_rho.rhoci_up[i + 1]; }
+  CPOPTS *op = &cp->cpopts;
+  op->cp_lda = 1; op->cp_lsda = 0; op->cp_nonint = 0; op->cp_para_opt = 0; op->cp_lyp = 0; op->cp_lypm1 = 0;
+  op->fftw3dFlag = 1;
+  STAT_AVG *sa = &r->gd.stat_avg;
+  sa->cp_ehart = sa->cp_eext = sa->cp_exc = sa->cp_muxc = 0.0;
+  CP_COMM_STATE_PKG up, dn;
+  memset(&up, 0, sizeof up); memset(&dn, 0, sizeof dn);
+  up.nstate = 1; up.num_proc = 1;
+  double ks_offset = 0.0;
+  double pvten[10] = {0};
+  char typ[16];
+  strcpy(typ, xc == 2 ? "pw_lda" : "pz_lda");
+  cpGetVksStodft(op, scr, cpew, ew, &cp->communicate, &up, &dn, sa, &ks_offset, cell, typ, pvten, 0.0, 1.0, 1, 0, 0, 0,
+                 0, 0, &lg, &lg, &lg, &lg, 0);
+  memcpy(vks, &scr->cpscr_rho.v_ks_up[1], sizeof(double) * N);
+  energies[0] = sa->cp_ehart; energies[1] = sa->cp_eext; energies[2] = sa->cp_exc; energies[3] = sa->cp_muxc;
+  /* 4. the local-pseudopotential and Ewald reciprocal forces of the atoms
+   * (calcLocExtPostScf -> control_ewd_loc, energy/cp/cp_energy_eext.c:646,
+   * with the rho(G) of step 3) and the Ewald self and background energies
+   * (ewald3d_selfbgr_cp, :2200) as calcEnergyForce forms them
+   * (stodft/calc-nuclei-force.c:254, 581-590) */
+  if (force) {
+    CLATOMS_INFO *ci2 = &r->cls.clatoms_info;
+    CLATOMS_POS *ap = &r->apos;
+    double *q_keep = ci2->q;
+    ci2->q = d1(r->natm);
+    for (int a = 0; a < r->natm; a++) ci2->q[a + 1] = q[a];
+    ps->q_pseud[1] = q_pseud;
+    ew->alp_ewd = alp_ewd;
+    ew->self_erf = 1.0;
+    cpew->ewaldLocalOpt = 0;
+    cpew->realSparseOpt = 0;
+    ap->fxCl = d1(r->natm); ap->fyCl = d1(r->natm); ap->fzCl = d1(r->natm);
+    for (int a = 1; a <= r->natm; a++) {
+      ap->fx[a] = ap->fy[a] = ap->fz[a] = 0.0;
+      r->cls.ewd_scr.fx2[a] = r->cls.ewd_scr.fy2[a] = r->cls.ewd_scr.fz2[a] = 0.0;
+    }
+    if (!r->gd.ptens.pvten_tot) r->gd.ptens.pvten_tot = d1(9);
+    if (!r->gd.ptens.pvten) r->gd.ptens.pvten = d1(9);
+    double vrec = 0.0, hl = 0.0, vself = 0.0, vbgr = 0.0;
+    control_ewd_loc(ci2, ap, cell, &r->gd.ptens, ew, cpew, scr, ps, &r->cls.ewd_scr, &cp->cpopts, &r->cls.atommaps,
+                    &vrec, &hl, &cp->communicate, &r->cls.for_scr, 0, 0);
+    ewald3d_selfbgr_cp(ci2, ew, &r->gd.ptens, fabs(getdeth(cell->hmat)), &vself, &vbgr, 3);
+    for (int a = 0; a < r->natm; a++) {
+      force[3 * a] = ap->fx[a + 1]; force[3 * a + 1] = ap->fy[a + 1]; force[3 * a + 2] = ap->fz[a + 1];
+    }
+    ewald_e[0] = vrec; ewald_e[1] = vself; ewald_e[2] = vbgr;
+    ci2->q = q_keep;
+  }
+  /* the system as it was */
+  scr->cpscr_rho.v_ks_up = vks_keep;
+  cpew->ak2 = ak2_keep;
+  ps->vps0 = keep[0]; ps->vps1 = keep[1]; ps->vps2 = keep[2]; ps->vps3 = keep[3];
+  ps->dvps0 = keep[4]; ps->dvps1 = keep[5]; ps->dvps2 = keep[6]; ps->dvps3 = keep[7];
+  ps->n_ang_max = nang_keep;
+  ps->gzvps[1] = gz_keep;
+  ps->nsplin_g = nsp_keep; ps->gmin_spl = gmin_keep; ps->dg_spl = dg_keep;
+  return 0;
 }

@@ -1,0 +1,105 @@
+"""Restatement of the density side of the reference's SCF step in numpy.
+
+TEST INFRASTRUCTURE ONLY (the checker of sdft_vks_*; never called by the
+product path).  Follows, on one grid (cp_dual_grid_opt 0), periodic cell,
+spin-unpolarised:
+* controlEwdLocPreScf (stodft/reduced-energy/cp-energy-eext-stodft.c:340-470):
+  vext(G) = (1/vol) sum_a v(|G|) (cos, -sin)(2 pi k.s_a), s_a = h^-1 r_a,
+  v by get_vpsnow's cubic (energy/cp/cp_energy_eext.c:2139), vext(0) =
+  (1/vol) sum_a gzvps;
+* calcRhoStoRecipFullg (stodft/density.c:699): rho(G) = (1/N) sum_r rho(r)
+  e^{-iG.r} (para_fft_gen3d_bck_to_g with its 1/N: the sign its code applies,
+  pinned against the reference run), on the half sphere;
+* cpGetVksStodft (stodft/reduced-energy/cp-energy-ee-rho-stodft.c:644-1007):
+  E_H, E_ext, V(G) = vext + 4 pi rho/(|G|^2 vol), V(r) = sum over G and -G of
+  V(G) e^{+iG.r}, + V_xc of rho/vol (PZ81, energy/cp/xc_functionals.c:268),
+  transposed to the filter layout (c fastest).
+Grids are in the package layout, a fastest: index ia + n1 (ib + n2 ic)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _hinv(hmat):
+    return np.linalg.inv(np.asarray(hmat, dtype=np.float64).reshape(3, 3))
+
+
+def gvec_cart(hmat, ka, kb, kc):
+    """G = 2 pi h^-T k (the xk, yk, zk of the reference's loops)."""
+    hi = _hinv(hmat)
+    k = np.stack([ka, kb, kc], axis=1).astype(np.float64)
+    return 2.0 * math.pi * k @ hi
+
+
+def spline(tab, nsplin, gmin, dg, g):
+    """get_vpsnow on one Taylor-knot table tab[4][nsplin]."""
+    tab = np.asarray(tab, dtype=np.float64).reshape(4, nsplin)
+    iii = np.floor((g - gmin) / dg).astype(np.int64) + 1
+    iii = np.clip(iii, 1, nsplin)
+    h = g - ((iii - 1) * dg + gmin)
+    k = iii - 1
+    return ((tab[3, k] * h + tab[2, k]) * h + tab[1, k]) * h + tab[0, k]
+
+
+def vext(hmat, ka, kb, kc, pos, vtab, nsplin, gmin, dg, gzvps):
+    """vext on the half sphere (G = 0 last), one atom type."""
+    vol = abs(np.linalg.det(np.asarray(hmat, dtype=np.float64).reshape(3, 3)))
+    g = np.linalg.norm(gvec_cart(hmat, ka[:-1], kb[:-1], kc[:-1]), axis=1)
+    v = spline(vtab, nsplin, gmin, dg, g)
+    s = np.asarray(pos, dtype=np.float64) @ _hinv(hmat).T  # s_a = h^-1 r_a
+    k = np.stack([ka[:-1], kb[:-1], kc[:-1]], axis=1).astype(np.float64)
+    cs, sn = np.zeros(len(k)), np.zeros(len(k))
+    for a in range(0, len(k), 4096):  # blocks of G: the phases of one block at a time
+        arg = 2.0 * math.pi * (k[a:a + 4096] @ s.T)  # [G, atom]
+        cs[a:a + 4096] = np.cos(arg).sum(axis=1)
+        sn[a:a + 4096] = np.sin(arg).sum(axis=1)
+    re = np.append(cs * v / vol, len(pos) * gzvps / vol)
+    im = np.append(-sn * v / vol, 0.0)
+    return re, im
+
+
+def pz_lda(rho):
+    """PZ81 exchange-correlation: (V_xc, sum e_xc rho, sum V_xc rho) per point."""
+    r = np.where(rho <= 0.0, 1e-10, rho)
+    rs = (3.0 / (4.0 * np.pi * r)) ** (1.0 / 3.0)
+    x = -(3.0 * r / np.pi) ** (1.0 / 3.0)
+    g, b1, b2, a, b, c, d = -0.14230, 1.05290, 0.33340, 0.03110, -0.0480, 0.00200, -0.01160
+    f1 = 1.0 + b1 * np.sqrt(rs) + b2 * rs
+    f2 = 1.0 + 7.0 / 6.0 * b1 * np.sqrt(rs) + 4.0 / 3.0 * b2 * rs
+    lr = np.log(rs)
+    cf = np.where(rs >= 1.0, g / f1, a * lr + b + c * rs * lr + d * rs)
+    mu = np.where(rs >= 1.0, g / f1 * f2 / f1,
+                  a * lr + (b - a / 3.0) + 2.0 / 3.0 * c * rs * lr + (2.0 * d - c) / 3.0 * rs)
+    return x + mu, 0.75 * np.sum(x * r) + np.sum(cf * r), np.sum((x + mu) * r)
+
+
+def vks_from_rho(grid, hmat, ka, kb, kc, vre, vim, rho_in, xc=True):
+    """Returns (V_KS in the filter layout, rho(G) re, im, [E_H, E_ext, E_xc, mu_xc])."""
+    n1, n2, n3 = grid
+    N = n1 * n2 * n3
+    vol = abs(np.linalg.det(np.asarray(hmat, dtype=np.float64).reshape(3, 3)))
+    z = np.asarray(rho_in, dtype=np.float64).reshape(n3, n2, n1)  # [ic, ib, ia]
+    zg = np.fft.fftn(z) / N  # (1/N) sum_r z e^{-2 pi i k.r}
+    ia, ib, ic = np.mod(ka, n1), np.mod(kb, n2), np.mod(kc, n3)
+    rg = zg[ic, ib, ia]
+    rre, rim = rg.real.copy(), rg.imag.copy()
+    rim[-1] = 0.0
+    g2 = (gvec_cart(hmat, ka, kb, kc) ** 2).sum(axis=1)
+    gh = 4.0 * math.pi / (g2[:-1] * vol)
+    eh = 2.0 * np.sum(0.5 * gh * (rre[:-1] ** 2 + rim[:-1] ** 2))
+    eext = 2.0 * np.sum(vre[:-1] * rre[:-1] + vim[:-1] * rim[:-1]) + vre[-1] * rre[-1]
+    Vr = np.append(vre[:-1] + gh * rre[:-1], vre[-1])
+    Vi = np.append(vim[:-1] + gh * rim[:-1], 0.0)
+    vg = np.zeros((n3, n2, n1), dtype=np.complex128)
+    vg[np.mod(-kc[:-1], n3), np.mod(-kb[:-1], n2), np.mod(-ka[:-1], n1)] = Vr[:-1] - 1j * Vi[:-1]
+    vg[ic, ib, ia] = Vr + 1j * Vi
+    v = (np.fft.ifftn(vg) * N).real  # sum_G V(G) e^{+2 pi i k.r}
+    exc = muxc = 0.0
+    if xc:
+        vx, ex, mx = pz_lda(np.asarray(rho_in, dtype=np.float64).reshape(n3, n2, n1) / vol)
+        v = v + vx
+        exc, muxc = ex * vol / N, mx * vol / N
+    vf = np.ascontiguousarray(np.transpose(v, (2, 1, 0))).reshape(-1)  # [ia][ib][ic], c fastest
+    return vf, rre, rim, np.array([eh, eext, exc, muxc])

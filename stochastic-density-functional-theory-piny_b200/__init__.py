@@ -119,6 +119,11 @@ _sig("sdft_ctx_selftest_wait", C.c_int, [_vp, C.c_longlong])
 _sig("sdft_set_device_memory_limit", C.c_int, [C.c_int, C.c_longlong])
 _sig("sdft_device_memory_in_use", C.c_longlong, [C.c_int])
 _sig("sdft_set_device", C.c_int, [C.c_int])
+_sig("sdft_vks_create", C.c_int, [C.c_int, C.c_int, C.c_int, _dp, C.c_int, _ip, _ip, _ip, C.c_int, C.POINTER(_vp)])
+_sig("sdft_vks_destroy", C.c_int, [_vp])
+_sig("sdft_vks_set_local", C.c_int, [_vp, C.c_int, _dp, C.c_int, _ip, C.c_int, C.c_double, C.c_double, _dp, _dp])
+_sig("sdft_vks_from_rho", C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp])
+_sig("sdft_vks_get_vext", C.c_int, [_vp, _dp, _dp])
 _sig("sdft_event_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)])
 _sig("sdft_event_record", C.c_int, [_vp, _vp])
 _sig("sdft_event_query", C.c_int, [_vp, C.POINTER(C.c_int)])
@@ -583,6 +588,78 @@ class Context:
         im = np.zeros(nstate * self.ncoef)
         _chk(lib.sdft_download_filtered(self._p, nstate, imu, _d(re), _d(im)))
         return re, im
+
+
+class DensityGrid:
+    """The density side of the SCF step on one grid (sdft_vks): the density
+    in G space (calcRhoStoRecipFullg), the Hartree and local-pseudopotential
+    parts of V_KS with the LDA exchange-correlation (cpGetVksStodft), and the
+    local pseudopotential on the density sphere (controlEwdLocPreScf).
+
+    ka, kb, kc: the half sphere of the density cutoff in PINY order with
+    G = 0 last (setkvec3d_sm(hmat, 4 * Ecut, kmax) gives it); the grid must
+    hold it."""
+
+    def __init__(self, n1, n2, n3, hmat, ka, kb, kc, device=0):
+        self.n = (int(n1), int(n2), int(n3))
+        self.ka, self.kb, self.kc = _i32(ka), _i32(kb), _i32(kc)
+        self.ncoef = len(self.ka)
+        h = _f64(np.asarray(hmat, dtype=np.float64).reshape(3, 3).T.reshape(9))
+        p = _vp()
+        _chk(lib.sdft_vks_create(n1, n2, n3, _d(h), self.ncoef, _i(self.ka), _i(self.kb), _i(self.kc), int(device),
+                                 C.byref(p)))
+        self._p = p
+
+    def set_local(self, pos, table, gmin, dg, gzvps, types=None):
+        """Local pseudopotential: per-type Taylor-knot tables table[ntype][4][nsplin]
+        (or one [4][nsplin] table), knots gmin + k dg, G = 0 values gzvps[ntype]."""
+        pos = _f64(np.asarray(pos, dtype=np.float64).reshape(-1, 3))
+        tab = _f64(table)
+        nsplin = tab.shape[-1]
+        ntype = tab.size // (4 * nsplin)
+        types = _i32(np.zeros(len(pos), np.int32) if types is None else types)
+        gz = _f64(np.atleast_1d(gzvps))
+        _chk(lib.sdft_vks_set_local(self._p, len(pos), _d(pos), ntype, _i(types), nsplin, float(gmin), float(dg),
+                                    _d(tab), _d(gz)))
+
+    def vks_from_rho(self, rho, xc_kind=SDFT_XC_PZ_LDA, out_ptr=None):
+        """rho: the density times the volume, package layout (a fastest), a
+        host array or a device address (int).  Returns (V_KS in the filter
+        layout -- None if out_ptr, a device address, received it --,
+        rho(G) re, rho(G) im, [E_H, E_ext, E_xc, mu_xc])."""
+        N = self.n[0] * self.n[1] * self.n[2]
+        if isinstance(rho, (int, np.integer)):
+            rp = C.c_void_p(int(rho))
+        else:
+            rho = _f64(rho)
+            assert rho.size == N
+            rp = C.c_void_p(rho.ctypes.data)
+        v = None
+        if out_ptr is None:
+            v = np.zeros(N)
+            vp = C.c_void_p(v.ctypes.data)
+        else:
+            vp = C.c_void_p(int(out_ptr))
+        rg = np.zeros(2 * self.ncoef)
+        e = np.zeros(4)
+        _chk(lib.sdft_vks_from_rho(self._p, rp, int(xc_kind), vp, _d(rg), _d(e)))
+        return v, rg[:self.ncoef], rg[self.ncoef:], e
+
+    def vext(self):
+        re, im = np.zeros(self.ncoef), np.zeros(self.ncoef)
+        _chk(lib.sdft_vks_get_vext(self._p, _d(re), _d(im)))
+        return re, im
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib.sdft_vks_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class DensityMixer:

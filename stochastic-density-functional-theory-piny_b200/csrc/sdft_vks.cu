@@ -12,13 +12,14 @@
 // vext(G), and a complex FP64 work grid.  The steps of one call:
 //   1. z(r) = rho_in(r) + 0 i, rho_in in the package layout (a fastest), the
 //      density times the cell volume as calcRhoStoRecipFullg receives it;
-//   2. three-axis FFT with exp(+i G.r) and 1/N (para_fft_gen3d_bck_to_g with
-//      scale_opt 1): rho(G) on the half sphere;
+//   2. three-axis FFT with exp(-i G.r) and 1/N (para_fft_gen3d_bck_to_g with
+//      scale_opt 1; the sign is the one its code applies): rho(G) on the
+//      half sphere;
 //   3. E_H = 2 sum_{G!=0} 1/2 (4 pi / (|G|^2 vol)) |rho(G)|^2,
 //      E_ext = 2 sum_{G!=0} Re(vext(G) conj-free dot rho(G)) + vext(0) rho(0),
 //      V(G) = vext(G) + 4 pi rho(G) / (|G|^2 vol) (G != 0), V(0) = vext(0);
 //   4. V(G) and its conjugate at -G on a zeroed grid, three-axis FFT with
-//      exp(-i G.r), no scale (para_fft_gen3d_fwd_to_r), real part;
+//      exp(+i G.r), no scale (para_fft_gen3d_fwd_to_r), real part;
 //   5. + V_xc(rho_in / vol) by PZ81 or PW92 (sdft_xc_lda_dev) when asked;
 //   6. transpose to the filter layout, c fastest.
 // Every reduction is a fixed-order sum over fixed blocks.
@@ -454,14 +455,14 @@ extern "C" int sdft_vks_from_rho(sdft_vks *v, const double *rho, int xc_kind, do
   CKV(cudaMemcpyAsync(v->d_nr, rho, N * sizeof(double), cudaMemcpyDefault, v->st));
   k_pack_real<<<blocks, 256, 0, v->st>>>(v->d_nr, v->d_z, N);
   int r;
-  if ((r = fft3(v, +1, 1.0 / (double)N))) return r;
+  if ((r = fft3(v, -1, 1.0 / (double)N))) return r;
   k_vks_gspace<<<kGBlocks, kGThreads, 0, v->st>>>(v->d_z, v->d_map, v->d_ak2, v->d_vext, v->ncoef, v->vol, v->d_vg,
                                                  v->d_rhog, v->d_part);
   k_vks_energies<<<1, 1, 0, v->st>>>(v->d_part, v->d_vext, v->d_rhog, v->ncoef, v->d_part + 2 * kGBlocks);
   CKV(cudaMemsetAsync(v->d_z, 0, N * sizeof(double2), v->st));
   k_vks_scatter<<<(int)std::min(((long long)v->ncoef + 255) / 256, 148LL * 8), 256, 0, v->st>>>(
       v->d_vg, v->d_map, v->d_mapc, v->ncoef, v->d_z);
-  if ((r = fft3(v, -1, 1.0))) return r;
+  if ((r = fft3(v, +1, 1.0))) return r;
   // d_nr held rho_in; V(r) into d_vpkg, rho_in / vol back into d_nr
   k_vks_real<<<blocks, 256, 0, v->st>>>(v->d_z, v->d_nr, 1.0 / v->vol, v->d_vpkg, v->d_nr, N);
   CKV(cudaGetLastError());

@@ -128,6 +128,47 @@ def _ff(l, g):
     return f, f1, f2, f3
 
 
+def local_table(ecut=ECUT_HA, nsplin=4096):
+    """The local potential of local_potential() in G space, as the reference
+    tabulates a local channel: v(g) = V0 (2 pi sigma^2)^(3/2) exp(-g^2
+    sigma^2 / 2), the Fourier transform of one atom's Gaussian, on knots
+    gmin + k dg up to past the density cutoff (|G| <= 2 sqrt(2 Ecut)), as
+    per-knot Taylor coefficients (f and its first three derivatives over
+    0!, 1!, 2!, 3!).  Returns (table [4][nsplin], gmin, dg, v(0)) for
+    sdft_vks_set_local."""
+    gmax = 2.0 * math.sqrt(2.0 * ecut) * 1.05 + 0.5
+    dg = gmax / (nsplin - 1)
+    g = np.arange(nsplin) * dg
+    s2 = SIGMA_LOC ** 2
+    A = V0_LOC * (2.0 * math.pi * s2) ** 1.5
+    e = np.exp(-0.5 * s2 * g * g)
+    f = A * e
+    f1 = A * (-s2 * g) * e
+    f2 = A * (s2 * s2 * g * g - s2) * e
+    f3 = A * (-(s2 ** 3) * g ** 3 + 3.0 * s2 * s2 * g) * e
+    return np.stack([f, f1, f2 / 2.0, f3 / 6.0]), 0.0, dg, A
+
+
+def density_grid(L, ecut=ECUT_HA):
+    """Per axis, the smallest 2^a 3^b edge that holds the density sphere
+    0.5 |G|^2 <= 4 Ecut of an orthorhombic cell of edges L (2 kmax + 1
+    points, kmax = the sphere's largest |k| on that axis)."""
+    def ok(n):
+        while n % 2 == 0:
+            n //= 2
+        while n % 3 == 0:
+            n //= 3
+        return n == 1
+    out = []
+    for Li in L:
+        kmax = int(math.floor(2.0 * math.sqrt(2.0 * ecut) * Li / (2.0 * math.pi)))
+        n = 2 * kmax + 1
+        while not ok(n):
+            n += 1
+        out.append(n)
+    return tuple(out)
+
+
 def kb_projectors(pos, ecut, L, nsplin=2048):
     gmax = math.sqrt(2 * ecut) * 1.05 + 0.5
     dg = gmax / (nsplin - 1)

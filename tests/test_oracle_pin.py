@@ -154,3 +154,39 @@ def test_chempot_pinned(pkg, wl, sys1, init, gap):
         a = R.num_elec(L, emin, emax, wl.BETA, wl.OCC, m, x)
         b = pkg.calcNumElecCheby(L, ediff, em, wl.BETA, x, wl.OCC, m)
         assert abs(a - b) <= 1e-13 * abs(a)
+
+
+@pytest.fixture(scope="module")
+def dens_sys(wl):
+    """The 8-atom cell on the grid that holds its density sphere (32^3)."""
+    return wl.make_system(1, wl.density_grid(wl.make_system(1, (24, 24, 24))["L"]))
+
+
+def test_vks_pinned(pkg, wl, dens_sys):
+    """The density side of the SCF step: the reference's controlEwdLocPreScf,
+    calcRhoStoRecipFullg and cpGetVksStodft (run by oracle/_ref on its own
+    density sphere from setkvec3d) against the numpy restatement
+    (oracle/vks.py), and the sphere against the library's setkvec3d_sm at
+    4 Ecut."""
+    from oracle import vks as V
+    s = dens_sys
+    r = R.RefSys(s, 4)
+    o = O.OracleSys(s)
+    cr, ci = o.noise(4, 10.0)
+    rho = o.density(cr, ci)
+    rho_in = rho * (s["num_elec"] / rho.mean())
+    vtab, gmin, dg, gz = wl.local_table()
+    ref = r.vks(wl.ECUT_HA, vtab, gmin, dg, gz, 1, rho_in)
+    ka, kb, kc = ref["ka"], ref["kb"], ref["kc"]
+    lk = pkg.setkvec3d_sm(s["hmat"], 4 * wl.ECUT_HA, list(s["grid"]))
+    for x, y in zip(lk[:3], (ka, kb, kc)):
+        assert np.array_equal(x, y)
+    vre, vim = V.vext(s["hmat"], ka, kb, kc, s["pos"], vtab, vtab.shape[1], gmin, dg, gz)
+    assert rel_l2(vre, ref["vext_re"]) < 1e-13 and rel_l2(vim, ref["vext_im"]) < 1e-13
+    vf, rre, rim, e = V.vks_from_rho(s["grid"], s["hmat"], ka, kb, kc, ref["vext_re"], ref["vext_im"], rho_in)
+    assert rel_l2(rre, ref["rhog_re"]) < 1e-13 and rel_l2(rim, ref["rhog_im"]) < 1e-13
+    assert rel_l2(vf, ref["vks"]) < 1e-13
+    assert np.all(np.abs(e - ref["energies"]) <= 1e-13 * np.abs(ref["energies"]))
+    # the local pseudopotential alone, back in real space, is the Gaussian potential of the workload
+    v0, _, _, _ = V.vks_from_rho(s["grid"], s["hmat"], ka, kb, kc, vre, vim, np.zeros_like(rho_in), xc=False)
+    assert rel_l2(v0, s["vks"]) < 1e-10

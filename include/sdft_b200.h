@@ -34,6 +34,8 @@
  *                                        stodft/reduced-energy/cp-energy-ee-rho-stodft.c:644
  *   sdft_vks_set_local                <- controlEwdLocPreScf's vext(G) loop
  *                                        stodft/reduced-energy/cp-energy-eext-stodft.c:340-470
+ *   sdft_vks_local_forces             <- calcLocExtPostScf / control_ewd_loc energy/cp/cp_energy_eext.c:646
+ *                                        + ewald3d_selfbgr_cp :2200 (calc-nuclei-force.c:254,581)
  *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
  *                                        stodft/checkpointIO.c:32,218
  */
@@ -315,6 +317,23 @@ int sdft_vks_from_rho(sdft_vks *v, const double *rho, int xc_kind, double *vks_f
                       double *energies);
 /* vext(G) of the last sdft_vks_set_local: re[ncoef], im[ncoef] (host).  */
 int sdft_vks_get_vext(sdft_vks *v, double *re, double *im);
+/* The local-pseudopotential and Ewald reciprocal-space forces on the atoms
+ * of sdft_vks_set_local, from rho(G) of the last sdft_vks_from_rho: the
+ * part of calcEnergyForce (stodft/calc-nuclei-force.c:254) that
+ * calcLocExtPostScf runs through control_ewd_loc (energy/cp/
+ * cp_energy_eext.c:646, periodic, ewaldLocalOpt 0), plus the Ewald self
+ * and background energies (ewald3d_selfbgr_cp, :2200, calc-nuclei-force.c:
+ * 581-590).  Over the half sphere, per atom a of charge q[a] and type t:
+ *   vt = v_t(|G|) - 4 pi (q[a] - q_pseud[t]) / G^2,
+ *   S(G) = sum_b q_b e^{i 2 pi k.s_b}, preg = e^{-G^2/4 alp^2} 4 pi/(G^2 vol),
+ *   F_a += G [(2 preg Re S q_a + 2 Re rho vt/vol) sin(2 pi k.s_a)
+ *             - (2 preg Im S q_a - 2 Im rho vt/vol) cos(2 pi k.s_a)].
+ * force[natm*3] (hartree/bohr); ewald = {vrecip = sum preg |S|^2,
+ * vself = -alp/sqrt(pi) sum q^2, vbgr = -pi (sum q)^2 / (2 alp^2 vol)}.
+ * The real-space ion-ion Ewald sum (energy_control_inter_real, PINY's
+ * classical force engine) is not part of this call. */
+int sdft_vks_local_forces(sdft_vks *v, const double *q, const double *q_pseud, double alp_ewd, double *force,
+                          double *ewald);
 
 /* ---- density mixing and checkpoint files -------------------------------- */
 /* genDensityMix (stodft/diis.c:34-464) with the densities on the device,

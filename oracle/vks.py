@@ -103,3 +103,42 @@ def vks_from_rho(grid, hmat, ka, kb, kc, vre, vim, rho_in, xc=True):
         exc, muxc = ex * vol / N, mx * vol / N
     vf = np.ascontiguousarray(np.transpose(v, (2, 1, 0))).reshape(-1)  # [ia][ib][ic], c fastest
     return vf, rre, rim, np.array([eh, eext, exc, muxc])
+
+
+def local_forces(hmat, ka, kb, kc, pos, q, q_pseud, vtab, nsplin, gmin, dg, rre, rim, alp):
+    """control_ewd_loc (energy/cp/cp_energy_eext.c:646-1290) for a periodic
+    cell, one atom type, ewaldLocalOpt 0, with ewald3d_selfbgr_cp (:2200):
+    over the half sphere (G != 0),
+      vtemp_a = v(|G|) - 4 pi (q_a - q_pseud) / G^2,
+      S = sum_b q_b e^{i 2 pi k.s_b},  preg = exp(-G^2 / 4 alp^2) 4 pi / (G^2 vol),
+      F_a += G [(2 preg Re S q_a + 2 rho_r vtemp_a / vol) sin(2 pi k.s_a)
+              - (2 preg Im S q_a - 2 rho_i vtemp_a / vol) cos(2 pi k.s_a)],
+      vrecip = sum preg |S|^2;
+    vself = -alp / sqrt(pi) sum q^2, vbgr = -pi (sum q)^2 / (2 alp^2 vol).
+    Returns (F [natm, 3], [vrecip, vself, vbgr])."""
+    h = np.asarray(hmat, dtype=np.float64).reshape(3, 3)
+    vol = abs(np.linalg.det(h))
+    q = np.asarray(q, dtype=np.float64)
+    s = np.asarray(pos, dtype=np.float64) @ _hinv(hmat).T
+    k = np.stack([ka[:-1], kb[:-1], kc[:-1]], axis=1).astype(np.float64)
+    G = gvec_cart(hmat, ka[:-1], kb[:-1], kc[:-1])
+    g2 = (G ** 2).sum(axis=1)
+    v = spline(vtab, nsplin, gmin, dg, np.sqrt(g2))
+    preg = np.exp(-g2 / (4.0 * alp * alp)) * 4.0 * math.pi / (g2 * vol)
+    rre, rim = np.asarray(rre)[:-1], np.asarray(rim)[:-1]  # G != 0
+    F = np.zeros((len(q), 3))
+    vrec = 0.0
+    for a0 in range(0, len(k), 4096):
+        sl = slice(a0, a0 + 4096)
+        arg = 2.0 * math.pi * (k[sl] @ s.T)  # [G, atom]
+        cs, sn = np.cos(arg), np.sin(arg)
+        sr_, si_ = cs @ q, sn @ q
+        vrec += np.sum(preg[sl] * (sr_ * sr_ + si_ * si_))
+        vt = v[sl, None] - 4.0 * math.pi * (q[None, :] - q_pseud) / g2[sl, None]
+        pr = 2.0 * preg[sl, None] * sr_[:, None] * q[None, :] + 2.0 * rre[sl, None] * vt / vol
+        pi_ = 2.0 * preg[sl, None] * si_[:, None] * q[None, :] - 2.0 * rim[sl, None] * vt / vol
+        w = pr * sn - pi_ * cs  # [G, atom]
+        F += w.T @ G[sl]
+    vself = -np.dot(q, q) * alp / math.sqrt(math.pi)
+    vbgr = -0.5 * q.sum() ** 2 * math.pi / (alp * alp * vol)
+    return F, np.array([vrec, vself, vbgr])

@@ -124,6 +124,7 @@ _sig("sdft_vks_destroy", C.c_int, [_vp])
 _sig("sdft_vks_set_local", C.c_int, [_vp, C.c_int, _dp, C.c_int, _ip, C.c_int, C.c_double, C.c_double, _dp, _dp])
 _sig("sdft_vks_from_rho", C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp])
 _sig("sdft_vks_get_vext", C.c_int, [_vp, _dp, _dp])
+_sig("sdft_vks_local_forces", C.c_int, [_vp, _dp, _dp, C.c_double, _dp, _dp])
 _sig("sdft_event_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)])
 _sig("sdft_event_record", C.c_int, [_vp, _vp])
 _sig("sdft_event_query", C.c_int, [_vp, C.POINTER(C.c_int)])
@@ -649,6 +650,17 @@ class DensityGrid:
         re, im = np.zeros(self.ncoef), np.zeros(self.ncoef)
         _chk(lib.sdft_vks_get_vext(self._p, _d(re), _d(im)))
         return re, im
+
+    def local_forces(self, q, q_pseud, alp_ewd):
+        """Local-pseudopotential + Ewald reciprocal forces [natm, 3] from the
+        last vks_from_rho density, and [vrecip, vself, vbgr] (calcLocExtPostScf,
+        ewald3d_selfbgr_cp).  q: per-atom charges; q_pseud: per-type."""
+        q = _f64(q)
+        qp = _f64(np.atleast_1d(q_pseud))
+        f = np.zeros(3 * q.size)
+        e = np.zeros(3)
+        _chk(lib.sdft_vks_local_forces(self._p, _d(q), _d(qp), float(alp_ewd), _d(f), _d(e)))
+        return f.reshape(-1, 3), e
 
     def close(self):
         if getattr(self, "_p", None):

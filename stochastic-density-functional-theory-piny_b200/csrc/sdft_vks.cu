@@ -47,7 +47,11 @@ struct sdft_vks {
   double2 *d_tw = nullptr;                  // exp(-2 pi i t / n_axis), n1 + n2 + n3
   double *d_part = nullptr;                 // reduction partials + results
   double *d_rhog = nullptr;                 // rho(G) re/im of the last call [2][ncoef]
-  bool have_local = false;
+  bool have_local = false, have_rho = false;
+  // kept from sdft_vks_set_local for the atomic forces
+  int natm = 0, ntype = 0;
+  int *d_kabc = nullptr, *d_type = nullptr;  // [3 ncoef], [natm]
+  double *d_frac = nullptr, *d_vgt = nullptr;  // [3 natm], [ntype][ncoef - 1]
 };
 
 namespace sdft {
@@ -232,6 +236,109 @@ __global__ void k_vext(const int *__restrict__ kabc, const double *__restrict__ 
   }
 }
 
+struct Mat3 { double m[9]; };
+constexpr int kFChunks = 8;
+
+// Ewald structure factor of the charges per G != 0:
+// ab[i] = 2 preg (Re S, Im S), S = sum_b q_b e^{i 2 pi k.s_b},
+// preg = exp(-G^2 / 4 alp^2) 4 pi / (G^2 vol); part[b] = block b's sum of preg |S|^2
+__global__ void __launch_bounds__(kGThreads)
+k_ewald_sfac(const int *__restrict__ kabc, const double *__restrict__ frac, const double *__restrict__ q, int natm,
+             int ncoef, Mat3 hi, double vol, double alp, double2 *__restrict__ ab, double *__restrict__ part) {
+  const int nk = ncoef - 1;
+  double vr = 0.0;
+  for (int i = blockIdx.x * kGThreads + threadIdx.x; i < nk; i += kGBlocks * kGThreads) {
+    const double ka = kabc[3 * i], kb = kabc[3 * i + 1], kc = kabc[3 * i + 2];
+    const double xk = (ka * hi.m[0] + kb * hi.m[1] + kc * hi.m[2]) * (2.0 * M_PI);
+    const double yk = (ka * hi.m[3] + kb * hi.m[4] + kc * hi.m[5]) * (2.0 * M_PI);
+    const double zk = (ka * hi.m[6] + kb * hi.m[7] + kc * hi.m[8]) * (2.0 * M_PI);
+    const double g2 = xk * xk + yk * yk + zk * zk;
+    double sr = 0.0, si = 0.0;
+    for (int b = 0; b < natm; b++) {
+      double sn, cs;
+      sincos((ka * frac[3 * b] + kb * frac[3 * b + 1] + kc * frac[3 * b + 2]) * (2.0 * M_PI), &sn, &cs);
+      sr += q[b] * cs;
+      si += q[b] * sn;
+    }
+    const double preg = exp(-g2 / (4.0 * alp * alp)) * 4.0 * M_PI / (g2 * vol);
+    vr += preg * (sr * sr + si * si);
+    ab[i] = make_double2(2.0 * preg * sr, 2.0 * preg * si);
+  }
+  __shared__ double s0[kGThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) vr += __shfl_down_sync(0xffffffffu, vr, o);
+  if ((threadIdx.x & 31) == 0) s0[threadIdx.x >> 5] = vr;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < kGThreads / 32; w++) a += s0[w];
+    part[blockIdx.x] = a;
+  }
+}
+
+// Force partials: block (a, j) sums atom a's terms over G chunk j
+// (control_ewd_loc's loop, energy/cp/cp_energy_eext.c:1120-1175):
+//   vt = v_t(|G|) - 4 pi (q_a - q_pseud_t) / G^2,
+//   F_a += G [(AB.x q_a + 2 rho_r vt / vol) sin(arg) - (AB.y q_a - 2 rho_i vt / vol) cos(arg)]
+__global__ void __launch_bounds__(kGThreads)
+k_loc_force(const int *__restrict__ kabc, const double *__restrict__ frac, const int *__restrict__ type,
+            const double *__restrict__ q, const double *__restrict__ qps, int ncoef, Mat3 hi, double vol,
+            const double *__restrict__ vgt, const double2 *__restrict__ ab, const double *__restrict__ rhog,
+            double *__restrict__ fpart) {
+  const int a = blockIdx.x, j = blockIdx.y, nk = ncoef - 1;
+  const int t = type[a];
+  const double qa = q[a], dq = q[a] - qps[t];
+  const double sa = frac[3 * a], sb = frac[3 * a + 1], sc = frac[3 * a + 2];
+  const int per = (nk + kFChunks - 1) / kFChunks;
+  const int i0 = j * per, i1 = min(nk, i0 + per);
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  for (int i = i0 + threadIdx.x; i < i1; i += kGThreads) {
+    const double ka = kabc[3 * i], kb = kabc[3 * i + 1], kc = kabc[3 * i + 2];
+    const double xk = (ka * hi.m[0] + kb * hi.m[1] + kc * hi.m[2]) * (2.0 * M_PI);
+    const double yk = (ka * hi.m[3] + kb * hi.m[4] + kc * hi.m[5]) * (2.0 * M_PI);
+    const double zk = (ka * hi.m[6] + kb * hi.m[7] + kc * hi.m[8]) * (2.0 * M_PI);
+    const double g2 = xk * xk + yk * yk + zk * zk;
+    const double vt = vgt[(size_t)t * nk + i] - 4.0 * M_PI * dq / g2;
+    double sn, cs;
+    sincos((ka * sa + kb * sb + kc * sc) * (2.0 * M_PI), &sn, &cs);
+    const double2 s = ab[i];
+    const double pr = s.x * qa + 2.0 * rhog[i] * vt / vol;
+    const double pi = s.y * qa - 2.0 * rhog[ncoef + i] * vt / vol;
+    const double w = pr * sn - pi * cs;
+    fx += w * xk;
+    fy += w * yk;
+    fz += w * zk;
+  }
+  __shared__ double r[3][kGThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_down_sync(0xffffffffu, fx, o);
+    fy += __shfl_down_sync(0xffffffffu, fy, o);
+    fz += __shfl_down_sync(0xffffffffu, fz, o);
+  }
+  if ((threadIdx.x & 31) == 0) { r[0][threadIdx.x >> 5] = fx; r[1][threadIdx.x >> 5] = fy; r[2][threadIdx.x >> 5] = fz; }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double acc = 0.0;
+    for (int w = 0; w < kGThreads / 32; w++) acc += r[threadIdx.x][w];
+    fpart[((size_t)a * kFChunks + j) * 3 + threadIdx.x] = acc;
+  }
+}
+
+// chunks of every atom summed in order; out[natm*3] then vrecip from part
+__global__ void k_loc_force_sum(const double *__restrict__ fpart, int natm, const double *__restrict__ part,
+                                double *__restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 3 * natm; e += gridDim.x * blockDim.x) {
+    const int a = e / 3, d = e - 3 * a;
+    double acc = 0.0;
+    for (int j = 0; j < kFChunks; j++) acc += fpart[((size_t)a * kFChunks + j) * 3 + d];
+    out[e] = acc;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double v = 0.0;
+    for (int b = 0; b < kGBlocks; b++) v += part[b];
+    out[3 * natm] = v;
+  }
+}
+
 void inv3(const double *h, double *hi, double *det) {
   const double d = h[0] * (h[4] * h[8] - h[7] * h[5]) - h[3] * (h[1] * h[8] - h[7] * h[2]) +
                    h[6] * (h[1] * h[5] - h[4] * h[2]);
@@ -279,7 +386,7 @@ extern "C" int sdft_vks_destroy(sdft_vks *v) {
   if (!v) return SDFT_OK;
   cudaSetDevice(v->device);
   void *ptrs[] = {v->d_map, v->d_mapc, v->d_ak2, v->d_vext, v->d_vg, v->d_z, v->d_vpkg, v->d_nr, v->d_tw, v->d_part,
-                  v->d_rhog};
+                  v->d_rhog, v->d_kabc, v->d_type, v->d_frac, v->d_vgt};
   for (void *p : ptrs) dev_free(p, v->st);
   if (v->st) {
     cudaStreamSynchronize(v->st);
@@ -436,10 +543,64 @@ extern "C" int sdft_vks_set_local(sdft_vks *v, int natm, const double *pos, int 
     r = ck(cudaGetLastError());
     if (!r) r = ck(cudaStreamSynchronize(v->st));
   }
-  for (void *p : {(void *)d_k, (void *)d_t, (void *)d_f, (void *)d_vg, (void *)d_gz}) dev_free(p, v->st);
+  dev_free(d_gz, v->st);
+  if (r) {
+    for (void *p : {(void *)d_k, (void *)d_t, (void *)d_f, (void *)d_vg}) dev_free(p, v->st);
+    cudaStreamSynchronize(v->st);
+    return r;
+  }
+  // the atoms and the radial values stay for sdft_vks_local_forces
+  for (void *p : {(void *)v->d_kabc, (void *)v->d_type, (void *)v->d_frac, (void *)v->d_vgt}) dev_free(p, v->st);
+  v->d_kabc = d_k; v->d_type = d_t; v->d_frac = d_f; v->d_vgt = d_vg;
+  v->natm = natm; v->ntype = ntype;
   cudaStreamSynchronize(v->st);
-  if (!r) v->have_local = true;
-  return r;
+  v->have_local = true;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_vks_local_forces(sdft_vks *v, const double *q, const double *q_pseud, double alp_ewd,
+                                     double *force, double *ewald) {
+  if (!v || !q || !q_pseud || !force || !ewald || !(alp_ewd > 0.0))
+    return set_error(SDFT_ERR_ARG, "vks_local_forces: bad argument");
+  if (!v->have_local || !v->have_rho)
+    return set_error(SDFT_ERR_STATE, "vks_local_forces: needs sdft_vks_set_local and sdft_vks_from_rho first");
+  cudaSetDevice(v->device);
+  const int natm = v->natm;
+  const int nk = v->ncoef - 1;
+  double *d_q = nullptr, *d_qp = nullptr, *d_fp = nullptr, *d_out = nullptr;
+  double2 *d_ab = nullptr;
+  int r = SDFT_OK;
+  auto ck = [&](cudaError_t e) { return e == cudaSuccess ? SDFT_OK : set_error(SDFT_ERR_CUDA, cudaGetErrorString(e)); };
+  std::vector<double> out(3 * (size_t)natm + 1);
+  Mat3 hi;
+  for (int i = 0; i < 9; i++) hi.m[i] = v->hmati[i];
+  if (!(r = dev_alloc(v->device, v->st, (void **)&d_q, natm * sizeof(double))) &&
+      !(r = dev_alloc(v->device, v->st, (void **)&d_qp, v->ntype * sizeof(double))) &&
+      !(r = dev_alloc(v->device, v->st, (void **)&d_ab, std::max(nk, 1) * sizeof(double2))) &&
+      !(r = dev_alloc(v->device, v->st, (void **)&d_fp, (size_t)natm * kFChunks * 3 * sizeof(double))) &&
+      !(r = dev_alloc(v->device, v->st, (void **)&d_out, out.size() * sizeof(double))) &&
+      !(r = ck(cudaMemcpyAsync(d_q, q, natm * sizeof(double), cudaMemcpyHostToDevice, v->st))) &&
+      !(r = ck(cudaMemcpyAsync(d_qp, q_pseud, v->ntype * sizeof(double), cudaMemcpyHostToDevice, v->st)))) {
+    k_ewald_sfac<<<kGBlocks, kGThreads, 0, v->st>>>(v->d_kabc, v->d_frac, d_q, natm, v->ncoef, hi, v->vol, alp_ewd,
+                                                   d_ab, v->d_part);
+    k_loc_force<<<dim3(natm, kFChunks), kGThreads, 0, v->st>>>(v->d_kabc, v->d_frac, v->d_type, d_q, d_qp, v->ncoef,
+                                                               hi, v->vol, v->d_vgt, d_ab, v->d_rhog, d_fp);
+    k_loc_force_sum<<<(3 * natm + 255) / 256, 256, 0, v->st>>>(d_fp, natm, v->d_part, d_out);
+    r = ck(cudaGetLastError());
+    if (!r) r = ck(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, v->st));
+    if (!r) r = ck(cudaStreamSynchronize(v->st));
+  }
+  for (void *p : {(void *)d_q, (void *)d_qp, (void *)d_ab, (void *)d_fp, (void *)d_out}) dev_free(p, v->st);
+  cudaStreamSynchronize(v->st);
+  if (r) return r;
+  for (int i = 0; i < 3 * natm; i++) force[i] = out[i];
+  // ewald3d_selfbgr_cp (energy/cp/cp_energy_eext.c:2200), self_erf = 1
+  double sq = 0.0, sq2 = 0.0;
+  for (int a = 0; a < natm; a++) { sq += q[a]; sq2 += q[a] * q[a]; }
+  ewald[0] = out[3 * (size_t)natm];
+  ewald[1] = -sq2 * alp_ewd / std::sqrt(M_PI);
+  ewald[2] = -0.5 * sq * sq * M_PI / (alp_ewd * alp_ewd * v->vol);
+  return SDFT_OK;
 }
 
 extern "C" int sdft_vks_from_rho(sdft_vks *v, const double *rho, int xc_kind, double *vks_filter, double *rho_g,
@@ -483,6 +644,7 @@ extern "C" int sdft_vks_from_rho(sdft_vks *v, const double *rho, int xc_kind, do
   if (rho_g) CKV(cudaMemcpyAsync(rho_g, v->d_rhog, 2 * (size_t)v->ncoef * sizeof(double), cudaMemcpyDefault, v->st));
   CKV(cudaMemcpyAsync(e, v->d_part + 2 * kGBlocks, 2 * sizeof(double), cudaMemcpyDeviceToHost, v->st));
   CKV(cudaStreamSynchronize(v->st));
+  v->have_rho = true;
   if (energies) for (int i = 0; i < 4; i++) energies[i] = e[i];
   return SDFT_OK;
 }

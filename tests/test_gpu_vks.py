@@ -97,3 +97,32 @@ def test_scf_step_on_device(pkg, wl):
     finally:
         g.close()
         c.close()
+
+
+@pytest.mark.parametrize("nrep,grid,q_pseud", [(1, (32, 32, 32), 4.0), (1, (32, 32, 32), 3.5),
+                                               (4, (128, 128, 128), 4.0)])
+def test_local_forces(pkg, wl, nrep, grid, q_pseud):
+    """Local-pseudopotential + Ewald reciprocal forces and the Ewald energies
+    (calcLocExtPostScf / ewald3d_selfbgr_cp) on displaced atoms, against the
+    numpy restatement (pinned to the reference's control_ewd_loc), relative
+    to the largest force component: 1e-12."""
+    s = wl.make_system(nrep, grid, disp_sigma=0.05, seed=2, with_kb=nrep == 1)
+    if nrep == 1:
+        o = O.OracleSys(s)
+        cr, ci = o.noise(4, 10.0)
+        rho = o.density(cr, ci)
+    else:
+        rho = 1.0 + 0.5 * np.random.default_rng(5).random(int(np.prod(grid)))
+    rho_in = rho * (s["num_elec"] / rho.mean())
+    q = np.full(s["natm"], 4.0)
+    g, (ka, kb, kc), (vtab, gmin, dg, gz) = _grid_for(pkg, wl, s)
+    try:
+        g.vks_from_rho(rho_in, pkg.SDFT_XC_PZ_LDA)
+        F, e = g.local_forces(q, [q_pseud], 1.2)
+    finally:
+        g.close()
+    vre, vim = V.vext(s["hmat"], ka, kb, kc, s["pos"], vtab, vtab.shape[1], gmin, dg, gz)
+    _, rre, rim, _ = V.vks_from_rho(s["grid"], s["hmat"], ka, kb, kc, vre, vim, rho_in)
+    oF, oe = V.local_forces(s["hmat"], ka, kb, kc, s["pos"], q, q_pseud, vtab, vtab.shape[1], gmin, dg, rre, rim, 1.2)
+    assert np.abs(F - oF).max() < 1e-12 * np.abs(oF).max()
+    assert np.all(np.abs(e - oe) <= 1e-12 * np.abs(oe))

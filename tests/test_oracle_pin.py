@@ -190,3 +190,54 @@ def test_vks_pinned(pkg, wl, dens_sys):
     # the local pseudopotential alone, back in real space, is the Gaussian potential of the workload
     v0, _, _, _ = V.vks_from_rho(s["grid"], s["hmat"], ka, kb, kc, vre, vim, np.zeros_like(rho_in), xc=False)
     assert rel_l2(v0, s["vks"]) < 1e-10
+
+
+@pytest.mark.parametrize("q_pseud", [4.0, 3.5])
+def test_local_forces_pinned(wl, q_pseud):
+    """The local-pseudopotential + Ewald reciprocal forces of calcLocExtPostScf
+    (control_ewd_loc) and the Ewald self / background energies
+    (ewald3d_selfbgr_cp) of the reference against the numpy restatement, with
+    the charge correction on (q_pseud 3.5) and off; and the restatement's
+    force is -dE/dR of E_loc + vrecip at fixed rho(G) (central differences)."""
+    from oracle import vks as V
+    s = wl.make_system(1, (32, 32, 32), disp_sigma=0.05, seed=2)
+    r = R.RefSys(s, 4)
+    o = O.OracleSys(s)
+    cr, ci = o.noise(4, 10.0)
+    rho = o.density(cr, ci)
+    rho_in = rho * (s["num_elec"] / rho.mean())
+    vtab, gmin, dg, gz = wl.local_table()
+    q = np.full(s["natm"], 4.0)
+    ref = r.vks(wl.ECUT_HA, vtab, gmin, dg, gz, 1, rho_in, q=q, q_pseud=q_pseud, alp_ewd=1.2)
+    ka, kb, kc = ref["ka"], ref["kb"], ref["kc"]
+    args = (s["hmat"], ka, kb, kc)
+    F, e = V.local_forces(*args, s["pos"], q, q_pseud, vtab, vtab.shape[1], gmin, dg, ref["rhog_re"],
+                          ref["rhog_im"], 1.2)
+    assert np.abs(F - ref["force"]).max() < 1e-12 * np.abs(ref["force"]).max()
+    assert np.all(np.abs(e - ref["ewald"]) <= 1e-13 * np.abs(ref["ewald"]))
+    # E(R) = 2 sum_G Re(vt-weighted vext . rho) + vrecip, rho(G) fixed
+    import math
+    h = np.asarray(s["hmat"], float)
+    vol = abs(np.linalg.det(h))
+    G = V.gvec_cart(s["hmat"], ka[:-1], kb[:-1], kc[:-1])
+    g2 = (G ** 2).sum(axis=1)
+    v = V.spline(vtab, vtab.shape[1], gmin, dg, np.sqrt(g2))
+    kk = np.stack([ka[:-1], kb[:-1], kc[:-1]], axis=1).astype(float)
+    rr, ri = ref["rhog_re"][:-1], ref["rhog_im"][:-1]
+
+    def energy(pos):
+        sfr = pos @ np.linalg.inv(h).T
+        arg = 2.0 * math.pi * (kk @ sfr.T)
+        vt = v[:, None] - 4.0 * math.pi * (q[None, :] - q_pseud) / g2[:, None]
+        ve_r = (np.cos(arg) * vt).sum(axis=1) / vol
+        ve_i = -(np.sin(arg) * vt).sum(axis=1) / vol
+        sr_, si_ = np.cos(arg) @ q, np.sin(arg) @ q
+        preg = np.exp(-g2 / (4.0 * 1.2 ** 2)) * 4.0 * math.pi / (g2 * vol)
+        return 2.0 * np.sum(ve_r * rr + ve_i * ri) + np.sum(preg * (sr_ ** 2 + si_ ** 2))
+    d = 1e-5
+    for a, c in ((0, 0), (3, 1), (5, 2)):
+        p1, p2 = s["pos"].copy(), s["pos"].copy()
+        p1[a, c] += d
+        p2[a, c] -= d
+        num = -(energy(p1) - energy(p2)) / (2 * d)
+        assert abs(num - F[a, c]) < 1e-6 * np.abs(F).max()

@@ -123,7 +123,8 @@ int sdft_ctx_destroy(sdft_ctx *ctx);
 int sdft_ctx_set_kinetic_cap(sdft_ctx *ctx, double gcut);
 /* V_KS(r): nkf1*nkf2*nkf3 doubles in the filter layout, c fastest
  * (the reference's v_ks_up after the transpose at
- * stodft/reduced-energy/cp-energy-ee-rho-stodft.c:984-1007).           */
+ * stodft/reduced-energy/cp-energy-ee-rho-stodft.c:984-1007), in host or
+ * device memory (sdft_vks_from_rho can leave it on the device).         */
 int sdft_ctx_set_vks(sdft_ctx *ctx, const double *v_ks);
 /* KB nonlocal projectors; kb == NULL or kb->natm == 0 disables them.   */
 int sdft_ctx_set_kb(sdft_ctx *ctx, const sdft_kb_desc *kb);

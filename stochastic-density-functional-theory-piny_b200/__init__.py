@@ -378,6 +378,10 @@ class Context:
         assert v.size == self.n[0] * self.n[1] * self.n[2]
         _chk(lib.sdft_ctx_set_vks(self._p, _d(v)))
 
+    def set_vks_dev_ptr(self, ptr):
+        """V_KS from device memory (an address, e.g. a buffer sdft_vks_from_rho filled)."""
+        _chk(lib.sdft_ctx_set_vks(self._p, C.cast(C.c_void_p(int(ptr)), _dp)))
+
     def set_kinetic_cap(self, gcut):
         _chk(lib.sdft_ctx_set_kinetic_cap(self._p, float(gcut)))
 

@@ -773,7 +773,8 @@ extern "C" int sdft_ctx_set_kinetic_cap(sdft_ctx *ctx, double gcut) {
 extern "C" int sdft_ctx_set_vks(sdft_ctx *ctx, const double *v) {
   if (!ctx || !v) return set_error(SDFT_ERR_ARG, "set_vks: null");
   cudaSetDevice(ctx->device);
-  CK(cudaMemcpyAsync(ctx->d_vks_tmp, v, (size_t)ctx->N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  // host or device memory (a V_KS that sdft_vks_from_rho left on the device)
+  CK(cudaMemcpyAsync(ctx->d_vks_tmp, v, (size_t)ctx->N * sizeof(double), cudaMemcpyDefault, ctx->st));
   if (ctx->fast) {
     if (is_fp64(ctx)) fast_vks_perm<double>(ctx->g, ctx->d_vks_tmp, (double *)ctx->d_vp, ctx->st);
     else fast_vks_perm<float>(ctx->g, ctx->d_vks_tmp, (float *)ctx->d_vp, ctx->st);

@@ -88,7 +88,7 @@ def test_scf_step_on_device(pkg, wl):
         v = v_d.cpu().numpy()
         assert rel_l2(v, ov) < 1e-12
         assert np.all(np.abs(e - oe) <= 1e-12 * np.abs(oe))
-        c.set_vks(v)
+        c.set_vks_dev_ptr(v_d.data_ptr())  # V_KS straight from the device buffer
         s2 = dict(s, vks=v)
         cr, ci = O.OracleSys(s).noise(3, seed=4.0)
         fr, fi = c.calc_coef_force(cr, ci)

@@ -267,6 +267,8 @@ def run_ours(args):
     ctx = pkg.Context(*s["grid"], s["ka"], s["kb"], s["kc"], s["hmat"], precision=prec, max_states=nsto, device=local)
     ctx.set_vks(s["vks"])
     ctx.set_kb(s["kb_desc"])
+    if args.plane_threads != "tuned" and prec != pkg.SDFT_PREC_FP64:
+        ctx.set_plane_threads(int(args.plane_threads))
     t0 = time.time()
     emin, emax = ctx.lanczos_bounds(20, seed=15, margin=0.1)[:2]  # 20 device Lanczos steps
     ediff, emean = emax - emin, 0.5 * (emin + emax)
@@ -682,7 +684,7 @@ def run_reference(args):
             v = rc.rate(L, k, scale, emean, ec, seed0=100 * i)
             if i >= args.warmup:
                 vals.append(v)
-                ms.append(1e3 * nsto / v)
+                ms.append(1e3 * (time.perf_counter() - t))  # the sample's own wall time
     finally:
         rc.close()
     v = statistics.median(vals)
@@ -699,6 +701,9 @@ def run_reference(args):
            "cpu_baseline": {"value": v, "unit": "orbitals/s", "cores": rc.cores, "kind": rc.kind,
                             "sample": f"per step {rc.cores} processes x 2 orbitals x {k} Chebyshev steps, "
                                       f"extrapolated linearly to L={L}"},
+           "step": (f"one bounded sample ({rc.cores} x 2 orbitals x {k} steps); ms_per_step is its wall time, "
+                    f"value the rate extrapolated to the full order (the full {nsto}-orbital step would take "
+                    f"{nsto / v:.0f} s)"),
            "e2e": {"value": v, "unit": "orbitals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -728,6 +733,11 @@ def run_batch(args):
         s = wl.build_spec(sp)
         systems.append(s)
         preps.append(serve.prepare(pkg, wl, s, sp["nsto"], sp["L"], prec, seed=10.0 + i, tuner=tuner))
+        if args.plane_threads != "tuned":  # one fixed plane-stage CTA size for every system
+            try:
+                preps[-1]["ctx"].set_plane_threads(int(args.plane_threads))
+            except pkg.SdftError:
+                pass
     setup_s = time.time() - t0
     nsto = [sp["nsto"] for sp in specs]
     total = sum(nsto)
@@ -797,8 +807,11 @@ def run_batch(args):
         "data": "synthetic (seeded Si supercells, Gaussian V_loc, Gaussian s+p KB, +-1 noise)",
         "config": {"workload": f"cfg4: {len(specs)} systems, {sum(s['natm'] for s in systems)} atoms, "
                                f"{total} orbitals, grids 24..72 per axis, orders 128..512",
+                   "plane_threads": args.plane_threads,
                    "systems": [{"atoms": s["natm"], "grid": list(s["grid"]), "orbitals": sp["nsto"], "L": sp["L"],
-                                "gemm_split": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])]["split"]}
+                                "gemm_split": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])]["split"],
+                                "plane_threads": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])].get(
+                                    "plane_threads")}
                                for s, sp, p in zip(systems, specs, preps)],
                    "setup_s": setup_s, "capture_s": capture_s, "l2": "per-system orbitals in HBM; no flush"},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[-1]},
@@ -936,6 +949,9 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="time the eager step only")
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
+    ap.add_argument("--plane-threads", default="tuned", choices=["tuned", "256", "128"],
+                    help="plane-stage CTA size: cfg4 the autotuner's choice per system (tuned) or one size for all; "
+                         "cfg1-3 the library default (tuned) or the given size")
     ap.add_argument("--sat-requests", type=int, default=64,
                     help="cfg5: requests queued at once to measure the saturation rate")
     ap.add_argument("--sustained-requests", type=int, default=200,

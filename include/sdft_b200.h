@@ -371,6 +371,12 @@ int sdft_mixer_destroy(sdft_mixer *m);
  * Split-K of the nonlocal projection GEMM: 0 = built-in cost model,
  * 1..64 = fixed (chosen by the autotuner in tuner.py).                    */
 int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split);
+/* Threads per CTA of the FP32 plane stage (one CTA per plane and orbital
+ * pair): 0 or 256 (the default) or 128, which fits twice the CTAs per SM
+ * and can be faster for small planes.  Mixed-precision contexts on the
+ * fast FFT path only; chosen per system by the autotuner (tuner.py).  No
+ * counterpart in the reference. */
+int sdft_ctx_set_plane_threads(sdft_ctx *ctx, int nt);
 /* CUDA stream priority of the context's stream (lower = more urgent, 0 =
  * default; clamped to the device's range).  Call while the context is idle:
  * the stream is replaced.  A server gives cheap requests the urgent

@@ -136,6 +136,7 @@ _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
+_sig("sdft_ctx_set_plane_threads", C.c_int, [_vp, C.c_int])
 _sig("sdft_xc_lda_dev", C.c_int, [C.c_int, C.c_longlong, _vp, _vp, C.c_double, _dp, _dp, _vp])
 _sig("sdft_mixer_create", C.c_int, [C.c_int, C.c_longlong, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.POINTER(_vp)])
@@ -540,6 +541,10 @@ class Context:
         """Split-K of the nonlocal projection GEMM (0 = cost model)."""
         _chk(lib.sdft_ctx_set_gemm_split(self._p, int(split)))
 
+    def set_plane_threads(self, nt):
+        """Threads per CTA of the FP32 plane stage: 0 (default 256), 128 or 256."""
+        _chk(lib.sdft_ctx_set_plane_threads(self._p, int(nt)))
+
     def set_priority(self, priority):
         """CUDA priority of the context's stream (lower = more urgent); idle only."""
         _chk(lib.sdft_ctx_set_priority(self._p, int(priority)))
@@ -755,6 +760,10 @@ class Batch:
 
     def sync(self):
         _chk(lib.sdft_batch_sync(self._p))
+
+    def set_plane_threads(self, nt):
+        """Threads per CTA of the FP32 plane stage: 0 (default 256), 128 or 256."""
+        _chk(lib.sdft_ctx_set_plane_threads(self._p, int(nt)))
 
     def set_priority(self, priority):
         """CUDA priority of the stream the graph is launched into; idle only."""

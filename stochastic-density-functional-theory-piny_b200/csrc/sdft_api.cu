@@ -1414,6 +1414,15 @@ out:
 #undef CKG
 }
 
+extern "C" int sdft_ctx_set_plane_threads(sdft_ctx *ctx, int nt) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (nt != 0 && nt != 128 && nt != 256) return set_error(SDFT_ERR_ARG, "plane_threads: 0 (default), 128 or 256");
+  if (nt == 128 && (is_fp64(ctx) || !ctx->fast))
+    return set_error(SDFT_ERR_UNSUPPORTED, "plane_threads: 128 exists for the FP32 fast plane stage only");
+  ctx->g.plane_nt = nt == 256 ? 0 : nt;
+  return SDFT_OK;
+}
+
 extern "C" int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split) {
   if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
   if (split < 0 || split > 64) return set_error(SDFT_ERR_ARG, "gemm_split: 0 (cost model) or 1..64");

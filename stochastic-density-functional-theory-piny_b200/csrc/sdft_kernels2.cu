@@ -12,6 +12,7 @@
 // So no data movement is ever spent on undoing an FFT permutation.
 #include <cuda_runtime.h>
 #include <cmath>
+#include <type_traits>
 #include "sdft_fft2.cuh"
 #include "sdft_internal.h"
 #include "sdft_kernels.cuh"
@@ -546,11 +547,13 @@ template <int N2> struct RowKb {
   }
 };
 
-template <typename T, int N1, int N2>
-__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
+// NT threads per plane CTA: PlaneCfg's default, or (FP32) the 128-thread
+// instance that the autotuner may pick for small planes (more resident CTAs)
+template <typename T, int N1, int N2, int NT = PlaneCfg<T>::NT, int MINB = PlaneCfg<T>::MINB>
+__global__ void __launch_bounds__(NT, MINB)
 kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict__ Vp) {
   using C2 = typename CT<T>::type;
-  constexpr int NT = PlaneCfg<T>::NT, P2 = N2 + 1;
+  constexpr int P2 = N2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // (the first N1 + N2 complex slots held twiddles before they moved to
   // constant memory; the row kb ranges use the first N1 of them)
@@ -772,14 +775,25 @@ template <typename T>
 bool fast_stage_b(const DevGeom &g, void *X, const T *Vp, int npairs, cudaStream_t st) {
   dim3 grid(g.n3, npairs);
   const size_t sm = pl_smem<T>(g.n1, g.n2);
+  const bool small = std::is_same<T, float>::value && g.plane_nt == 128;
+#define LBK(k, NTH)                                                                            \
+  do {                                                                                         \
+    static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true); (void)attr_once;             \
+    k<<<grid, NTH, sm, st>>>(g, (typename CT<T>::type *)X, Vp);                                \
+  } while (0)
 #define LB(A, B)                                                                               \
   do {                                                                                         \
-    auto k = kf_stage_b<T, A, B>;                                                              \
-    static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true); (void)attr_once;             \
-    k<<<grid, PlaneCfg<T>::NT, sm, st>>>(g, (typename CT<T>::type *)X, Vp);                    \
+    if (small) {                                                                               \
+      auto k = kf_stage_b<T, A, B, 128, 6>;                                                    \
+      LBK(k, 128);                                                                             \
+    } else {                                                                                   \
+      auto k = kf_stage_b<T, A, B>;                                                            \
+      LBK(k, PlaneCfg<T>::NT);                                                                 \
+    }                                                                                          \
   } while (0)
   SDFT_FOR_PLANE(LB);
 #undef LB
+#undef LBK
   return true;
 }
 

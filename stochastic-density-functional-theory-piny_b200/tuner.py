@@ -1,10 +1,15 @@
 """Autotuner for the per-system launch shapes of the filter.
 
-The tunable shape is the split-K factor of the nonlocal projection GEMM
-(Z = Pj C: M = projectors, N = orbitals, K = 2 ncoef): few-orbital, small
-systems have only a handful of output tiles, so the K range per CTA decides
-how many of the 148 SMs work.  The built-in wave-quantisation cost model
-(choice 0) is one candidate; fixed splits are the others.  Each candidate is
+Two shapes are tuned per problem shape:
+* the split-K factor of the nonlocal projection GEMM (Z = Pj C: M =
+  projectors, N = orbitals, K = 2 ncoef): few-orbital, small systems have
+  only a handful of output tiles, so the K range per CTA decides how many of
+  the 148 SMs work.  The built-in wave-quantisation cost model (choice 0) is
+  one candidate; fixed splits are the others;
+* the CTA size of the FP32 plane FFT stage (one CTA per plane and orbital
+  pair): 256 threads, or 128, which fits twice the CTAs per SM and can be
+  faster on small planes (mixed contexts on the fast FFT path).
+Each candidate is
 timed on a short Chebyshev filter of the context's resident orbitals (the
 filter kernels themselves, device time by CUDA events on the context
 stream, through the library's own event calls), and the fastest is set on
@@ -23,6 +28,7 @@ import os
 import numpy as np
 
 CANDIDATES = (0, 1, 2, 4, 8, 16, 32)
+PLANE_THREADS = (256, 128)
 
 
 class Tuner:
@@ -58,15 +64,30 @@ class Tuner:
             b.close()
 
     def tune(self, ctx, nstate, nproj, scale=0.1, emean=0.0):
-        """Pick and set the projection split-K for (ctx, nstate); returns it."""
+        """Pick and set the projection split-K and the plane-stage CTA size
+        for (ctx, nstate); returns the split."""
         k = self.key(ctx, nstate, nproj)
         if k not in self.cache:
             times = {str(c): self._time(ctx, nstate, c, scale, emean) for c in self.candidates}
-            best = min(times, key=times.get)
-            self.cache[k] = {"split": int(best), "ms": times}
+            best = int(min(times, key=times.get))
+            entry = {"split": best, "ms": times}
+            plane = {}
+            for nt in PLANE_THREADS:
+                try:
+                    ctx.set_plane_threads(nt)
+                except self.pkg.SdftError:  # FP64 or the generic FFT path: one plane shape only
+                    continue
+                plane[str(nt)] = self._time(ctx, nstate, best, scale, emean)
+            if plane:
+                entry["plane_threads"] = int(min(plane, key=plane.get))
+                entry["plane_ms"] = plane
+            self.cache[k] = entry
             if self.path:
                 with open(self.path, "w") as f:
                     json.dump(self.cache, f, indent=1, sort_keys=True)
-        split = int(self.cache[k]["split"])
+        entry = self.cache[k]
+        split = int(entry["split"])
         ctx.set_gemm_split(split)
+        if "plane_threads" in entry:
+            ctx.set_plane_threads(int(entry["plane_threads"]))
         return split

@@ -811,7 +811,8 @@ def run_batch(args):
                    "systems": [{"atoms": s["natm"], "grid": list(s["grid"]), "orbitals": sp["nsto"], "L": sp["L"],
                                 "gemm_split": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])]["split"],
                                 "plane_threads": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])].get(
-                                    "plane_threads")}
+                                    "plane_threads"),
+                                "gemm_bn": tuner.cache[tuner.key(p["ctx"], sp["nsto"], 4 * s["natm"])].get("gemm_bn")}
                                for s, sp, p in zip(systems, specs, preps)],
                    "setup_s": setup_s, "capture_s": capture_s, "l2": "per-system orbitals in HBM; no flush"},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[-1]},

@@ -371,6 +371,12 @@ int sdft_mixer_destroy(sdft_mixer *m);
  * Split-K of the nonlocal projection GEMM: 0 = built-in cost model,
  * 1..64 = fixed (chosen by the autotuner in tuner.py).                    */
 int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split);
+/* Orbital columns per output tile of the mixed-precision KB GEMMs: 0 = per
+ * call (64 where it pads the orbital count less than 128, e.g. 16..64 or
+ * 129..192 orbitals), 64 or 128 = fixed (chosen by the autotuner in
+ * tuner.py).  Results are bitwise equal for every width: each output is the
+ * same exact integer sum per K range.  No counterpart in the reference. */
+int sdft_ctx_set_gemm_bn(sdft_ctx *ctx, int bn);
 /* Threads per CTA of the FP32 plane stage (one CTA per plane and orbital
  * pair): 0 or 256 (the default) or 128, which fits twice the CTAs per SM
  * and can be faster for small planes.  Mixed-precision contexts on the

@@ -135,6 +135,7 @@ _sig("sdft_launch_count", C.c_longlong, [_vp])
 _sig("sdft_ctx_set_timing", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_read_timing", C.c_int, [_vp, _dp, C.POINTER(C.c_longlong)])
 _sig("sdft_ctx_set_gemm_split", C.c_int, [_vp, C.c_int])
+_sig("sdft_ctx_set_gemm_bn", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_priority", C.c_int, [_vp, C.c_int])
 _sig("sdft_ctx_set_plane_threads", C.c_int, [_vp, C.c_int])
 _sig("sdft_xc_lda_dev", C.c_int, [C.c_int, C.c_longlong, _vp, _vp, C.c_double, _dp, _dp, _vp])
@@ -540,6 +541,11 @@ class Context:
     def set_gemm_split(self, split):
         """Split-K of the nonlocal projection GEMM (0 = cost model)."""
         _chk(lib.sdft_ctx_set_gemm_split(self._p, int(split)))
+
+    def set_gemm_bn(self, bn):
+        """Orbital columns per tile of the mixed-precision KB GEMMs: 0 (per
+        call, 64 where it pads the orbital count less), 64 or 128."""
+        _chk(lib.sdft_ctx_set_gemm_bn(self._p, int(bn)))
 
     def set_plane_threads(self, nt):
         """Threads per CTA of the FP32 plane stage: 0 (default 256), 128 or 256."""

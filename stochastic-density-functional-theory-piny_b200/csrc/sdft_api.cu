@@ -289,7 +289,9 @@ static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl, bool back = true,
                      const double *gk = nullptr, const unsigned long long *gk_max = nullptr) {
   const int K1 = 2 * ctx->ngp, S = ctx->s_oz, Ppad = ctx->Ppad;
-  const int N = (nstate + 127) / 128 * 128;
+  // tile width of both GEMMs: the set one, else 64 where it pads the orbitals less
+  const int bn = ctx->gemm_bn ? ctx->gemm_bn : ((nstate + 63) / 64 * 64 < (nstate + 127) / 128 * 128 ? 64 : 128);
+  const int N = (nstate + bn - 1) / bn * bn;
   {
     TScope ts(ctx, 7);
     if (gk) {
@@ -310,18 +312,26 @@ static int run_kb_oz(sdft_ctx *ctx, const double *vec, int nstate, bool want_enl
   OzGemm g1 = ctx->om1, g2 = ctx->om2;
   g1.N = N; g1.Nst = nstate;
   g2.N = N; g2.Nst = nstate;
+  g1.bn = g2.bn = bn;
+  if (bn == 64) {
+    g1.tB = ctx->om1_tb64;
+    g2.tB = ctx->om2_tb64;
+  }
   const size_t stride = (size_t)N * Ppad;
   const int max_split = (int)std::min<size_t>(32, ctx->oz_part_elems / stride);
-  const int split = ctx->gemm_split > 0 ? std::min(ctx->gemm_split, std::max(1, max_split))
-                                        : oz_choose_split((Ppad / 128) * (N / 128), ctx->kp_oz / 64, max_split);
+  const int min_split = oz_min_split(ctx->kp_oz, OZ_7x4);
+  if (min_split > max_split) return set_error(SDFT_ERR_NOMEM, "oz gemm: partial buffer too small for K");
+  const int split = ctx->gemm_split > 0 ? std::max(min_split, std::min(ctx->gemm_split, std::max(1, max_split)))
+                                        : oz_choose_split((Ppad / 128) * (N / bn), ctx->kp_oz / 64, max_split);
   int r;
   {
     TScope ts(ctx, 3);
-    r = run_gemm_oz(g1, split, ctx->d_oz_part, stride, ctx->d_err, ctx->st);
+    int used = split;  // the partials the launch writes (K tiles dealt out evenly)
+    r = run_gemm_oz(g1, split, ctx->d_oz_part, stride, ctx->d_err, ctx->st, &used);
     if (r) return r;
     // also zeroes d_rowmax[0, nstate) for the next stage C (the slice above
     // has consumed it)
-    launch_oz_reduce_slice(ctx->d_oz_part, split, stride, Ppad, ctx->P, nstate, ctx->d_z, ctx->d_z_dig,
+    launch_oz_reduce_slice(ctx->d_oz_part, used, stride, Ppad, ctx->P, nstate, ctx->d_z, ctx->d_z_dig,
                            (size_t)S * Ppad, ctx->d_z_sc, ctx->d_rowmax, ctx->st, ctx->om2.fmt);
     ctx->launches += 2;
     ctx->rowmax_zero_n = nstate;
@@ -1420,6 +1430,13 @@ extern "C" int sdft_ctx_set_plane_threads(sdft_ctx *ctx, int nt) {
   if (nt == 128 && (is_fp64(ctx) || !ctx->fast))
     return set_error(SDFT_ERR_UNSUPPORTED, "plane_threads: 128 exists for the FP32 fast plane stage only");
   ctx->g.plane_nt = nt == 256 ? 0 : nt;
+  return SDFT_OK;
+}
+
+extern "C" int sdft_ctx_set_gemm_bn(sdft_ctx *ctx, int bn) {
+  if (!ctx) return set_error(SDFT_ERR_ARG, "null context");
+  if (bn != 0 && bn != 64 && bn != 128) return set_error(SDFT_ERR_ARG, "gemm_bn: 0 (per call), 64 or 128");
+  ctx->gemm_bn = bn;
   return SDFT_OK;
 }
 

@@ -81,10 +81,12 @@ struct sdft_ctx {
   double *d_oz_part = nullptr;
   size_t oz_part_elems = 0;
   sdft::OzGemm om1{}, om2{};
+  CUtensorMap om1_tb64{}, om2_tb64{};  // the B operands' maps with 64-row boxes (64-wide tiles)
   // Inside a filter / moments loop, stage C records the per-orbital max of
   // the vector it writes (d_rowmax), so the next projection can form that
   // vector's digits without another pass over it.
   int gemm_split = 0;                // projection split-K override (0: cost model)
+  int gemm_bn = 0;                   // KB GEMM tile width: 0 = per call (64 where it pads less), 64 or 128
   bool track_omax = false;
   const double *omax_vec = nullptr;  // vector whose row maxima d_rowmax holds
   int omax_n = 0;

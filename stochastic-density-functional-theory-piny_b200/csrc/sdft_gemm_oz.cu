@@ -2,12 +2,13 @@
 // (Ozaki scheme: split each operand into int8 digits under a per-row
 // power-of-two scale, multiply digit slices exactly, recombine exactly).
 //
-// CTA = 10 warps over one 128 x 128 output tile and one K range:
+// CTA = 10 warps over one 128 x BN output tile (BN = 128, or 64 for orbital
+// counts that a 128-wide tile would pad more) and one K range:
 //   warp 0    TMA producer: per 64-wide K tile one 3-D box per operand
 //             carrying all four digit slices (64 B rows, 64B swizzle),
 //             three-stage ring of 64 KB stages;
-//   warp 1    TMEM owner (512 columns = four int32 accumulators of 128
-//             columns, one per digit order q = s + t) and single-thread
+//   warp 1    TMEM owner (four int32 accumulators of BN columns, one per
+//             digit order q = s + t: 512 columns, or 256 at BN = 64) and single-thread
 //             issuer of tcgen05.mma.kind::i8 (10 slice pairs x 2 K steps
 //             of 32 per stage);
 //   warps 2-9 epilogue (two per TMEM lane quadrant, one column half each):
@@ -31,7 +32,7 @@
 
 namespace sdft {
 
-constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 64;
+constexpr int OZ_BM = 128, OZ_BK = 64;
 // split-1 GEMMs (the back projection) run as the persistent kernel: the
 // next tile's loads overlap the epilogue (measured 4 % faster than one CTA
 // per tile at 28-bit digits, 7 % at 24-bit)
@@ -47,16 +48,20 @@ template <> struct OzF<OZ_8x3> {
   static constexpr int NS = 3, BITS = 8, STAGES = 4, MAX_KRANGE = 16384, SCALE_EXP = -30;
 };
 
-template <int FMT> struct OzSmem {
-  static constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES;
+// BN: output columns (orbitals) per tile, 128 or 64.  The 64-wide tile
+// pads small orbital counts less; its stages are smaller, so it keeps one
+// more of them.
+template <int FMT, int BN = 128> struct OzSmem {
+  static constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES + (BN == 64 ? 1 : 0);
   static constexpr int A_SLICE = OZ_BM * OZ_BK;          // 8 KB
-  static constexpr int B_SLICE = OZ_BN * OZ_BK;          // 8 KB
+  static constexpr int B_SLICE = BN * OZ_BK;             // 8 KB (BN = 128) or 4 KB
   static constexpr int A_BYTES = NS * A_SLICE;
   static constexpr int B_BYTES = NS * B_SLICE;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 64 KB (7x4) or 48 KB (8x3)
   static constexpr int BAR_OFF = OZ_STAGES * STAGE_BYTES;
   static constexpr int TOTAL = BAR_OFF + 8 * (2 * OZ_STAGES + 2) + 16 + 1024;  // + alignment slack
-  static constexpr int TMEM_COLS = 512;                                         // NS accumulators of OZ_BN
+  // NS accumulators of BN columns, rounded up to a power of two
+  static constexpr int TMEM_COLS = NS * BN <= 256 ? 256 : 512;
 };
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
@@ -69,13 +74,13 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, 
 constexpr int OZ_EPI_WARPS = 8;                 // two per TMEM lane quadrant
 constexpr int OZ_THREADS = 32 * (2 + OZ_EPI_WARPS);
 
-template <typename OutT, int FMT>
+template <typename OutT, int FMT, int BN>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int ktiles_total,
            int ktiles_per_split, const double *__restrict__ sa, const double *__restrict__ sb,
            OutT *__restrict__ out, size_t split_stride, int ldo, int Mst, int Nst, int *err) {
-  using S = OzSmem<FMT>;
-  constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES, BITS = OzF<FMT>::BITS;
+  using S = OzSmem<FMT, BN>;
+  constexpr int NS = OzF<FMT>::NS, OZ_STAGES = S::OZ_STAGES, BITS = OzF<FMT>::BITS;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_u32(smem);
@@ -84,7 +89,7 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
   const uint32_t bar_tmem = bar_empty + 8 * OZ_STAGES;
   uint32_t *tmem_slot = (uint32_t *)(smem + S::BAR_OFF + 8 * (2 * OZ_STAGES + 1));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n0 = blockIdx.x * OZ_BN, m0 = blockIdx.y * OZ_BM;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * OZ_BM;
   const int kt0 = blockIdx.z * ktiles_per_split;
   const int nkt = max(0, min(ktiles_total, kt0 + ktiles_per_split) - kt0);
 
@@ -124,7 +129,7 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
     if (lane == 0) {  // MMA issuer
       // D = S32, A / B = signed (1) or unsigned (0) 8-bit, K-major, N = 128, M = 128;
       // OZ_8x3: digit 0 signed, digits 1 and 2 unsigned
-      constexpr uint32_t idesc0 = (2u << 4) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+      constexpr uint32_t idesc0 = (2u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
       uint32_t started = 0;  // bit q: accumulator q holds data
       for (int it = 0; it < nkt; it++) {
         const int s = it % OZ_STAGES;
@@ -142,7 +147,7 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
               const uint32_t idesc = idesc0 | (as ? 1u << 7 : 0u) | (bs ? 1u << 10 : 0u);
               const uint64_t ad = smem_desc<64>(st + sa_ * S::A_SLICE + ks * 32);
               const uint64_t bd = smem_desc<64>(st + S::A_BYTES + tb * S::B_SLICE + ks * 32);
-              mma_i8(tmem + (uint32_t)(q * OZ_BN), ad, bd, idesc, (started >> q) & 1u);
+              mma_i8(tmem + (uint32_t)(q * BN), ad, bd, idesc, (started >> q) & 1u);
               started |= 1u << q;
             }
           }
@@ -160,14 +165,14 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
     const bool row_ok = ok && m < Mst && nkt > 0;
     const double fa = row_ok ? ldexp(sa[m], OzF<FMT>::SCALE_EXP) : 0.0;
     const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
-    constexpr int CH = OZ_BN / 16 / 2;  // 16-column chunks per epilogue warp
+    constexpr int CH = BN / 16 / 2;  // 16-column chunks per epilogue warp
 #pragma unroll 1
     for (int c = half * CH; c < (half + 1) * CH; c++) {
       uint32_t r0[16], r1[16], r2[16], r3[16];
-      tmem_ld16(tl + 0 * OZ_BN + c * 16, r0);
-      tmem_ld16(tl + 1 * OZ_BN + c * 16, r1);
-      tmem_ld16(tl + 2 * OZ_BN + c * 16, r2);
-      if constexpr (NS == 4) tmem_ld16(tl + 3 * OZ_BN + c * 16, r3);
+      tmem_ld16(tl + 0 * BN + c * 16, r0);
+      tmem_ld16(tl + 1 * BN + c * 16, r1);
+      tmem_ld16(tl + 2 * BN + c * 16, r2);
+      if constexpr (NS == 4) tmem_ld16(tl + 3 * BN + c * 16, r3);
       tmem_ld_wait();
       if (!(ok && m < Mst)) continue;
 #pragma unroll
@@ -204,13 +209,13 @@ k_gemm_oz8(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUten
 // MMAs wait between tiles.
 constexpr int OZP_EPI_WARPS = 16;
 constexpr int OZP_THREADS = 32 * (2 + OZP_EPI_WARPS);
-template <typename OutT, int FMT>
+template <typename OutT, int FMT, int BN>
 __global__ void __launch_bounds__(OZP_THREADS, 1)
 k_gemm_oz8p(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, int nkt, int ntn,
             int ntiles, const double *__restrict__ sa, const double *__restrict__ sb, OutT *__restrict__ out,
             int ldo, int Mst, int Nst, int *err) {
-  using S = OzSmem<FMT>;
-  constexpr int NS = OzF<FMT>::NS, OZ_STAGES = OzF<FMT>::STAGES, BITS = OzF<FMT>::BITS;
+  using S = OzSmem<FMT, BN>;
+  constexpr int NS = OzF<FMT>::NS, OZ_STAGES = S::OZ_STAGES, BITS = OzF<FMT>::BITS;
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_u32(smem);
@@ -245,7 +250,7 @@ k_gemm_oz8p(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUte
     if (lane == 0) {  // TMA producer, continuous over the CTA's tiles
       bool go = true;
       for (int tile = blockIdx.x, ti = 0; go && tile < ntiles; tile += gridDim.x, ti++) {
-        const int n0 = (tile % ntn) * OZ_BN, m0 = (tile / ntn) * OZ_BM;
+        const int n0 = (tile % ntn) * BN, m0 = (tile / ntn) * OZ_BM;
         for (int it = 0; it < nkt; it++) {
           const int g = ti * nkt + it, s = g % OZ_STAGES;
           if (!mbar_wait(bar_empty + 8 * s, ((g / OZ_STAGES) & 1) ^ 1, err)) { go = false; break; }
@@ -258,7 +263,7 @@ k_gemm_oz8p(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUte
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      constexpr uint32_t idesc0 = (2u << 4) | ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+      constexpr uint32_t idesc0 = (2u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
       bool go = true;
       for (int tile = blockIdx.x, ti = 0; go && tile < ntiles; tile += gridDim.x, ti++) {
         if (ti > 0) {  // accumulators of the previous tile read out
@@ -282,7 +287,7 @@ k_gemm_oz8p(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUte
                 const uint32_t idesc = idesc0 | (as ? 1u << 7 : 0u) | (bs ? 1u << 10 : 0u);
                 const uint64_t ad = smem_desc<64>(st + sa_ * S::A_SLICE + ks * 32);
                 const uint64_t bd = smem_desc<64>(st + S::A_BYTES + tb * S::B_SLICE + ks * 32);
-                mma_i8(tmem + (uint32_t)(q * OZ_BN), ad, bd, idesc, (started >> q) & 1u);
+                mma_i8(tmem + (uint32_t)(q * BN), ad, bd, idesc, (started >> q) & 1u);
                 started |= 1u << q;
               }
             }
@@ -296,21 +301,21 @@ k_gemm_oz8p(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUte
     const int qd = warp & 3;
     const int part = (warp - 2) >> 2;
     for (int tile = blockIdx.x, ti = 0; tile < ntiles; tile += gridDim.x, ti++) {
-      const int n0 = (tile % ntn) * OZ_BN, m0 = (tile / ntn) * OZ_BM;
+      const int n0 = (tile % ntn) * BN, m0 = (tile / ntn) * OZ_BM;
       const bool ok = mbar_wait(bar_tfull, ti & 1, err);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int m = m0 + 32 * qd + lane;
       const bool row_ok = ok && m < Mst;
       const double fa = row_ok ? ldexp(sa[m], OzF<FMT>::SCALE_EXP) : 0.0;
       const uint32_t tl = tmem + ((uint32_t)(32 * qd) << 16);
-      constexpr int CH = OZ_BN / 16 / (OZP_EPI_WARPS / 4);
+      constexpr int CH = BN / 16 / (OZP_EPI_WARPS / 4);
 #pragma unroll 1
       for (int c = part * CH; c < (part + 1) * CH; c++) {
         uint32_t r0[16], r1[16], r2[16], r3[16];
-        tmem_ld16(tl + 0 * OZ_BN + c * 16, r0);
-        tmem_ld16(tl + 1 * OZ_BN + c * 16, r1);
-        tmem_ld16(tl + 2 * OZ_BN + c * 16, r2);
-        if constexpr (NS == 4) tmem_ld16(tl + 3 * OZ_BN + c * 16, r3);
+        tmem_ld16(tl + 0 * BN + c * 16, r0);
+        tmem_ld16(tl + 1 * BN + c * 16, r1);
+        tmem_ld16(tl + 2 * BN + c * 16, r2);
+        if constexpr (NS == 4) tmem_ld16(tl + 3 * BN + c * 16, r3);
         tmem_ld_wait();
         if (c == (part + 1) * CH - 1) {
           // this warp's last accumulator read is complete: release the
@@ -510,20 +515,27 @@ static PFN_encodeTiledOz get_encode_oz() {
 
 bool gemm_oz_available() { return get_encode_oz() != nullptr; }
 
-int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt) {
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt, int box_rows) {
   PFN_encodeTiledOz enc = get_encode_oz();
   if (!enc) return set_error(SDFT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  if (box_rows != 64 && box_rows != 128) return set_error(SDFT_ERR_ARG, "oz tensor map box");
   if (((uintptr_t)dig & 15) || ld % OZ_BK || rows % 128) return set_error(SDFT_ERR_ARG, "oz tensor map alignment");
   const int ns = oz_slices(fmt);
   cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)ns};
   cuuint64_t strides[2] = {(cuuint64_t)ld, (cuuint64_t)ld * rows};
-  cuuint32_t box[3] = {(cuuint32_t)OZ_BK, 128u, (cuuint32_t)ns};
+  cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, (cuuint32_t)ns};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void *)dig, dims, strides, box, es,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(SDFT_ERR_CUDA, "cuTensorMapEncodeTiled failed (oz)");
   return SDFT_OK;
+}
+
+int oz_min_split(int K, int fmt) {
+  const int ktiles = (K + OZ_BK - 1) / OZ_BK;
+  const int kmax = (fmt == OZ_8x3 ? OzF<OZ_8x3>::MAX_KRANGE : OzF<OZ_7x4>::MAX_KRANGE) / OZ_BK;
+  return (ktiles + kmax - 1) / kmax;
 }
 
 int oz_choose_split(int tiles, int ktiles, int max_split) {
@@ -545,11 +557,12 @@ int oz_choose_split(int tiles, int ktiles, int max_split) {
   return best;
 }
 
-template <typename OutT, int FMT>
-static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_stride, int *err, cudaStream_t st) {
-  using S = OzSmem<FMT>;
+template <typename OutT, int FMT, int BN>
+static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_stride, int *err, cudaStream_t st,
+                         int *split_used) {
+  using S = OzSmem<FMT, BN>;
   const int ktiles = (g.K + OZ_BK - 1) / OZ_BK;
-  if (g.M % OZ_BM || g.N % OZ_BN || ktiles < 1) return set_error(SDFT_ERR_ARG, "oz gemm: shape");
+  if (g.M % OZ_BM || g.N % BN || ktiles < 1) return set_error(SDFT_ERR_ARG, "oz gemm: shape");
   if (split < 1) split = 1;
   if (split > ktiles) split = ktiles;
   int kps = (ktiles + split - 1) / split;
@@ -558,32 +571,43 @@ static int run_gemm_oz_t(const OzGemm &g, int split, OutT *out, size_t split_str
     kps = OzF<FMT>::MAX_KRANGE / OZ_BK;
   }
   split = (ktiles + kps - 1) / kps;
+  if (split_used) *split_used = split;  // the partials written: what a reduction must sum
   if (split == 1 && kOzPersistent) {
-    static const bool attr_p = (cudaFuncSetAttribute(k_gemm_oz8p<OutT, FMT>,
+    static const bool attr_p = (cudaFuncSetAttribute(k_gemm_oz8p<OutT, FMT, BN>,
                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL), true);
     (void)attr_p;
-    const int ntn = g.N / OZ_BN, ntiles = ntn * (g.M / OZ_BM);
+    const int ntn = g.N / BN, ntiles = ntn * (g.M / OZ_BM);
     const int grid = ntiles < 148 ? ntiles : 148;
-    k_gemm_oz8p<OutT, FMT><<<grid, OZP_THREADS, S::TOTAL, st>>>(g.tA, g.tB, ktiles, ntn, ntiles, g.sa, g.sb, out, g.ldo,
+    k_gemm_oz8p<OutT, FMT, BN><<<grid, OZP_THREADS, S::TOTAL, st>>>(g.tA, g.tB, ktiles, ntn, ntiles, g.sa, g.sb, out, g.ldo,
                                                                g.Mst, g.Nst, err);
     return SDFT_OK;
   }
   static const bool attr_once =
-      (cudaFuncSetAttribute(k_gemm_oz8<OutT, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL), true);
+      (cudaFuncSetAttribute(k_gemm_oz8<OutT, FMT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL), true);
   (void)attr_once;
-  dim3 grid(g.N / OZ_BN, g.M / OZ_BM, split);
-  k_gemm_oz8<OutT, FMT><<<grid, OZ_THREADS, S::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride,
+  dim3 grid(g.N / BN, g.M / OZ_BM, split);
+  k_gemm_oz8<OutT, FMT, BN><<<grid, OZ_THREADS, S::TOTAL, st>>>(g.tA, g.tB, ktiles, kps, g.sa, g.sb, out, split_stride,
                                                             g.ldo, g.Mst, g.Nst, err);
   return SDFT_OK;
 }
 
-int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st) {
-  return g.fmt == OZ_8x3 ? run_gemm_oz_t<double, OZ_8x3>(g, split, out, split_stride, err, st)
-                         : run_gemm_oz_t<double, OZ_7x4>(g, split, out, split_stride, err, st);
+template <typename OutT>
+static int run_gemm_oz_any(const OzGemm &g, int split, OutT *out, size_t split_stride, int *err, cudaStream_t st,
+                           int *su) {
+  if (g.bn != 64 && g.bn != 128) return set_error(SDFT_ERR_ARG, "oz gemm: tile width");
+  if (g.fmt == OZ_8x3)
+    return g.bn == 64 ? run_gemm_oz_t<OutT, OZ_8x3, 64>(g, split, out, split_stride, err, st, su)
+                      : run_gemm_oz_t<OutT, OZ_8x3, 128>(g, split, out, split_stride, err, st, su);
+  return g.bn == 64 ? run_gemm_oz_t<OutT, OZ_7x4, 64>(g, split, out, split_stride, err, st, su)
+                    : run_gemm_oz_t<OutT, OZ_7x4, 128>(g, split, out, split_stride, err, st, su);
 }
-int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st) {
-  return g.fmt == OZ_8x3 ? run_gemm_oz_t<float, OZ_8x3>(g, split, out, split_stride, err, st)
-                         : run_gemm_oz_t<float, OZ_7x4>(g, split, out, split_stride, err, st);
+int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st,
+                int *split_used) {
+  return run_gemm_oz_any(g, split, out, split_stride, err, st, split_used);
+}
+int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st,
+                int *split_used) {
+  return run_gemm_oz_any(g, split, out, split_stride, err, st, split_used);
 }
 
 template <typename SRC>

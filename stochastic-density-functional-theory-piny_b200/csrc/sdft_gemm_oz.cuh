@@ -35,23 +35,33 @@ __host__ __device__ constexpr int oz_slices(int fmt) { return fmt == OZ_8x3 ? 3 
 // accumulators and combined exactly in 64-bit integers, so a K range
 // contributes an exactly representable FP64 value and the only rounding is
 // the FP64 sum of split-K partials.  A: M x K (M multiple of 128), B: N x K
-// (N multiple of 128); only m < Mst, n < Nst are stored.
+// (N multiple of bn); only m < Mst, n < Nst are stored.
 struct OzGemm {
   CUtensorMap tA, tB;
   int M, N, K, ldo, Mst, Nst;
   const double *sa, *sb;  // row scales 2^E of A (M) and B (N)
   int fmt = OZ_7x4;       // digit format of both operands
+  int bn = 128;           // output columns per tile (128 or 64; tB's box height, N a multiple of it)
 };
 
 bool gemm_oz_available();
 // tensor map of a digit array [oz_slices(fmt)][rows][ld] (int8, K-major)
-int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt = OZ_7x4);
+// box_rows: the rows of one TMA box (128 for A operands, the tile width bn for B)
+int make_tmap_oz(CUtensorMap *tm, const int8_t *dig, int rows, int ld, int fmt = OZ_7x4, int box_rows = 128);
 // split == 1: out = result; split > 1: FP64 partial z at out + z*split_stride.
-int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st);
+// The K tiles are dealt out evenly, which can leave fewer partials than
+// asked for (e.g. 32 over 206 K tiles: 7 each, 30 partials); *split_used
+// (nullable) receives the count written, the one a reduction must sum.
+int run_gemm_oz(const OzGemm &g, int split, double *out, size_t split_stride, int *err, cudaStream_t st,
+                int *split_used = nullptr);
 // the same with FP32 output (rounded once from the exact FP64 tile value)
-int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st);
+int run_gemm_oz(const OzGemm &g, int split, float *out, size_t split_stride, int *err, cudaStream_t st,
+                int *split_used = nullptr);
 // split count for `tiles` output tiles over `ktiles` K tiles (<= max_split)
 int oz_choose_split(int tiles, int ktiles, int max_split);
+// the fewest K splits that keep every K range within the format's exact
+// int32 accumulation limit
+int oz_min_split(int K, int fmt);
 // Bounded-wait self-test: one thread waits on an mbarrier that nothing
 // arrives at, through the GEMMs' mbar_wait capped at `polls` polls; it gives
 // up and sets *err (the GEMMs' device error word).  polls <= kSelftestMaxPolls.

@@ -351,7 +351,9 @@ static int kb_build(sdft_ctx *ctx, const sdft_kb_desc *kb) {
     OzGemm &g1 = ctx->om1, &g2 = ctx->om2;
     if ((r = make_tmap_oz(&g1.tA, ctx->d_pj_dig, Ppad, Kp)) || (r = make_tmap_oz(&g1.tB, ctx->d_c_dig, S, Kp)) ||
         (r = make_tmap_oz(&g2.tA, ctx->d_bk_dig, Mpad2, Ppad, f2)) ||
-        (r = make_tmap_oz(&g2.tB, ctx->d_z_dig, S, Ppad, f2))) {
+        (r = make_tmap_oz(&g2.tB, ctx->d_z_dig, S, Ppad, f2)) ||
+        (r = make_tmap_oz(&ctx->om1_tb64, ctx->d_c_dig, S, Kp, OZ_7x4, 64)) ||
+        (r = make_tmap_oz(&ctx->om2_tb64, ctx->d_z_dig, S, Ppad, f2, 64))) {
       rc = r;
       goto done;
     }

@@ -1,6 +1,10 @@
 """Autotuner for the per-system launch shapes of the filter.
 
-Two shapes are tuned per problem shape:
+Three shapes are tuned per problem shape:
+* the orbital columns per tile of the mixed-precision KB GEMMs, 128 or 64:
+  the orbital count is padded to the tile width, so 64 wastes less on small
+  or just-over-128 counts, while 128 reads each projector tile fewer times
+  (timed first, at the cost model's split);
 * the split-K factor of the nonlocal projection GEMM (Z = Pj C: M =
   projectors, N = orbitals, K = 2 ncoef): few-orbital, small systems have
   only a handful of output tiles, so the K range per CTA decides how many of
@@ -14,7 +18,7 @@ timed on a short Chebyshev filter of the context's resident orbitals (the
 filter kernels themselves, device time by CUDA events on the context
 stream, through the library's own event calls), and the fastest is set on
 the context.  Results are cached per
-problem shape (grid, projectors, orbital tiles of 128, precision), in
+problem shape (grid, projectors, orbital tiles of 64, precision), in
 memory and optionally in a JSON file.
 
 Tuning overwrites the context's filter accumulators: run it before the real
@@ -29,6 +33,7 @@ import numpy as np
 
 CANDIDATES = (0, 1, 2, 4, 8, 16, 32)
 PLANE_THREADS = (256, 128)
+GEMM_BN = (128, 64)
 
 
 class Tuner:
@@ -45,8 +50,8 @@ class Tuner:
     @staticmethod
     def key(ctx, nstate, nproj):
         # the GEMM tile grid depends on the projector count and the orbitals
-        # in 128-wide tiles; K (2 ncoef) follows from the grid
-        return f"{ctx.n[0]}x{ctx.n[1]}x{ctx.n[2]}/P{nproj}/N{(nstate + 127) // 128}/prec{ctx.precision}"
+        # in 64-wide tiles; K (2 ncoef) follows from the grid
+        return f"{ctx.n[0]}x{ctx.n[1]}x{ctx.n[2]}/P{nproj}/N{(nstate + 63) // 64}/prec{ctx.precision}"
 
     def _time(self, ctx, nstate, split, scale, emean):
         ctx.set_gemm_split(split)
@@ -64,13 +69,22 @@ class Tuner:
             b.close()
 
     def tune(self, ctx, nstate, nproj, scale=0.1, emean=0.0):
-        """Pick and set the projection split-K and the plane-stage CTA size
-        for (ctx, nstate); returns the split."""
+        """Pick and set the KB GEMM tile width, the projection split-K and
+        the plane-stage CTA size for (ctx, nstate); returns the split."""
         k = self.key(ctx, nstate, nproj)
         if k not in self.cache:
+            bn = {}
+            if ctx.precision != self.pkg.SDFT_PREC_FP64:  # the FP64 GEMM has one tile shape
+                for w in GEMM_BN:
+                    ctx.set_gemm_bn(w)
+                    bn[str(w)] = self._time(ctx, nstate, 0, scale, emean)
+                ctx.set_gemm_bn(int(min(bn, key=bn.get)))
             times = {str(c): self._time(ctx, nstate, c, scale, emean) for c in self.candidates}
             best = int(min(times, key=times.get))
             entry = {"split": best, "ms": times}
+            if bn:
+                entry["gemm_bn"] = int(min(bn, key=bn.get))
+                entry["gemm_bn_ms"] = bn
             plane = {}
             for nt in PLANE_THREADS:
                 try:
@@ -88,6 +102,8 @@ class Tuner:
         entry = self.cache[k]
         split = int(entry["split"])
         ctx.set_gemm_split(split)
+        if "gemm_bn" in entry:
+            ctx.set_gemm_bn(int(entry["gemm_bn"]))
         if "plane_threads" in entry:
             ctx.set_plane_threads(int(entry["plane_threads"]))
         return split

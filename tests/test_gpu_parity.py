@@ -332,3 +332,82 @@ def test_plane_threads_same_result(pkg, wl, grid):
         assert e.value.code == 5
     finally:
         d.close()
+
+
+@pytest.mark.parametrize("prec_name", ["SDFT_PREC_MIXED", "SDFT_PREC_MIXED_FAST"])
+def test_gemm_tile_width_bitwise(pkg, sys2, prec_name):
+    """The 64- and 128-column tiles of the KB GEMMs give bitwise-equal H.psi
+    and E_NL: each output is the same exact integer sum per K range.  The
+    orbital counts leave a 64-wide tile partly empty, fill it exactly, and
+    cross 128 (where the per-call choice takes 64 for 130 and 128 for 200)."""
+    prec = getattr(pkg, prec_name)
+    c = _ctx(pkg, sys2, 200, prec=prec)
+    try:
+        for ns in (5, 64, 130, 200):
+            cr, ci = _rand(sys2["ncoef"], ns, 31 + ns)
+            out = {}
+            for bn in (128, 64, 0):
+                c.set_gemm_bn(bn)
+                fr, fi, e = c.calc_coef_force(cr, ci, want_enl=True)
+                out[bn] = (np.concatenate([fr, fi]), e)
+            assert np.array_equal(out[64][0], out[128][0]), ns
+            assert out[64][1] == out[128][1], ns
+            assert np.array_equal(out[0][0], out[128][0]), ns
+        with pytest.raises(pkg.SdftError) as e:
+            c.set_gemm_bn(32)
+        assert e.value.code == 1
+    finally:
+        c.close()
+
+
+def test_tuner_sets_shapes(pkg, wl, sys2):
+    """The autotuner times the GEMM tile width, the split-K and the plane CTA
+    size on the context's own orbitals, sets them, caches the entry, and the
+    tuned context filters the same orbitals as an untuned one (to the mixed
+    filter's rounding)."""
+    tuner_mod = __import__(pkg.__name__ + ".tuner", fromlist=["Tuner"])
+    ns = 40
+    cr, ci = _rand(sys2["ncoef"], ns, 5)
+    res = []
+    for tuned in (False, True):
+        c = _ctx(pkg, sys2, ns, prec=1)
+        try:
+            emin, emax = c.lanczos_bounds(12, seed=15, margin=0.1)[:2]
+            scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+            if tuned:
+                t = tuner_mod.Tuner(pkg, steps=2)
+                c.upload(cr, ci)
+                t.tune(c, ns, 4 * sys2["natm"], scale, em)
+                entry = t.cache[t.key(c, ns, 4 * sys2["natm"])]
+                assert entry["gemm_bn"] in (64, 128) and set(entry["gemm_bn_ms"]) == {"64", "128"}
+                assert entry["plane_threads"] in (128, 256)
+            coef = pkg.calcChebyCoeff(16, emax - emin, em, 10.0, em, fun_flag=2)
+            (sr,), (si,) = c.filterChebyPolyHerm(cr, ci, coef, 1, scale, em)
+            res.append(np.concatenate([sr, si]))
+        finally:
+            c.close()
+    assert rel_l2(res[1], res[0]) < 1e-6
+
+
+def test_forced_split_sums_written_partials(pkg, sys2):
+    """A forced split-K that does not divide the K tiles evenly (32 asked for
+    206 K tiles: 7 each, 30 partials written) reduces only the partials the
+    launch wrote.  The 128-wide tile at that split runs first and leaves its
+    partials in the buffer at another stride; the 64-wide tile's filter must
+    still equal the cost model's."""
+    ns = 40
+    cr, ci = _rand(sys2["ncoef"], ns, 5)
+    c = _ctx(pkg, sys2, ns, prec=1)
+    try:
+        emin, emax = c.lanczos_bounds(12, seed=15, margin=0.1)[:2]
+        scale, em = 2.0 / (emax - emin), 0.5 * (emin + emax)
+        coef = pkg.calcChebyCoeff(16, emax - emin, em, 10.0, em, fun_flag=2)
+        (r0,), (i0,) = c.filterChebyPolyHerm(cr, ci, coef, 1, scale, em)
+        ref = np.concatenate([r0, i0])
+        for bn in (128, 64):
+            c.set_gemm_bn(bn)
+            c.set_gemm_split(32)
+            (r,), (i,) = c.filterChebyPolyHerm(cr, ci, coef, 1, scale, em)
+            assert rel_l2(np.concatenate([r, i]), ref) < 1e-12, bn
+    finally:
+        c.close()

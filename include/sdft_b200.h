@@ -36,6 +36,8 @@
  *                                        stodft/reduced-energy/cp-energy-eext-stodft.c:340-470
  *   sdft_vks_local_forces             <- calcLocExtPostScf / control_ewd_loc energy/cp/cp_energy_eext.c:646
  *                                        + ewald3d_selfbgr_cp :2200 (calc-nuclei-force.c:254,581)
+ *   sdft_ewald_real                   <- energy_control_inter_real's Ewald pair term (calc-nuclei-force.c:605,635;
+ *                                        vcoul_bin interface/inter_params/spline_fit.c:415-437)
  *   sdft_mixer_*                      <- genDensityMix stodft/diis.c:34; checkpointOutput/Input
  *                                        stodft/checkpointIO.c:32,218
  */
@@ -333,6 +335,24 @@ int sdft_vks_get_vext(sdft_vks *v, double *re, double *im);
  * vself = -alp/sqrt(pi) sum q^2, vbgr = -pi (sum q)^2 / (2 alp^2 vol)}.
  * The real-space ion-ion Ewald sum (energy_control_inter_real, PINY's
  * classical force engine) is not part of this call. */
+/* The real-space ion-ion Ewald sum of the nuclear force: what
+ * calc-nuclei-force.c:605/635 takes from PINY's pair engine
+ * (energy_control_inter_real over the vcoul_bin table,
+ * interface/inter_params/spline_fit.c:415-437, iperd > 0), summed here
+ * directly over every pair and periodic image closer than rmax:
+ *   E = 1/2 sum_a sum_{b, n; (b, n) != (a, 0)} v(|r_a - r_b - h n|),
+ *   v(r) = q_a q_b gerfc(alp r)/r with the reference's fit of erfc,
+ *   ishift 0: as is; 1: shifted to 0 at rmax; 2: times the reference's cubic
+ *   switch over [rmax - rheal, rmax] (spline_fit.c:61-72, 87-92).
+ * pos[natm*3] Cartesian (bohr), q[natm], hmat as elsewhere (cell vectors in
+ * columns); force[natm*3] = -dE/dR, *energy = E (hartree).  The reference
+ * interpolates v from a table; this evaluates it at each distance, FP64.
+ * Host arrays; runs on the current device and `stream` (may be 0), returns
+ * after it completes.  rmax may span at most 16 cells per direction.
+ * Together with sdft_vks_local_forces' reciprocal, self and background
+ * terms it is the full Ewald ion-ion energy. */
+int sdft_ewald_real(int natm, const double *pos, const double *q, const double *hmat, double alp_ewd, double rmax,
+                    int ishift, double rheal, double *force, double *energy, void *stream);
 int sdft_vks_local_forces(sdft_vks *v, const double *q, const double *q_pseud, double alp_ewd, double *force,
                           double *ewald);
 

@@ -18,7 +18,7 @@ SRCS="stodft/filter.c stodft/normh.c stodft/calc-chempot-chebyshev.c stodft/coef
       mathlib/mathlib.c energy/cp/cp_energy_eext_nonloc.c energy/cp/cp_energy_eext.c
       energy/cp/cp_energy_ee_rho.c interface/cp_ewald/set_cp_ewald.c friend_lib/cmalloc.c
       stodft/density.c stodft/gen-noise.c stodft/diis.c stodft/checkpointIO.c energy/cp/xc_functionals.c
-      stodft/reduced-energy/energy-wrapper-post-scf.c"
+      stodft/reduced-energy/energy-wrapper-post-scf.c interface/inter_params/spline_fit.c"
 OBJS=""
 for f in $SRCS; do
   o="$OUT/obj/$(echo "$f" | tr '/' '_').o"

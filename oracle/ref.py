@@ -53,6 +53,8 @@ def lib(adapter=False):
                               _dp, _dp]
         L.ref_chempot.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        L.ref_coul_table.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                     _dp, _dp, _dp]
         L.ref_num_elec.restype = C.c_double
         L.ref_num_elec.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, C.c_double]
         _libs[path] = L
@@ -262,3 +264,12 @@ def num_elec(L, emin, emax, beta, occ, moments_normalised, mu):
     coefficients of F on [emin, emax]."""
     m = f64(moments_normalised)
     return lib().ref_num_elec(L, emin, emax, beta, occ, _d(m), mu)
+
+
+def coul_table(n, rmin, rmax, alp, qij, ishift=0, rheal=0.0):
+    """The reference's real-space Ewald pair table (ref_coul_table): its r
+    grid, v and dv = -(dv/dr)/r."""
+    r, v, dv = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().ref_coul_table(int(n), rmin, rmax, alp, qij, int(ishift), rheal, _d(r), _d(v), _d(dv))
+    return r, v, dv
+

@@ -52,6 +52,9 @@ void control_ewd_loc(CLATOMS_INFO *, CLATOMS_POS *, CELL *, PTENS *, EWALD *, CP
                      CPOPTS *, ATOMMAPS *, double *, double *, COMMUNICATE *, FOR_SCR *, int, int);
 void ewald3d_selfbgr_cp(CLATOMS_INFO *, EWALD *, PTENS *, double, double *, double *, int);
 double getdeth(double *);
+void spline_vdv(double, double, double *, double *, int, double *, double *, double, double, double, double, double,
+                double, double, double, double, double, double, double, int, int, int, double, int, double, double,
+                double);
 void cpGetVksStodft(CPOPTS *, CPSCR *, CPEWALD *, EWALD *, COMMUNICATE *, CP_COMM_STATE_PKG *, CP_COMM_STATE_PKG *,
                     STAT_AVG *, double *, CELL *, char *, double *, double, double, int, int, int, int, int, int,
                     PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, PARA_FFT_PKG3D *, int);
@@ -990,4 +993,17 @@ int ref_vks(RefSys *r, double ecut, int nsp_loc, double gmin_loc, double dg_loc,
   ps->gzvps[1] = gz_keep;
   ps->nsplin_g = nsp_keep; ps->gmin_spl = gmin_keep; ps->dg_spl = dg_keep;
   return 0;
+}
+
+/* The reference's real-space Ewald pair table (spline_vdv with itype 1,
+ * iperd 1: vcoul_bin's fitted erfc, interface/inter_params/spline_fit.c:
+ * 28-101, 415-437) on its own r grid r_i = dr (i - 3) + rmin, i = 1..n,
+ * dr = (rmax - rmin)/(n - 5): r, v and dv = -(dv/dr)/r at each point, for
+ * ishift 0 (plain), 1 (shifted to 0 at rmax) or 2 (switched over rheal). */
+void ref_coul_table(int n, double rmin, double rmax, double alp, double qij, int ishift, double rheal, double *r,
+                    double *v, double *dv) {
+  double dr = 0.0, dri = 0.0;
+  spline_vdv(rmin, rmax, v - 1, dv - 1, n, &dr, &dri, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, alp, qij, 1,
+             1, ishift, rheal, 0, 0.0, 0.0, 1.0);
+  for (int i = 1; i <= n; i++) r[i - 1] = dr * (double)(i - 3) + rmin;
 }

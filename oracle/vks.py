@@ -142,3 +142,91 @@ def local_forces(hmat, ka, kb, kc, pos, q, q_pseud, vtab, nsplin, gmin, dg, rre,
     vself = -np.dot(q, q) * alp / math.sqrt(math.pi)
     vbgr = -0.5 * q.sum() ** 2 * math.pi / (alp * alp * vol)
     return F, np.array([vrec, vself, vbgr])
+
+
+# The reference's fit of erfc(x) (vcoul_bin, interface/inter_params/
+# spline_fit.c:371-380): erfc(x) ~ sum_i e_i t^i exp(-x^2), t = 1/(1 + p x),
+# within 2.3e-9 of erfc on [0, 6].
+_GERFC_P = 0.3614
+_GERFC_E = (0.2041422096422003, 0.1997535956961481, 0.2213176596405576, 0.03360430734640255,
+            0.4732592578721755, -0.509078520069735, 0.6772631491947646, -0.369912979092217,
+            0.06965131976970335)
+
+
+def coul_pair(r, qij, alp, rmax, ishift=0, rheal=0.0):
+    """vcoul_bin's real-space Ewald pair term (spline_fit.c:415-437, iperd >
+    0) with spline_vdv's switch and shift (:61-72, :87-92), evaluated at r
+    instead of tabulated:
+      v  = qij gerfc(alp r) / r,
+      dv = (gerfc/r^2 + dgerfc/r) qij / r = -(dv/dr) / r,
+    ishift 2: v sw, dv sw + v dsw, sw = 1 + rp^2 (2 rp - 3), rp =
+    clip((r - rmax + rheal)/rheal, 0, 1), dsw = -6 (rp/rheal)(rp - 1)/r;
+    ishift 1: v - v(rmax).  Returns (v, dv)."""
+    r = np.asarray(r, dtype=np.float64)
+
+    def g_dg(rr):
+        x = rr * alp
+        ex = np.exp(-x * x)
+        t = 1.0 / (1.0 + _GERFC_P * x)
+        poly = np.zeros_like(rr)
+        dpoly = np.zeros_like(rr)
+        for i in range(len(_GERFC_E), 0, -1):
+            poly = poly * t + _GERFC_E[i - 1]
+            dpoly = dpoly * t + i * _GERFC_E[i - 1]
+        g = poly * t * ex
+        dg = dpoly * t * t * ex * _GERFC_P * alp + 2.0 * alp * alp * g * rr
+        return g, dg
+
+    g, dg = g_dg(r)
+    v = qij * g / r
+    dv = (g / (r * r) + dg / r) * qij / r
+    if ishift == 2:
+        rp = np.clip((r - rmax + rheal) / rheal, 0.0, 1.0)
+        sw = 1.0 + rp * rp * (2.0 * rp - 3.0)
+        dsw = -6.0 * (rp / rheal) * (rp - 1.0) / r
+        v, dv = v * sw, dv * sw + v * dsw
+    elif ishift == 1:
+        gm, _ = g_dg(np.array([rmax], dtype=np.float64))
+        v = v - qij * gm[0] / rmax
+    return v, dv
+
+
+def ewald_images(hmat, rmax):
+    """Lattice translations h n that can bring a pair (fractional offsets in
+    (-1, 1)) within rmax: |n_i| <= ceil(rmax / w_i) + 1, w_i the cell's
+    width across face i.  Returns [nimg, 3] with n = 0 first."""
+    h = np.asarray(hmat, dtype=np.float64).reshape(3, 3)
+    cols = [h[:, j] for j in range(3)]
+    vol = abs(np.linalg.det(h))
+    nmax = [int(math.ceil(rmax / (vol / np.linalg.norm(np.cross(cols[(j + 1) % 3], cols[(j + 2) % 3]))))) + 1
+            for j in range(3)]
+    ns = [(0, 0, 0)] + [(i, j, k) for i in range(-nmax[0], nmax[0] + 1) for j in range(-nmax[1], nmax[1] + 1)
+                        for k in range(-nmax[2], nmax[2] + 1) if (i, j, k) != (0, 0, 0)]
+    return np.array(ns, dtype=np.float64) @ h.T
+
+
+def ewald_real(hmat, pos, q, alp, rmax, ishift=0, rheal=0.0):
+    """The real-space ion-ion Ewald sum that calc-nuclei-force.c:605/635 gets
+    from energy_control_inter_real (PINY's pair engine over the vcoul_bin
+    table), summed directly over all pairs and periodic images with r <
+    rmax: E = 1/2 sum_a sum_{b, n; (b, n) != (a, 0)} v(|r_a - r_b - h n|),
+    F_a = sum dv (r_a - r_b - h n).  Positions are wrapped into the cell
+    first.  Returns (F [natm, 3], E)."""
+    h = np.asarray(hmat, dtype=np.float64).reshape(3, 3)
+    q = np.asarray(q, dtype=np.float64)
+    s = np.asarray(pos, dtype=np.float64).reshape(-1, 3) @ _hinv(hmat).T
+    s -= np.floor(s)
+    x = s @ h.T
+    img = ewald_images(hmat, rmax)
+    n = len(q)
+    F = np.zeros((n, 3))
+    E = 0.0
+    for a in range(n):
+        d = (x[a] - x)[:, None, :] - img[None, :, :]  # [b, image, 3]
+        r = np.sqrt((d * d).sum(axis=2))
+        m = r < rmax
+        m[a, 0] = False
+        v, dv = coul_pair(r[m], q[a] * q[np.nonzero(m)[0]], alp, rmax, ishift, rheal)
+        E += 0.5 * v.sum()
+        F[a] = (dv[:, None] * d[m]).sum(axis=0)
+    return F, E

@@ -125,6 +125,8 @@ _sig("sdft_vks_set_local", C.c_int, [_vp, C.c_int, _dp, C.c_int, _ip, C.c_int, C
 _sig("sdft_vks_from_rho", C.c_int, [_vp, _vp, C.c_int, _vp, _dp, _dp])
 _sig("sdft_vks_get_vext", C.c_int, [_vp, _dp, _dp])
 _sig("sdft_vks_local_forces", C.c_int, [_vp, _dp, _dp, C.c_double, _dp, _dp])
+_sig("sdft_ewald_real", C.c_int, [C.c_int, _dp, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_double, _dp, _dp,
+                                  _vp])
 _sig("sdft_event_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)])
 _sig("sdft_event_record", C.c_int, [_vp, _vp])
 _sig("sdft_event_query", C.c_int, [_vp, C.POINTER(C.c_int)])
@@ -604,6 +606,20 @@ class Context:
         im = np.zeros(nstate * self.ncoef)
         _chk(lib.sdft_download_filtered(self._p, nstate, imu, _d(re), _d(im)))
         return re, im
+
+
+def ewald_real(hmat, pos, q, alp_ewd, rmax, ishift=0, rheal=0.0, stream=None):
+    """Real-space ion-ion Ewald forces [natm, 3] and energy on the device
+    (the pair term of PINY's energy_control_inter_real, vcoul_bin's fitted
+    erfc; ishift 0 plain, 1 shifted to 0 at rmax, 2 switched over rheal)."""
+    pos = _f64(pos).reshape(-1)
+    q = _f64(q)
+    h = _f64(np.asarray(hmat, dtype=np.float64).reshape(3, 3).T.reshape(9))  # column-major, as the library takes it
+    f = np.zeros(3 * q.size)
+    e = C.c_double(0.0)
+    _chk(lib.sdft_ewald_real(int(q.size), _d(pos), _d(q), _d(h), float(alp_ewd), float(rmax), int(ishift),
+                             float(rheal), _d(f), C.byref(e), stream))
+    return f.reshape(-1, 3), e.value
 
 
 class DensityGrid:

@@ -658,3 +658,174 @@ extern "C" int sdft_vks_get_vext(sdft_vks *v, double *re, double *im) {
   for (int i = 0; i < v->ncoef; i++) { re[i] = h[i].x; im[i] = h[i].y; }
   return SDFT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Real-space ion-ion Ewald sum (the part of calcEnergyForce's nuclear force
+// that calc-nuclei-force.c:605/635 gets from PINY's pair engine,
+// energy_control_inter_real, over the vcoul_bin table).  The pair term is
+// vcoul_bin's (interface/inter_params/spline_fit.c:415-437, iperd > 0) with
+// spline_vdv's shift or switch (:61-72, :87-92), evaluated at each distance
+// in FP64 instead of interpolated from a table:
+//   v = qq gerfc(alp r)/r,  dv = -(dv/dr)/r = (gerfc/r^2 + dgerfc/r) qq/r,
+//   gerfc(x) = sum_i e_i t^i exp(-x^2), t = 1/(1 + p x)  (the reference's fit
+//   of erfc, within 2.3e-9 of it).
+// One CTA per atom a sums its pairs (b, image n) over a fixed thread split and
+// reduces them in a fixed order, so results are reproducible.
+// ---------------------------------------------------------------------------
+namespace sdft {
+namespace {
+constexpr int kEwThreads = 256;
+// the fit's constants, spline_fit.c:373-376
+__device__ __forceinline__ void gerfc_fit(double x, double alp, double r, double &g, double &dg) {
+  constexpr double p = 0.3614;
+  constexpr double e[9] = {0.2041422096422003, 0.1997535956961481, 0.2213176596405576, 0.03360430734640255,
+                           0.4732592578721755, -0.509078520069735,  0.6772631491947646, -0.369912979092217,
+                           0.06965131976970335};
+  const double ex = exp(-x * x);
+  const double t = 1.0 / (1.0 + p * x);
+  double poly = 0.0, dpoly = 0.0;
+#pragma unroll
+  for (int i = 9; i >= 1; i--) {
+    poly = poly * t + e[i - 1];
+    dpoly = dpoly * t + i * e[i - 1];
+  }
+  g = poly * t * ex;
+  dg = dpoly * t * t * ex * p * alp + 2.0 * alp * alp * g * r;
+}
+
+__global__ void __launch_bounds__(kEwThreads)
+k_ewald_real(const double *__restrict__ x, const double *__restrict__ q, int natm, const double *__restrict__ img,
+             int nimg, double alp, double rmax, int ishift, double rheal, double vshift, double *__restrict__ force,
+             double *__restrict__ epart) {
+  const int a = blockIdx.x;
+  const double xa = x[3 * a], ya = x[3 * a + 1], za = x[3 * a + 2], qa = q[a];
+  const double rmax2 = rmax * rmax;
+  double fx = 0.0, fy = 0.0, fz = 0.0, en = 0.0;
+  const long long tot = (long long)natm * nimg;
+  for (long long t = threadIdx.x; t < tot; t += kEwThreads) {
+    const int b = (int)(t / nimg), m = (int)(t - (long long)b * nimg);
+    if (b == a && m == 0) continue;  // image 0 is n = 0
+    const double dx = xa - x[3 * b] - img[3 * m], dy = ya - x[3 * b + 1] - img[3 * m + 1],
+                 dz = za - x[3 * b + 2] - img[3 * m + 2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 >= rmax2) continue;
+    const double r = sqrt(r2), qq = qa * q[b];
+    double g, dg;
+    gerfc_fit(r * alp, alp, r, g, dg);
+    double v = qq * g / r;
+    double dv = (g / r2 + dg / r) * qq / r;
+    if (ishift == 2) {
+      double rp = (r - rmax + rheal) / rheal;
+      rp = fmin(fmax(rp, 0.0), 1.0);
+      const double sw = 1.0 + rp * rp * (2.0 * rp - 3.0);
+      const double dsw = -6.0 * (rp / rheal) * (rp - 1.0) / r;
+      dv = dv * sw + v * dsw;
+      v = v * sw;
+    } else if (ishift == 1) {
+      v -= qq * vshift;
+    }
+    en += 0.5 * v;
+    fx += dv * dx;
+    fy += dv * dy;
+    fz += dv * dz;
+  }
+  __shared__ double red[kEwThreads / 32][4];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_down_sync(0xffffffffu, fx, o);
+    fy += __shfl_down_sync(0xffffffffu, fy, o);
+    fz += __shfl_down_sync(0xffffffffu, fz, o);
+    en += __shfl_down_sync(0xffffffffu, en, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    const int w = threadIdx.x >> 5;
+    red[w][0] = fx; red[w][1] = fy; red[w][2] = fz; red[w][3] = en;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < kEwThreads / 32; w++)
+      for (int c = 0; c < 4; c++) s[c] += red[w][c];
+    force[3 * a] = s[0]; force[3 * a + 1] = s[1]; force[3 * a + 2] = s[2];
+    epart[a] = s[3];
+  }
+}
+
+double gerfc_host(double x) {  // the same fit on the host (the ishift 1 shift)
+  const double p = 0.3614;
+  const double e[9] = {0.2041422096422003, 0.1997535956961481, 0.2213176596405576, 0.03360430734640255,
+                       0.4732592578721755, -0.509078520069735,  0.6772631491947646, -0.369912979092217,
+                       0.06965131976970335};
+  const double t = 1.0 / (1.0 + p * x);
+  double poly = 0.0;
+  for (int i = 9; i >= 1; i--) poly = poly * t + e[i - 1];
+  return poly * t * std::exp(-x * x);
+}
+}  // namespace
+}  // namespace sdft
+
+extern "C" int sdft_ewald_real(int natm, const double *pos, const double *q, const double *hmat, double alp_ewd,
+                               double rmax, int ishift, double rheal, double *force, double *energy, void *stream) {
+  if (natm < 1 || !pos || !q || !hmat || !force || !energy || !(alp_ewd > 0.0) || !(rmax > 0.0) || ishift < 0 ||
+      ishift > 2 || (ishift == 2 && !(rheal > 0.0 && rheal <= rmax)))
+    return set_error(SDFT_ERR_ARG, "ewald_real: bad argument");
+  double hi[9], vol;
+  inv3(hmat, hi, &vol);
+  vol = std::fabs(vol);
+  if (!(vol > 0.0)) return set_error(SDFT_ERR_ARG, "ewald_real: singular cell");
+  // positions wrapped into the cell; lattice translations h n with |n_i| <=
+  // ceil(rmax / w_i) + 1 (w_i the width across face i), n = 0 first
+  std::vector<double> x(3 * (size_t)natm);
+  for (int a = 0; a < natm; a++) {
+    double s[3];
+    for (int i = 0; i < 3; i++) {
+      s[i] = pos[3 * a] * hi[i] + pos[3 * a + 1] * hi[i + 3] + pos[3 * a + 2] * hi[i + 6];
+      s[i] -= std::floor(s[i]);
+    }
+    for (int i = 0; i < 3; i++) x[3 * a + i] = hmat[i] * s[0] + hmat[i + 3] * s[1] + hmat[i + 6] * s[2];
+  }
+  int nmax[3];
+  for (int j = 0; j < 3; j++) {
+    const double *u = hmat + 3 * ((j + 1) % 3), *w = hmat + 3 * ((j + 2) % 3);
+    const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+    const double width = vol / std::sqrt(cx * cx + cy * cy + cz * cz);
+    const double n = std::ceil(rmax / width) + 1.0;
+    if (n > 16.0) return set_error(SDFT_ERR_ARG, "ewald_real: cutoff spans more than 16 cells");
+    nmax[j] = (int)n;
+  }
+  std::vector<double> img(3, 0.0);
+  for (int i = -nmax[0]; i <= nmax[0]; i++)
+    for (int j = -nmax[1]; j <= nmax[1]; j++)
+      for (int k = -nmax[2]; k <= nmax[2]; k++) {
+        if (!i && !j && !k) continue;
+        for (int c = 0; c < 3; c++) img.push_back(hmat[c] * i + hmat[c + 3] * j + hmat[c + 6] * k);
+      }
+  const int nimg = (int)(img.size() / 3);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(SDFT_ERR_NODEVICE, "ewald_real: no device");
+  const size_t bytes = (x.size() + natm + img.size() + 4 * (size_t)natm) * sizeof(double);
+  void *buf = nullptr;
+  int r = dev_alloc(dev, stream, &buf, bytes);
+  if (r) return r;
+  double *d_x = static_cast<double *>(buf), *d_q = d_x + x.size(), *d_img = d_q + natm, *d_f = d_img + img.size(),
+         *d_e = d_f + 3 * (size_t)natm;
+  std::vector<double> ep(natm);
+  cudaError_t e = cudaMemcpyAsync(d_x, x.data(), x.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_q, q, natm * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, img.data(), img.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    k_ewald_real<<<natm, kEwThreads, 0, st>>>(d_x, d_q, natm, d_img, nimg, alp_ewd, rmax, ishift, rheal,
+                                              gerfc_host(alp_ewd * rmax) / rmax, d_f, d_e);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(force, d_f, 3 * (size_t)natm * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ep.data(), d_e, natm * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  dev_free(buf, stream);
+  if (e != cudaSuccess) return set_error(SDFT_ERR_CUDA, cudaGetErrorString(e));
+  double s = 0.0;
+  for (int a = 0; a < natm; a++) s += ep[a];
+  *energy = s;
+  return SDFT_OK;
+}

@@ -241,3 +241,45 @@ def test_local_forces_pinned(wl, q_pseud):
         p2[a, c] -= d
         num = -(energy(p1) - energy(p2)) / (2 * d)
         assert abs(num - F[a, c]) < 1e-6 * np.abs(F).max()
+
+
+@pytest.mark.parametrize("alp,ishift", [(0.3, 0), (0.9, 0), (0.3, 1), (0.3, 2), (1.2, 2)])
+def test_coul_pair_pinned(alp, ishift):
+    """The real-space Ewald pair term of the restatement (vcoul_bin's fitted
+    erfc with spline_vdv's shift or switch) against the reference's own
+    table on its own r grid."""
+    from oracle import vks as V
+    r, v, dv = R.coul_table(3000, 0.5, 9.0, alp, 3.7, ishift, 1.5)
+    ov, odv = V.coul_pair(r, 3.7, alp, 9.0, ishift, 1.5)
+    assert np.abs(ov - v).max() <= 1e-14 * np.abs(v).max()
+    assert np.abs(odv - dv).max() <= 1e-14 * np.abs(dv).max()
+
+
+def test_ewald_real_forces_and_alpha(wl):
+    """The restated real-space ion-ion Ewald sum: its force is -dE/dR (central
+    differences), and the full Ewald energy -- this sum plus the reference's
+    own reciprocal, self and background terms -- does not depend on the
+    splitting parameter, to the accuracy of the erfc fit (2.3e-9)."""
+    from oracle import vks as V
+    s = wl.make_system(1, (32, 32, 32), disp_sigma=0.05, seed=2)
+    q = np.full(s["natm"], 4.0)
+    F, E = V.ewald_real(s["hmat"], s["pos"], q, 1.0, 9.0)
+    d = 1e-5
+    for a, c in ((0, 0), (3, 1), (5, 2)):
+        p1, p2 = s["pos"].copy(), s["pos"].copy()
+        p1[a, c] += d
+        p2[a, c] -= d
+        num = -(V.ewald_real(s["hmat"], p1, q, 1.0, 9.0)[1] - V.ewald_real(s["hmat"], p2, q, 1.0, 9.0)[1]) / (2 * d)
+        assert abs(num - F[a, c]) < 1e-7 * np.abs(F).max()
+    r = R.RefSys(s, 4)
+    vtab, gmin, dg, gz = wl.local_table()
+    rho_in = np.full(int(np.prod(s["grid"])), s["num_elec"] / np.prod(s["grid"]))
+    # alp 0.4 and 0.5 with a 20 bohr cutoff: the real-space part moves from
+    # 0.70 to 0.10 hartree of a -33.6 total, the reciprocal part from 3.9 to 8.4
+    tot, real = [], []
+    for alp in (0.4, 0.5):
+        ref = r.vks(wl.ECUT_HA, vtab, gmin, dg, gz, 1, rho_in, q=q, q_pseud=4.0, alp_ewd=alp)
+        real.append(V.ewald_real(s["hmat"], s["pos"], q, alp, 20.0)[1])
+        tot.append(real[-1] + ref["ewald"].sum())
+    assert real[0] - real[1] > 0.5
+    assert abs(tot[0] - tot[1]) < 1e-9 * abs(tot[1])

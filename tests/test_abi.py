@@ -3,6 +3,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -34,6 +35,23 @@ def test_no_device_is_reported_cleanly(pkg, sys1):
 def test_host_validation(pkg):
     with pytest.raises(pkg.SdftError):
         pkg.calcChebyCoeff(0, 1.0, 0.0, 1000.0, 0.0)
+
+
+@pytest.mark.parametrize("kw", [dict(alp=0.0), dict(rmax=-1.0), dict(ishift=3), dict(ishift=2, rheal=0.0),
+                                dict(ishift=2, rheal=30.0), dict(rmax=400.0), dict(natm=0)])
+def test_ewald_real_arguments_checked_before_the_device(pkg, kw):
+    """sdft_ewald_real refuses bad arguments with SDFT_ERR_ARG before it
+    touches a device: a non-positive splitting parameter or cutoff, an unknown
+    shift option, a switching width outside (0, rmax], a cutoff spanning more
+    than 16 cells, no atoms."""
+    h = np.eye(3) * 10.0
+    a = dict(alp=0.5, rmax=20.0, ishift=0, rheal=1.0, natm=2)
+    a.update(kw)
+    pos = np.zeros((max(a["natm"], 1), 3))
+    q = np.ones(a["natm"])
+    with pytest.raises(pkg.SdftError) as e:
+        pkg.ewald_real(h, pos[:a["natm"]] if a["natm"] else pos[:0], q, a["alp"], a["rmax"], a["ishift"], a["rheal"])
+    assert e.value.code == 1  # SDFT_ERR_ARG
 
 
 ADAPTED = ("filterChebyPolyHerm", "filterNewtonPolyHerm", "normHCheby", "normHNewtonHerm", "calcChebyMoments",

@@ -161,11 +161,20 @@ struct AllElems {
   __device__ __forceinline__ AllK line(int) const { return AllK{}; }
 };
 
+// P34 (R1 = 8 only): the elements j2 + R2 j1 with j1 = 3, 4 -- natural
+// indices 3N/8 .. 5N/8 - 1, i.e. |k| >= 3N/8 -- hold no data on input (dif)
+// and are not needed on output (dit), as for a sphere narrower than 3N/8:
+// they are neither read nor written, and no mask is evaluated for them.
+template <int R1> __device__ __forceinline__ constexpr bool band34(bool p34, int j1) {
+  return p34 && R1 == 8 && (j1 == 3 || j1 == 4);
+}
+
 // natural -> permuted.  twN: exp(-2 pi i t/N) (shared-memory table or accessor).
-template <int N, int ES, int DIR, typename C, typename LM, typename TW, typename MK = AllElems>
+template <int N, int ES, int DIR, bool P34 = false, typename C, typename LM, typename TW, typename MK = AllElems>
 __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr,
                                     const MK &mask = MK{}) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+  static_assert(!P34 || R1 == 8, "the j1 = 3, 4 band needs R1 = 8");
   if (nl > 0) {
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {
@@ -177,7 +186,7 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN,
 #pragma unroll
       for (int j1 = 0; j1 < R1; j1++) {
         const int k = j2 + R2 * j1;
-        v[j1] = in(k) ? p[k * ES] : cmk<C>(0.0, 0.0);
+        v[j1] = (!band34<R1>(P34, j1) && in(k)) ? p[k * ES] : cmk<C>(0.0, 0.0);
       }
       dftr<R1, DIR>(v);
       p[j2 * ES] = v[0];
@@ -208,10 +217,11 @@ __device__ __forceinline__ void dif(C *buf, const LM &lm, int nl, const TW &twN,
 }
 
 // permuted -> natural
-template <int N, int ES, int DIR, typename C, typename LM, typename TW, typename MK = AllElems>
+template <int N, int ES, int DIR, bool P34 = false, typename C, typename LM, typename TW, typename MK = AllElems>
 __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN, int tid, int nthr,
                                     const MK &mask = MK{}) {
   constexpr int R1 = Plan<N>::R1, R2 = Plan<N>::R2;
+  static_assert(!P34 || R1 == 8, "the j1 = 3, 4 band needs R1 = 8");
   if (nl > 0) {
 #pragma unroll 1
     for (UnitIter it(tid, nthr, nl); it.j < R1; it.next()) {
@@ -246,7 +256,7 @@ __device__ __forceinline__ void dit(C *buf, const LM &lm, int nl, const TW &twN,
 #pragma unroll
       for (int j1 = 0; j1 < R1; j1++) {
         const int k = j2 + R2 * j1;
-        if (out(k)) p[k * ES] = v[j1];
+        if (!band34<R1>(P34, j1) && out(k)) p[k * ES] = v[j1];
       }
     }
   }

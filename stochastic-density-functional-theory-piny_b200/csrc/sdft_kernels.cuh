@@ -21,6 +21,8 @@ struct DevGeom {
   const int2 *kb_rng;   // [n1] per plane row a: signed kb range [x, y] of its sphere columns
   int kb_contig;        // every row's columns fill its kb range (else kb_rng is not used)
   int plane_nt;         // FP32 plane stage threads per CTA: 0 = default (256), or 128
+  int kbmax;            // largest |kb| of the sphere columns
+  int prune34;          // 8 kamax < 3 n1 and 8 kbmax < 3 n2: the plane passes skip the j1 = 3, 4 band
   const int *cp_gstart; // [ncp] first G index of the pair's direct column
   const int *cp_gcount; // [ncp]
   const int *col_ab;    // [ncols] (ka mod n1) << 16 | (kb mod n2)

@@ -718,7 +718,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
       if (cnt[a] && cnt[a] != rng[a].y - rng[a].x + 1) g.kb_contig = 0;
       if (cnt[a]) g.kbmax = std::max(g.kbmax, std::max(std::abs(rng[a].x), std::abs(rng[a].y)));
     }
-    g.prune34 = (8 * g.kamax < 3 * n1 && 8 * g.kbmax < 3 * n2) ? 1 : 0;
+    g.prune34 = (8 * g.kamax < 3 * n1 && 8 * g.kbmax < 3 * n2) ? (4 * g.kamax >= n1 ? 2 : 1) : 0;
     DMF(ctx->d_kb_rng, n1 * sizeof(int2));
     CKF(cudaMemcpyAsync(ctx->d_kb_rng, rng.data(), n1 * sizeof(int2), cudaMemcpyHostToDevice, ctx->st));
     CKF(cudaStreamSynchronize(ctx->st));  // (rng is a local)

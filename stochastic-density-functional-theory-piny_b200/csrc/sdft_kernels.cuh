@@ -22,7 +22,8 @@ struct DevGeom {
   int kb_contig;        // every row's columns fill its kb range (else kb_rng is not used)
   int plane_nt;         // FP32 plane stage threads per CTA: 0 = default (256), or 128
   int kbmax;            // largest |kb| of the sphere columns
-  int prune34;          // 8 kamax < 3 n1 and 8 kbmax < 3 n2: the plane passes skip the j1 = 3, 4 band
+  int prune34;          // 1: 8 kamax < 3 n1 and 8 kbmax < 3 n2, the plane passes skip the j1 = 3, 4 band;
+                        // 2: also 4 kamax >= n1, the a-pass rows with j1 = 0, 1, 6, 7 are all inside
   const int *cp_gstart; // [ncp] first G index of the pair's direct column
   const int *cp_gcount; // [ncp]
   const int *col_ab;    // [ncols] (ka mod n1) << 16 | (kb mod n2)

@@ -469,14 +469,23 @@ template <int N1> struct RowsPerm {  // rows given in permuted-a order
 // DFT -> x V -> inverse DFT without a round trip through shared memory.
 // Rows with kamax < ka < N1 - kamax are zero on input (outside the sphere)
 // and not needed on output: they are neither read nor written.
-// P34: rows ka in the j1 = 3, 4 band (|ka| >= 3 N1/8, outside a sphere
+// PM >= 1: rows ka in the j1 = 3, 4 band (|ka| >= 3 N1/8, outside a sphere
 // narrower than that) are skipped at compile time, with no activity test.
-template <int N1, bool P34 = false, typename C2, typename T, typename TW>
+// PM == 2: the sphere is also at least N1/4 wide, so the rows with j1 = 0,
+// 1, 6, 7 are always inside it and only j1 = 2, 5 are tested.
+template <int N1, int PM = 0, typename C2, typename T, typename TW>
 __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, const T *__restrict__ Vpl, int kamax,
                                              const TW &tw1, int tid, int nthr) {
   constexpr int R1 = Plan<N1>::R1, R2 = Plan<N1>::R2;
+  constexpr bool P34 = PM >= 1;
   static_assert(!P34 || R1 == 8, "the j1 = 3, 4 band needs R1 = 8");
-  auto active = [&](int ka) { return ka <= kamax || ka >= N1 - kamax; };
+  auto active_ka = [&](int ka) { return ka <= kamax || ka >= N1 - kamax; };
+  // row ka = j2 + R2 j1 holds data (j1 a compile-time constant after unrolling)
+  auto active_j = [&](int j1, int ka) {
+    if (band34<R1>(P34, j1)) return false;
+    if (PM == 2 && (j1 == 0 || j1 == 1 || j1 == 6 || j1 == 7)) return true;
+    return active_ka(ka);
+  };
 #pragma unroll 1
   for (UnitIter it(tid, nthr, nl); it.j < R2; it.next()) {  // forward pass 1
     const int l = it.l, j2 = it.j;
@@ -485,7 +494,7 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
 #pragma unroll
     for (int j1 = 0; j1 < R1; j1++) {
       const int ka = j2 + R2 * j1;
-      v[j1] = (!band34<R1>(P34, j1) && active(ka)) ? p[ka * P2] : cmk<C2>(0.0, 0.0);
+      v[j1] = active_j(j1, ka) ? p[ka * P2] : cmk<C2>(0.0, 0.0);
     }
     dftr<R1, +1>(v);
     p[j2 * P2] = v[0];
@@ -525,7 +534,7 @@ __device__ __forceinline__ void plane_a_vmul(C2 *pl, int P2, int nl, int N2, con
 #pragma unroll
     for (int j1 = 0; j1 < R1; j1++) {
       const int ka = j2 + R2 * j1;
-      if (!band34<R1>(P34, j1) && active(ka)) p[ka * P2] = v[j1];
+      if (active_j(j1, ka)) p[ka * P2] = v[j1];
     }
   }
   __syncthreads();
@@ -552,9 +561,11 @@ template <int N2> struct RowKb {
 
 // NT threads per plane CTA: PlaneCfg's default, or (FP32) the 128-thread
 // instance that the autotuner may pick for small planes (more resident CTAs).
-// P34: the sphere is narrower than 3/8 of both plane edges (R1 = 8 plans):
-// the j1 = 3, 4 band of the first forward and last inverse passes is skipped.
-template <typename T, int N1, int N2, int NT = PlaneCfg<T>::NT, int MINB = PlaneCfg<T>::MINB, bool P34 = false>
+// PM (DevGeom::prune34): 1 = the sphere is narrower than 3/8 of both plane
+// edges (R1 = 8 plans): the j1 = 3, 4 band of the first forward and last
+// inverse passes is skipped; 2 = also at least a quarter of N1 wide, so the
+// a-pass tests only the rows with j1 = 2, 5.
+template <typename T, int N1, int N2, int NT = PlaneCfg<T>::NT, int MINB = PlaneCfg<T>::MINB, int PM = 0>
 __global__ void __launch_bounds__(NT, MINB)
 kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict__ Vp) {
   using C2 = typename CT<T>::type;
@@ -590,13 +601,13 @@ kf_stage_b(DevGeom g, typename CT<T>::type *__restrict__ X, const T *__restrict_
   const Lines2P rowsp{ka + 1, g1, ka, P2, (N1 - ka) * P2};
   if (contig) {  // only the sphere's elements are read before and written after the b-transforms
     const RowKb<N2> m{rng, g1, N1 - ka};
-    dif<N2, 1, +1, P34>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
-    plane_a_vmul<N1, P34>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
-    dit<N2, 1, -1, P34>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
+    dif<N2, 1, +1, (PM >= 1)>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
+    plane_a_vmul<N1, PM>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
+    dit<N2, 1, -1, (PM >= 1)>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT, m);
   } else {
-    dif<N2, 1, +1, P34>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
-    plane_a_vmul<N1, P34>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
-    dit<N2, 1, -1, P34>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+    dif<N2, 1, +1, (PM >= 1)>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
+    plane_a_vmul<N1, PM>(pl, P2, N2, N2, Vp + (size_t)r * N1 * N2, ka, TwC<N1, C2>{}, tid, NT);
+    dit<N2, 1, -1, (PM >= 1)>(pl, rowsp, g1 + g2, TwC<N2, C2>{}, tid, NT);
   }
   for (int col = tid; col < g.ncols; col += NT) {
     const int ab = g.col_ab[col];
@@ -776,9 +787,9 @@ bool fast_stage_c(const DevGeom &g, const void *X, const EpiArgs &e, int npairs,
   return true;
 }
 
-template <typename T, int A, int B, int NT, int MINB, bool P34>
+template <typename T, int A, int B, int NT, int MINB, int PM>
 static void launch_plane_b(const DevGeom &g, dim3 grid, size_t sm, void *X, const T *Vp, cudaStream_t st) {
-  auto k = kf_stage_b<T, A, B, NT, MINB, P34>;
+  auto k = kf_stage_b<T, A, B, NT, MINB, PM>;
   static const bool attr_once = (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), true);
   (void)attr_once;
   k<<<grid, NT, sm, st>>>(g, (typename CT<T>::type *)X, Vp);
@@ -791,20 +802,23 @@ bool fast_stage_b(const DevGeom &g, void *X, const T *Vp, int npairs, cudaStream
   const bool small = std::is_same<T, float>::value && g.plane_nt == 128;
   // the j1 = 3, 4 band skipped where both edges factor with R1 = 8 and the
   // sphere is narrower than 3/8 of them (DevGeom::prune34)
-#define LB(A, B)                                                                                          \
+#define LBP(NT_, MB_)                                                                                     \
   do {                                                                                                    \
+    if (pm == 2) launch_plane_b<T, A, B, NT_, MB_, (ok34 ? 2 : 0)>(g, grid, sm, X, Vp, st);               \
+    else if (pm == 1) launch_plane_b<T, A, B, NT_, MB_, (ok34 ? 1 : 0)>(g, grid, sm, X, Vp, st);          \
+    else launch_plane_b<T, A, B, NT_, MB_, 0>(g, grid, sm, X, Vp, st);                                    \
+  } while (0)
+#define LB(A_, B_)                                                                                        \
+  do {                                                                                                    \
+    constexpr int A = A_, B = B_;                                                                         \
     constexpr bool ok34 = Plan<A>::R1 == 8 && Plan<B>::R1 == 8;                                           \
-    const bool p34 = ok34 && g.prune34;                                                                   \
-    if (small) {                                                                                          \
-      if (p34) launch_plane_b<T, A, B, 128, 6, ok34>(g, grid, sm, X, Vp, st);                             \
-      else launch_plane_b<T, A, B, 128, 6, false>(g, grid, sm, X, Vp, st);                                \
-    } else {                                                                                              \
-      if (p34) launch_plane_b<T, A, B, PlaneCfg<T>::NT, PlaneCfg<T>::MINB, ok34>(g, grid, sm, X, Vp, st); \
-      else launch_plane_b<T, A, B, PlaneCfg<T>::NT, PlaneCfg<T>::MINB, false>(g, grid, sm, X, Vp, st);    \
-    }                                                                                                     \
+    const int pm = ok34 ? g.prune34 : 0;                                                                  \
+    if (small) LBP(128, 6);                                                                               \
+    else LBP(PlaneCfg<T>::NT, PlaneCfg<T>::MINB);                                                         \
   } while (0)
   SDFT_FOR_PLANE(LB);
 #undef LB
+#undef LBP
   return true;
 }
 

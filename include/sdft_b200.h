@@ -398,10 +398,11 @@ int sdft_ctx_set_gemm_split(sdft_ctx *ctx, int split);
  * same exact integer sum per K range.  No counterpart in the reference. */
 int sdft_ctx_set_gemm_bn(sdft_ctx *ctx, int bn);
 /* Threads per CTA of the FP32 plane stage (one CTA per plane and orbital
- * pair): 0 or 256 (the default) or 128, which fits twice the CTAs per SM
- * and can be faster for small planes.  Mixed-precision contexts on the
- * fast FFT path only; chosen per system by the autotuner (tuner.py).  No
- * counterpart in the reference. */
+ * pair): 256, 128 (more CTAs per SM, faster on small planes), or 0 = the
+ * library's default, 128 for planes of 48 x 48 to 72 x 72 points and 256
+ * otherwise.  128 is
+ * accepted by mixed-precision contexts on the fast FFT path only; chosen
+ * per system by the autotuner (tuner.py).  No counterpart in the reference. */
 int sdft_ctx_set_plane_threads(sdft_ctx *ctx, int nt);
 /* CUDA stream priority of the context's stream (lower = more urgent, 0 =
  * default; clamped to the device's range).  Call while the context is idle:

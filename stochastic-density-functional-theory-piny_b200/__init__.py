@@ -550,7 +550,8 @@ class Context:
         _chk(lib.sdft_ctx_set_gemm_bn(self._p, int(bn)))
 
     def set_plane_threads(self, nt):
-        """Threads per CTA of the FP32 plane stage: 0 (default 256), 128 or 256."""
+        """Threads per CTA of the FP32 plane stage: 128, 256, or 0 = the
+        library's default (128 for 48 x 48 to 72 x 72 planes, 256 otherwise)."""
         _chk(lib.sdft_ctx_set_plane_threads(self._p, int(nt)))
 
     def set_priority(self, priority):
@@ -784,7 +785,8 @@ class Batch:
         _chk(lib.sdft_batch_sync(self._p))
 
     def set_plane_threads(self, nt):
-        """Threads per CTA of the FP32 plane stage: 0 (default 256), 128 or 256."""
+        """Threads per CTA of the FP32 plane stage: 128, 256, or 0 = the
+        library's default (128 for 48 x 48 to 72 x 72 planes, 256 otherwise)."""
         _chk(lib.sdft_ctx_set_plane_threads(self._p, int(nt)))
 
     def set_priority(self, priority):

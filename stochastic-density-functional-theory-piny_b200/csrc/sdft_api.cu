@@ -280,6 +280,15 @@ static int download_block(sdft_ctx *ctx, const double *src, int nstate, double *
 
 static bool is_fp64(const sdft_ctx *c) { return c->fft64; }
 
+// Default CTA size of the FP32 plane stage: 128 threads for planes of 48 x 48
+// to 72 x 72 points, where registers, not the plane's shared memory, bound
+// the CTAs per SM (stage B 24 % faster at 48 x 48, config 2 +8.8 %; the
+// autotuner took 128 for 30 of the 32 batch systems), 256 otherwise (12 %
+// faster at 96 x 96; config 1's 24 x 24 planes 1.3 % faster at 256).
+static int default_plane_threads(const sdft_ctx *c) {
+  return (!c->fft64 && c->fast && c->n1 <= 72 && c->n2 <= 72 && c->n1 * c->n2 >= 48 * 48) ? 128 : 256;
+}
+
 // Nonlocal projection Z = Pj C and back projection FNL = Bk Z for `nstate`
 // orbitals held in `vec`, mixed precision: INT8 Ozaki GEMMs on the digit
 // form of the orbitals; Z = Pj C is split over K with FP64 partial sums, the
@@ -694,6 +703,7 @@ extern "C" int sdft_ctx_create(int n1, int n2, int n3, int ncoef, const int *ka,
   CKF(cudaMemcpyAsync(ctx->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
   DevGeom &g = ctx->g;
   g.n1 = n1; g.n2 = n2; g.n3 = n3; g.N = ctx->N;
+  g.plane_nt = default_plane_threads(ctx);
   g.ncoef = ncoef; g.ngp = ctx->ngp;
   g.ncols = ctx->cols.ncols; g.ncols_pad = ctx->cols.ncols_pad; g.ncp = ctx->cols.ncp; g.kamax = ctx->cols.kamax;
   g.nbatch = (g.ncp + kCPB - 1) / kCPB;
@@ -1433,7 +1443,7 @@ extern "C" int sdft_ctx_set_plane_threads(sdft_ctx *ctx, int nt) {
   if (nt != 0 && nt != 128 && nt != 256) return set_error(SDFT_ERR_ARG, "plane_threads: 0 (default), 128 or 256");
   if (nt == 128 && (is_fp64(ctx) || !ctx->fast))
     return set_error(SDFT_ERR_UNSUPPORTED, "plane_threads: 128 exists for the FP32 fast plane stage only");
-  ctx->g.plane_nt = nt == 256 ? 0 : nt;
+  ctx->g.plane_nt = nt == 0 ? default_plane_threads(ctx) : nt;
   return SDFT_OK;
 }
 

@@ -20,7 +20,7 @@ struct DevGeom {
   int nbatch;           // ceil(ncp / kCPB)
   const int2 *kb_rng;   // [n1] per plane row a: signed kb range [x, y] of its sphere columns
   int kb_contig;        // every row's columns fill its kb range (else kb_rng is not used)
-  int plane_nt;         // FP32 plane stage threads per CTA: 0 = default (256), or 128
+  int plane_nt;         // FP32 plane stage threads per CTA: 256 or 128
   int kbmax;            // largest |kb| of the sphere columns
   int prune34;          // 1: 8 kamax < 3 n1 and 8 kbmax < 3 n2, the plane passes skip the j1 = 3, 4 band;
                         // 2: also 4 kamax >= n1, the a-pass rows with j1 = 0, 1, 6, 7 are all inside

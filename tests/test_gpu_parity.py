@@ -310,19 +310,20 @@ def test_call_order_and_sizes_checked(pkg, sys1):
 
 @pytest.mark.parametrize("grid", [(24, 24, 24), (48, 48, 48), (96, 96, 96)])
 def test_plane_threads_same_result(pkg, wl, grid):
-    """The 128-thread plane-stage instance (an autotuner choice) computes the
-    same units as the 256-thread one: bitwise equal H.psi, and the knob is
-    refused where it does not exist (FP64)."""
+    """The 128-thread plane-stage instance (the default for 48 x 48 to 72 x 72 planes,
+    an autotuner choice) computes the same units as the 256-thread one:
+    bitwise equal H.psi for 256, 128 and the default, and the knob is refused
+    where it does not exist (FP64)."""
     nrep = grid[0] // 24
     s = wl.make_system(nrep, grid)
     c = _ctx(pkg, s, 6, prec=1)
     try:
         cr, ci = _rand(s["ncoef"], 6, 8)
-        a = np.concatenate(c.calc_coef_force(cr, ci))
-        c.set_plane_threads(128)
-        b = np.concatenate(c.calc_coef_force(cr, ci))
-        c.set_plane_threads(0)
-        assert np.array_equal(a, b)
+        out = []
+        for nt in (256, 128, 0):
+            c.set_plane_threads(nt)
+            out.append(np.concatenate(c.calc_coef_force(cr, ci)))
+        assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
     finally:
         c.close()
     d = _ctx(pkg, s, 2, prec=0)

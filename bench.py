@@ -277,6 +277,15 @@ def run_ours(args):
     t1 = time.time()
     chi_h = ctx.genNoiseOrbitalReal(nsto, seed=10.0, np_states=world, myid=rank)
     noise_s = time.time() - t1
+    # launch shapes from the autotuner (tile width and split-K of the KB GEMMs,
+    # plane-stage CTA size), timed on these resident noise orbitals
+    tuned = None
+    if args.plane_threads == "tuned" and prec != pkg.SDFT_PREC_FP64:
+        tn = __import__(pkg.__name__ + ".tuner", fromlist=["Tuner"]).Tuner(pkg)
+        tn.tune(ctx, nsto, s["_P"], scale, emean)
+        entry = tn.cache[tn.key(ctx, nsto, s["_P"])]
+        tuned = {"gemm_bn": entry.get("gemm_bn"), "gemm_split": entry["split"],
+                 "plane_threads": entry.get("plane_threads")}
     # chemical potential from the moments (calcChemPotCheby), summed over ranks
     states = __import__(pkg.__name__ + ".states", fromlist=["StateGroup"])
     grp = states.StateGroup(dist, device=f"cuda:{local}")
@@ -529,7 +538,8 @@ def run_ours(args):
                                f"{nsto} orbitals/GPU, Chebyshev L={L}, ncoef={s['ncoef']}, P={s['_P']}",
                    "orbitals_per_gpu": nsto, "L": L, "precision": args.prec, "mu": mu, "num_elec": ne,
                    "emin": emin, "emax": emax, "l2": "inputs (orbitals 0.43 GB/GPU) larger than L2; no flush",
-                   "setup_s": setup_s, "noise_host_s": noise_s, "parallelism": f"state-parallel x{world}"},
+                   "setup_s": setup_s, "noise_host_s": noise_s, "parallelism": f"state-parallel x{world}",
+                   "launch_shapes": tuned if tuned is not None else f"plane threads {args.plane_threads}"},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)]},
         "e2e": e2e, "gpu_launches": launches, "roofline": roof, "roofline_kernels": roof_all,
         "kernels": kernel_table, "eager": eager, "step_launch": "one CUDA graph" if graph else "eager", "fp64": fp64,
@@ -951,8 +961,8 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="cfg5: number of requests")
     ap.add_argument("--slots", type=int, default=16, help="cfg5: concurrent requests")
     ap.add_argument("--plane-threads", default="tuned", choices=["tuned", "256", "128"],
-                    help="plane-stage CTA size: cfg4 the autotuner's choice per system (tuned) or one size for all; "
-                         "cfg1-3 the library default (tuned) or the given size")
+                    help="plane-stage CTA size: the autotuner's choice (tuned: with the KB GEMM tile width and "
+                         "split-K, per system in cfg4) or one size for all (the GEMM shapes then per call)")
     ap.add_argument("--sat-requests", type=int, default=64,
                     help="cfg5: requests queued at once to measure the saturation rate")
     ap.add_argument("--sustained-requests", type=int, default=200,

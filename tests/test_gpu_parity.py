@@ -380,8 +380,9 @@ def test_tuner_sets_shapes(pkg, wl, sys2):
                 c.upload(cr, ci)
                 t.tune(c, ns, 4 * sys2["natm"], scale, em)
                 entry = t.cache[t.key(c, ns, 4 * sys2["natm"])]
-                assert entry["gemm_bn"] in (64, 128) and set(entry["gemm_bn_ms"]) == {"64", "128"}
-                assert entry["plane_threads"] in (128, 256)
+                assert entry["gemm_bn"] in (0, 64, 128) and set(entry["gemm_bn_ms"]) == {"0", "64", "128"}
+                assert entry["plane_threads"] in (0, 128, 256) and set(entry["plane_ms"]) == {"0", "128", "256"}
+                assert entry["split"] in (0, 1, 2, 4, 8, 16, 32)
             coef = pkg.calcChebyCoeff(16, emax - emin, em, 10.0, em, fun_flag=2)
             (sr,), (si,) = c.filterChebyPolyHerm(cr, ci, coef, 1, scale, em)
             res.append(np.concatenate([sr, si]))
